@@ -1,0 +1,210 @@
+/* piculator_b200.h -- C ABI of the B200 multiply engine for Piculator.
+ *
+ * Plain pointers and sizes only.  Every entry point returns a pic_status (the
+ * reference throws string literals instead; the mapping is listed on
+ * pic_status).  Device pointers are CUDA global-memory pointers on the device
+ * given to pic_init; host pointers are ordinary host memory.  Calls that take
+ * a pic_stream are ordered on that stream (NULL = the library's own stream);
+ * everything else is synchronous.  The library is thread-safe after pic_init
+ * (one internal lock serialises host-side bookkeeping).
+ *
+ * Reference interfaces replaced (file:line in vayun-mathur/Piculator):
+ *   NTT.h:4-9        ntt_* C API                   -> pic_ntt_*
+ *   FFT.h:4-9        fft_* C API                   -> pic_fft_*
+ *   Transform.h:5-33 Transform / mulNTT / mulFFT   -> pic_transform_*
+ *   BigFloat.h:8-46  class BigFloat (+ invsqrt)    -> pic_bf_* (handles)
+ *   BigFloat.cpp:326-444 BigFloat::mul's product   -> pic_mul, pic_mul_batch
+ *   PI.h:138-212     Pi(digits, threads)           -> pic_pi_hex
+ */
+#ifndef PICULATOR_B200_H
+#define PICULATOR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PIC_OK = 0,
+    PIC_ERR_INVALID = 1,         /* bad argument (null pointer, k out of range, ...) */
+    PIC_ERR_LENGTH = 2,          /* "FFT length is too small." FFT.cpp:501,536 NTT.cpp:353 */
+    PIC_ERR_DIVIDE_BY_ZERO = 3,  /* "Divide by Zero" BigFloat.cpp:451,524 */
+    PIC_ERR_LIMIT = 4,           /* "Limit Exceeded" PI.h:150-151 */
+    PIC_ERR_CUDA = 5,            /* a CUDA runtime call failed (see pic_last_error) */
+    PIC_ERR_NO_MEMORY = 6,       /* device or pinned-host allocation failed */
+    PIC_ERR_NOT_INITIALIZED = 7, /* pic_init has not succeeded */
+    PIC_ERR_IO = 8,              /* "Cannot Create File" PI.h:42 */
+    PIC_ERR_TIMEOUT = 9          /* a bounded device-side wait gave up */
+} pic_status;
+
+typedef void* pic_stream; /* a cudaStream_t */
+
+/* ---- library ------------------------------------------------------------ */
+pic_status pic_init(int device);
+pic_status pic_shutdown(void);
+const char* pic_last_error(void);
+const char* pic_status_string(pic_status s);
+pic_status pic_synchronize(void);
+/* Device bytes currently held by the library's pool and by live handles. */
+uint64_t pic_device_bytes_in_use(void);
+
+/* The library's own stream (a cudaStream_t), for callers that time or order
+ * work against it. */
+pic_stream pic_default_stream(void);
+
+/* Live kernel timing: between begin and end every instrumented launch is
+ * bracketed by CUDA events on its stream; end reports, per kernel class, the
+ * launches, summed device seconds and summed algorithmic bytes.  *n receives
+ * the number of classes (entries beyond cap are dropped). */
+typedef struct {
+    char name[24];
+    uint64_t launches;
+    double seconds;
+    double bytes;
+} pic_kernel_stat;
+pic_status pic_profile_begin(void);
+pic_status pic_profile_end(pic_kernel_stat* out, int cap, int* n);
+
+/* Test hook: make the next n device allocations fail with PIC_ERR_NO_MEMORY
+ * (host-side fault injection; no GPU fault is involved). */
+void pic_debug_fail_allocations(int n);
+
+/* ---- NTT.h:4-9 -- natural-order NTT mod the reference's prime for k ------ */
+/* T, A: device arrays of 2^k uint64 residues.  Same results word for word
+ * as the reference's ntt_forward / ntt_inverse / ntt_pointwise (prime table
+ * NTT.cpp:125-158, smallest generator NTT.cpp:104-123), for 11 <= k <= 32
+ * (the reference itself only serves k >= 27, NTT.cpp:299). */
+pic_status pic_ntt_ensure_table(int k);                                /* NTT.h:4 */
+pic_status pic_ntt_forward(uint64_t* T, int k, pic_stream s);          /* NTT.h:5 */
+pic_status pic_ntt_inverse(uint64_t* T, int k, pic_stream s);          /* NTT.h:6 */
+pic_status pic_ntt_pointwise(uint64_t* T, const uint64_t* A, int k,
+                             pic_stream s);                            /* NTT.h:7 */
+pic_status pic_int_to_ntt(uint64_t* T, int k, const uint32_t* A, size_t AL,
+                          pic_stream s);                               /* NTT.h:8 */
+pic_status pic_ntt_to_int(const uint64_t* T, int k, uint32_t* A, size_t AL,
+                          pic_stream s);                               /* NTT.h:9 */
+uint64_t pic_ntt_prime(int k); /* the reference's prime for 2^k (NTT.cpp:178) */
+
+/* ---- FFT.h:4-9 -- complex FP64 FFT, the reference's conventions ---------- */
+/* T, A: device arrays of 2^k complex doubles, interleaved (re, im).  forward
+ * is DIF with exp(+i theta) twiddles and bit-reversed output (FFT.cpp:64);
+ * inverse is DIT, bit-reversed in, natural out, unscaled (FFT.cpp:266).
+ * pic_fft_to_int rounds half up after scaling by 2^-k (FFT.cpp:520-571) and
+ * records the largest |x - round(x)| it saw (pic_fft_last_max_err). */
+pic_status pic_fft_ensure_table(int k);                                /* FFT.h:4 */
+pic_status pic_fft_forward(double* T, int k, pic_stream s);            /* FFT.h:5 */
+pic_status pic_fft_inverse(double* T, int k, pic_stream s);            /* FFT.h:6 */
+pic_status pic_fft_pointwise(double* T, const double* A, int k,
+                             pic_stream s);                            /* FFT.h:7 */
+pic_status pic_int_to_fft(double* T, int k, const uint32_t* A, size_t AL,
+                          pic_stream s);                               /* FFT.h:8 */
+pic_status pic_fft_to_int(const double* T, int k, uint32_t* A, size_t AL,
+                          pic_stream s);                               /* FFT.h:9 */
+double pic_fft_last_max_err(void);
+
+/* ---- whole products (the core of BigFloat::mul, BigFloat.cpp:413-487) ---- */
+/* z[0 .. na+nb) = a * b exactly, device words, little-endian base 2^32.
+ * z must not overlap a or b.  Any mode gives identical words. */
+enum {
+    PIC_MUL_AUTO = 0,     /* per-size choice from the tuned size classes */
+    PIC_MUL_NTT_REF = 1,  /* the reference's layout: 16-bit points, one prime,
+                             length 2^k >= 4(na+nb) (BigFloat.cpp:380-385) */
+    PIC_MUL_NTT3 = 2,     /* three 62-bit primes, 64-bit points, CRT */
+    PIC_MUL_FFT = 3,      /* FP64 FFT, limb split from the rounding bound,
+                             NTT recompute when max distance > 0.25 */
+    PIC_MUL_SCHOOL = 4    /* batched schoolbook (short operands) */
+};
+pic_status pic_mul(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b,
+                   size_t nb, int mode, pic_stream s);
+
+/* Many independent products in one call (device pointers in each record).
+ * The descriptor array itself is host memory. */
+typedef struct {
+    uint32_t* z;
+    const uint32_t* a;
+    const uint32_t* b;
+    uint64_t na;
+    uint64_t nb;
+} pic_mul_desc;
+pic_status pic_mul_batch(const pic_mul_desc* descs, size_t count, int mode,
+                         pic_stream s);
+
+/* Host-buffer convenience: copies in, multiplies, copies out (synchronous). */
+pic_status pic_mul_host(uint32_t* z, const uint32_t* a, size_t na,
+                        const uint32_t* b, size_t nb, int mode);
+
+/* ---- BigFloat (BigFloat.h:8-46) as device-resident handles -------------- */
+/* Semantics are the reference's exactly: sign/exp/L/T with exp counted in
+ * 32-bit words, precision p in words with 2 guard words
+ * (YCL_BIGFLOAT_EXTRA_PRECISION, BigFloat.h:6), p == 0 meaning exact. */
+typedef struct pic_bigfloat_s* pic_bf;
+
+pic_status pic_bf_from_words(pic_bf* out, int sign, int64_t exp,
+                             const uint32_t* words_host, size_t L);
+pic_status pic_bf_from_u32(pic_bf* out, uint32_t x, int sign); /* BigFloat.cpp:64 */
+pic_status pic_bf_free(pic_bf x);
+pic_status pic_bf_info(pic_bf x, int* sign, int64_t* exp, size_t* L);
+pic_status pic_bf_to_words(pic_bf x, uint32_t* words_host, size_t cap);
+pic_status pic_bf_negate(pic_bf x);                                  /* :150 */
+pic_status pic_bf_mul_u32(pic_bf* out, pic_bf a, uint32_t x);        /* :156 */
+pic_status pic_bf_add(pic_bf* out, pic_bf a, pic_bf b, size_t p);    /* :288 */
+pic_status pic_bf_sub(pic_bf* out, pic_bf a, pic_bf b, size_t p);    /* :306 */
+pic_status pic_bf_mul(pic_bf* out, pic_bf a, pic_bf b, size_t p, int mode); /* :326 */
+pic_status pic_bf_rcp(pic_bf* out, pic_bf a, size_t p, int mode);    /* :445 */
+pic_status pic_bf_div(pic_bf* out, pic_bf a, pic_bf b, size_t p, int mode); /* :512 */
+pic_status pic_bf_invsqrt(pic_bf* out, uint32_t x, size_t p, int mode); /* :516 */
+int pic_bf_ucmp(pic_bf a, pic_bf b);                                  /* :123 */
+pic_status pic_bf_to_hex(pic_bf x, size_t digits, char* buf, size_t cap); /* :95 */
+
+/* ---- Transform.h:5-33 -- transform-domain operands ----------------------- */
+/* A pic_transform holds one operand's forward transform (three-prime form)
+ * plus the BigFloat metadata of Transform.h:5-11, so a factor used in several
+ * products is transformed once.  mul accumulates pointwise like mulNTT. */
+typedef struct pic_transform_s* pic_transform;
+pic_status pic_transform_create(pic_transform* out, pic_bf x, size_t p, int k);
+pic_status pic_transform_mul(pic_transform t1, pic_transform t2); /* mulNTT, Transform.h:13-18 */
+pic_status pic_transform_to_bf(pic_bf* out, pic_transform t);
+pic_status pic_transform_free(pic_transform t);                    /* deleteNTT, :27-29 */
+
+/* ---- Pi (PI.h:138-212) ---------------------------------------------------- */
+enum {
+    PIC_PI_CHOSEN = 0, /* batched binary-splitting levels + tuned products */
+    PIC_PI_PLAIN = 1   /* one BigFloat::mul per product, reference-layout NTT */
+};
+typedef struct {
+    uint64_t hex_digits;   /* PI.h:141 */
+    uint64_t p_words;      /* PI.h:142 */
+    uint64_t terms;        /* PI.h:144 */
+    double seconds_bsr;    /* device time per phase (CUDA events) */
+    double seconds_div;
+    double seconds_invsqrt;
+    double seconds_final_mul;
+    double seconds_hex;
+    double seconds_total;
+    uint64_t kernel_launches;
+    uint64_t products;     /* number of big products formed */
+    double fft_max_err;    /* largest FFT rounding distance seen */
+    uint64_t fft_recomputes;
+} pic_pi_stats;
+
+/* Computes pi to decimal_digits and writes the text the reference dumps into
+ * pi.txt (to_string_hex, PI.h:204) into out (host), NUL-terminated.  Set
+ * out = NULL to compute without copying the digits back. */
+pic_status pic_pi_hex(uint64_t decimal_digits, int mode, char* out, size_t cap,
+                      size_t* out_len, pic_pi_stats* stats);
+
+/* Pi() without the final text: the result stays on the device as a BigFloat
+ * handle (free it with pic_bf_free; pic_bf_to_hex gives the text). */
+pic_status pic_pi_compute(uint64_t decimal_digits, int mode, pic_bf* out,
+                          pic_pi_stats* stats);
+
+/* Sizes Pi() derives from the digit count (PI.h:141-144). */
+pic_status pic_pi_sizes(uint64_t decimal_digits, uint64_t* hex_digits,
+                        uint64_t* p_words, uint64_t* terms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PICULATOR_B200_H */

@@ -1,0 +1,12 @@
+// Chudnovsky binary splitting (PI.h:64-136), batched form.
+#pragma once
+#include <stdint.h>
+
+#include "bigfloat.hpp"
+
+namespace pic {
+
+// Same P, Q, R as Pi_BSR(P, Q, R, a, b, p) word for word.
+void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, size_t p);
+
+}  // namespace pic

@@ -1,0 +1,560 @@
+// extern "C" entry points of include/piculator_b200.h.  Each one converts
+// internal exceptions into a pic_status and records the message for
+// pic_last_error().
+#include <string.h>
+
+#include <memory>
+#include <string>
+
+#include "bigfloat.hpp"
+#include "common.cuh"
+#include "fft.cuh"
+#include "mul.cuh"
+#include "ntt.cuh"
+#include "pi.cuh"
+#include "transform.cuh"
+
+namespace pic {
+void profile_begin();
+int profile_end(pic_kernel_stat* out, int cap);
+void init_context(int device);
+void shutdown_context();
+void set_last_error(const std::string& s);
+const std::string& last_error();
+}  // namespace pic
+
+using namespace pic;
+
+struct pic_bigfloat_s {
+    BigFloat v;
+};
+
+template <class F>
+static pic_status guarded(F&& f)
+{
+    try {
+        f();
+        return PIC_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return PIC_ERR_NO_MEMORY;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return PIC_ERR_INVALID;
+    }
+}
+
+static pic_bf wrap(BigFloat&& v)
+{
+    pic_bf h = new pic_bigfloat_s{std::move(v)};
+    return h;
+}
+
+template <class F>
+static void with_mode(int mode, F&& f)
+{
+    const int saved = get_mul_mode();
+    set_mul_mode(mode);
+    try {
+        f();
+    } catch (...) {
+        set_mul_mode(saved);
+        throw;
+    }
+    set_mul_mode(saved);
+}
+
+#define PIC_REQ_PTR(p) PIC_REQUIRE((p) != nullptr, PIC_ERR_INVALID, #p " is NULL")
+
+extern "C" {
+
+pic_status pic_init(int device)
+{
+    return guarded([&] { init_context(device); });
+}
+
+pic_status pic_shutdown(void)
+{
+    return guarded([&] { shutdown_context(); });
+}
+
+const char* pic_last_error(void) { return last_error().c_str(); }
+
+const char* pic_status_string(pic_status s)
+{
+    switch (s) {
+    case PIC_OK: return "ok";
+    case PIC_ERR_INVALID: return "invalid argument";
+    case PIC_ERR_LENGTH: return "FFT length is too small.";
+    case PIC_ERR_DIVIDE_BY_ZERO: return "Divide by Zero";
+    case PIC_ERR_LIMIT: return "Limit Exceeded";
+    case PIC_ERR_CUDA: return "CUDA error";
+    case PIC_ERR_NO_MEMORY: return "out of memory";
+    case PIC_ERR_NOT_INITIALIZED: return "not initialised";
+    case PIC_ERR_IO: return "Cannot Create File";
+    case PIC_ERR_TIMEOUT: return "device wait timed out";
+    }
+    return "unknown status";
+}
+
+pic_status pic_synchronize(void)
+{
+    return guarded([&] {
+        require_init();
+        PIC_CUDA(cudaStreamSynchronize(ctx().stream));
+    });
+}
+
+uint64_t pic_device_bytes_in_use(void) { return ctx().bytes_in_use.load(); }
+
+void pic_debug_fail_allocations(int n) { ctx().fail_allocs.store(n); }
+
+pic_stream pic_default_stream(void) { return initialized() ? (pic_stream)ctx().stream : nullptr; }
+
+pic_status pic_profile_begin(void)
+{
+    return guarded([&] {
+        require_init();
+        profile_begin();
+    });
+}
+
+pic_status pic_profile_end(pic_kernel_stat* out, int cap, int* n)
+{
+    return guarded([&] {
+        require_init();
+        const int m = profile_end(out, cap);
+        if (n) *n = m;
+    });
+}
+
+// ---- NTT.h ---------------------------------------------------------------------
+static PrimeDev ref_prime_dev(int k)
+{
+    PIC_REQUIRE(k >= 1 && k <= 32, PIC_ERR_INVALID, "k out of range (1..32)");
+    return prime_tables(reference_prime(k)).dev;
+}
+
+static NttBatch single(uint64_t* T, int k, const PrimeDev& P)
+{
+    NttBatch b;
+    b.data = T;
+    b.stride = (size_t)1 << k;
+    b.count = 1;
+    b.per_prime = 1;
+    b.prime[0] = P;
+    return b;
+}
+
+pic_status pic_ntt_ensure_table(int k)
+{
+    return guarded([&] {
+        require_init();
+        ref_prime_dev(k);
+    });
+}
+
+pic_status pic_ntt_forward(uint64_t* T, int k, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(T);
+        const PrimeDev P = ref_prime_dev(k);
+        NttBatch b = single(T, k, P);
+        ntt_forward_dif(b, k, resolve(s));
+        ntt_bitreverse(b, k, resolve(s));
+    });
+}
+
+pic_status pic_ntt_inverse(uint64_t* T, int k, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(T);
+        const PrimeDev P = ref_prime_dev(k);
+        NttBatch b = single(T, k, P);
+        ntt_bitreverse(b, k, resolve(s));
+        ntt_inverse_dit(b, k, resolve(s));
+        ntt_scale_ninv(T, k, P, resolve(s));  // rN, NTT.cpp:83
+    });
+}
+
+pic_status pic_ntt_pointwise(uint64_t* T, const uint64_t* A, int k, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(T);
+        PIC_REQ_PTR(A);
+        ntt_pointwise_plain(T, A, k, ref_prime_dev(k), resolve(s));
+    });
+}
+
+pic_status pic_int_to_ntt(uint64_t* T, int k, const uint32_t* A, size_t AL, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(T);
+        PIC_REQUIRE(AL == 0 || A, PIC_ERR_INVALID, "A is NULL");
+        PIC_REQUIRE(k >= 1 && k <= 32, PIC_ERR_INVALID, "k out of range");
+        int_to_ntt_dev(T, k, A, AL, resolve(s));
+    });
+}
+
+pic_status pic_ntt_to_int(const uint64_t* T, int k, uint32_t* A, size_t AL, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(T);
+        PIC_REQUIRE(AL == 0 || A, PIC_ERR_INVALID, "A is NULL");
+        PIC_REQUIRE(k >= 1 && k <= 32, PIC_ERR_INVALID, "k out of range");
+        ntt_to_int_dev(T, k, A, AL, resolve(s));
+    });
+}
+
+uint64_t pic_ntt_prime(int k) { return (k >= 1 && k <= 42) ? reference_prime(k) : 0; }
+
+// ---- FFT.h ---------------------------------------------------------------------
+pic_status pic_fft_ensure_table(int k)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQUIRE(k >= 1 && k <= 30, PIC_ERR_INVALID, "k out of range (1..30)");
+    });
+}
+
+pic_status pic_fft_forward(double* T, int k, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(T);
+        fft_forward_dif(FftBatch{(double2*)T, (size_t)1 << k, 1}, k, resolve(s));
+    });
+}
+
+pic_status pic_fft_inverse(double* T, int k, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(T);
+        fft_inverse_dit(FftBatch{(double2*)T, (size_t)1 << k, 1}, k, resolve(s));
+    });
+}
+
+pic_status pic_fft_pointwise(double* T, const double* A, int k, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(T);
+        PIC_REQ_PTR(A);
+        PIC_REQUIRE(k >= 1 && k <= 30, PIC_ERR_INVALID, "k out of range (1..30)");
+        fft_pointwise((double2*)T, (const double2*)A, (size_t)1 << k, resolve(s));
+    });
+}
+
+pic_status pic_int_to_fft(double* T, int k, const uint32_t* A, size_t AL, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(T);
+        PIC_REQUIRE(k >= 1 && k <= 30, PIC_ERR_INVALID, "k out of range (1..30)");
+        PIC_REQUIRE(((size_t)1 << k) >= 4 * AL, PIC_ERR_LENGTH, "FFT length is too small.");  // FFT.cpp:500-501
+        fft_split((double2*)T, k, A, AL, 8, resolve(s));
+    });
+}
+
+pic_status pic_fft_to_int(const double* T, int k, uint32_t* A, size_t AL, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(T);
+        PIC_REQUIRE(k >= 1 && k <= 30, PIC_ERR_INVALID, "k out of range (1..30)");
+        PIC_REQUIRE(((size_t)1 << k) >= 4 * AL, PIC_ERR_LENGTH, "FFT length is too small.");  // FFT.cpp:535-536
+        const double e = fft_coef_to_words((const double2*)T, 4 * AL, 1.0 / (double)((size_t)1 << k), 8, A, AL,
+                                           resolve(s));
+        fft_note_max_err(e);
+    });
+}
+
+double pic_fft_last_max_err(void) { return fft_last_max_err(); }
+
+// ---- products -----------------------------------------------------------------
+pic_status pic_mul(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int mode,
+                   pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(z);
+        PIC_REQ_PTR(a);
+        PIC_REQ_PTR(b);
+        PIC_REQUIRE(na > 0 && nb > 0, PIC_ERR_INVALID, "empty operand");
+        mul_dispatch(z, a, na, b, nb, mode, resolve(s));
+    });
+}
+
+pic_status pic_mul_batch(const pic_mul_desc* d, size_t count, int mode, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQUIRE(count == 0 || d, PIC_ERR_INVALID, "descs is NULL");
+        mul_batch(d, count, mode, resolve(s));
+    });
+}
+
+pic_status pic_mul_host(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int mode)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(z);
+        PIC_REQ_PTR(a);
+        PIC_REQ_PTR(b);
+        PIC_REQUIRE(na > 0 && nb > 0, PIC_ERR_INVALID, "empty operand");
+        cudaStream_t st = ctx().stream;
+        DevBuf<uint32_t> da(na, st), db(nb, st), dz(na + nb, st);
+        PIC_CUDA(cudaMemcpyAsync(da.get(), a, na * 4, cudaMemcpyHostToDevice, st));
+        PIC_CUDA(cudaMemcpyAsync(db.get(), b, nb * 4, cudaMemcpyHostToDevice, st));
+        mul_dispatch(dz.get(), da.get(), na, db.get(), nb, mode, st);
+        PIC_CUDA(cudaMemcpyAsync(z, dz.get(), (na + nb) * 4, cudaMemcpyDeviceToHost, st));
+        PIC_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+// ---- BigFloat handles ------------------------------------------------------------
+pic_status pic_bf_from_words(pic_bf* out, int sign, int64_t exp, const uint32_t* words, size_t L)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQUIRE(L == 0 || words, PIC_ERR_INVALID, "words is NULL");
+        *out = wrap(BigFloat::from_host(sign != 0, exp, words, L));
+    });
+}
+
+pic_status pic_bf_from_u32(pic_bf* out, uint32_t x, int sign)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        *out = wrap(BigFloat(x, sign != 0));
+    });
+}
+
+pic_status pic_bf_free(pic_bf x)
+{
+    return guarded([&] { delete x; });
+}
+
+pic_status pic_bf_info(pic_bf x, int* sign, int64_t* exp, size_t* L)
+{
+    return guarded([&] {
+        PIC_REQ_PTR(x);
+        if (sign) *sign = x->v.get_sign() ? 1 : 0;
+        if (exp) *exp = x->v.get_exponent();
+        if (L) *L = x->v.get_precision();
+    });
+}
+
+pic_status pic_bf_to_words(pic_bf x, uint32_t* words, size_t cap)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(x);
+        PIC_REQUIRE(cap >= x->v.get_precision(), PIC_ERR_INVALID, "capacity too small");
+        if (x->v.get_precision()) x->v.to_host(words);
+    });
+}
+
+pic_status pic_bf_negate(pic_bf x)
+{
+    return guarded([&] {
+        PIC_REQ_PTR(x);
+        x->v.negate();
+    });
+}
+
+pic_status pic_bf_mul_u32(pic_bf* out, pic_bf a, uint32_t x)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQ_PTR(a);
+        *out = wrap(a->v.mul(x));
+    });
+}
+
+pic_status pic_bf_add(pic_bf* out, pic_bf a, pic_bf b, size_t p)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQ_PTR(a);
+        PIC_REQ_PTR(b);
+        *out = wrap(a->v.add(b->v, p));
+    });
+}
+
+pic_status pic_bf_sub(pic_bf* out, pic_bf a, pic_bf b, size_t p)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQ_PTR(a);
+        PIC_REQ_PTR(b);
+        *out = wrap(a->v.sub(b->v, p));
+    });
+}
+
+pic_status pic_bf_mul(pic_bf* out, pic_bf a, pic_bf b, size_t p, int mode)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQ_PTR(a);
+        PIC_REQ_PTR(b);
+        with_mode(mode, [&] { *out = wrap(a->v.mul(b->v, p)); });
+    });
+}
+
+pic_status pic_bf_rcp(pic_bf* out, pic_bf a, size_t p, int mode)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQ_PTR(a);
+        with_mode(mode, [&] { *out = wrap(a->v.rcp(p)); });
+    });
+}
+
+pic_status pic_bf_div(pic_bf* out, pic_bf a, pic_bf b, size_t p, int mode)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQ_PTR(a);
+        PIC_REQ_PTR(b);
+        with_mode(mode, [&] { *out = wrap(a->v.div(b->v, p)); });
+    });
+}
+
+pic_status pic_bf_invsqrt(pic_bf* out, uint32_t x, size_t p, int mode)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        with_mode(mode, [&] { *out = wrap(invsqrt(x, p)); });
+    });
+}
+
+int pic_bf_ucmp(pic_bf a, pic_bf b)
+{
+    int r = 0;
+    pic_status st = guarded([&] {
+        require_init();
+        PIC_REQ_PTR(a);
+        PIC_REQ_PTR(b);
+        r = a->v.ucmp(b->v);
+    });
+    return st == PIC_OK ? r : -2;
+}
+
+pic_status pic_bf_to_hex(pic_bf x, size_t digits, char* buf, size_t cap)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(x);
+        PIC_REQ_PTR(buf);
+        x->v.hex_into(digits, buf, cap);
+    });
+}
+
+// ---- Transform.h ----------------------------------------------------------------
+struct pic_transform_s {
+    TransformOperand t;
+};
+
+pic_status pic_transform_create(pic_transform* out, pic_bf x, size_t p, int k)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQ_PTR(x);
+        *out = new pic_transform_s{transform_create(x->v, p, k)};
+    });
+}
+
+pic_status pic_transform_mul(pic_transform t1, pic_transform t2)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(t1);
+        PIC_REQ_PTR(t2);
+        transform_mul(t1->t, t2->t);
+    });
+}
+
+pic_status pic_transform_to_bf(pic_bf* out, pic_transform t)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQ_PTR(t);
+        *out = wrap(transform_to_bigfloat(t->t));
+    });
+}
+
+pic_status pic_transform_free(pic_transform t)
+{
+    return guarded([&] { delete t; });
+}
+
+// ---- Pi -------------------------------------------------------------------------
+pic_status pic_pi_sizes(uint64_t d, uint64_t* hex_digits, uint64_t* p_words, uint64_t* terms)
+{
+    return guarded([&] { pi_sizes(d, hex_digits, p_words, terms); });
+}
+
+pic_status pic_pi_compute(uint64_t decimal_digits, int mode, pic_bf* out, pic_pi_stats* stats)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQUIRE(mode == PIC_PI_CHOSEN || mode == PIC_PI_PLAIN, PIC_ERR_INVALID, "unknown pi mode");
+        pic_pi_stats local;
+        BigFloat P = pi_compute(decimal_digits, mode, &local);
+        *out = wrap(std::move(P));
+        if (stats) *stats = local;
+    });
+}
+
+pic_status pic_pi_hex(uint64_t decimal_digits, int mode, char* out, size_t cap, size_t* out_len,
+                      pic_pi_stats* stats)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQUIRE(mode == PIC_PI_CHOSEN || mode == PIC_PI_PLAIN, PIC_ERR_INVALID, "unknown pi mode");
+        pic_pi_stats local;
+        BigFloat P = pi_compute(decimal_digits, mode, &local);
+        uint64_t hex;
+        pi_sizes(decimal_digits, &hex, nullptr, nullptr);
+        if (out) {
+            cudaEvent_t e0, e1;
+            PIC_CUDA(cudaEventCreate(&e0));
+            PIC_CUDA(cudaEventCreate(&e1));
+            PIC_CUDA(cudaEventRecord(e0, ctx().stream));
+            const size_t n = P.hex_into((size_t)hex, out, cap);  // to_string_hex, PI.h:204
+            PIC_CUDA(cudaEventRecord(e1, ctx().stream));
+            PIC_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            local.seconds_hex = ms / 1000.0;
+            if (out_len) *out_len = n;
+        }
+        if (stats) *stats = local;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,566 @@
+// Exact products: piece split, multi-prime NTT convolution, CRT and carry.
+#include <math.h>
+#include <string.h>
+
+#include <atomic>
+
+#include "carry.cuh"
+#include "common.cuh"
+#include "mul.cuh"
+
+namespace pic {
+
+static inline int ceil_log2(size_t n)
+{
+    int k = 0;
+    while (((size_t)1 << k) < n) k++;
+    return k;
+}
+
+// ---- split -----------------------------------------------------------------
+// Three-prime form: piece j = a[2j] | a[2j+1] << 32, reduced mod each prime.
+__global__ void split3_kernel(uint64_t* __restrict__ out, const uint32_t* __restrict__ a, size_t na, size_t N,
+                              uint64_t p0, uint64_t p1, uint64_t p2)
+{
+    const size_t np = (na + 1) / 2;
+    for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < N; j += (size_t)gridDim.x * blockDim.x) {
+        uint64_t v = 0;
+        if (j < np) {
+            const uint64_t lo = a[2 * j];
+            const uint64_t hi = (2 * j + 1 < na) ? a[2 * j + 1] : 0u;
+            v = lo | (hi << 32);
+        }
+        uint64_t r0 = v, r1 = v, r2 = v;  // v < 2^64 < 5 p
+        while (r0 >= p0) r0 -= p0;
+        while (r1 >= p1) r1 -= p1;
+        while (r2 >= p2) r2 -= p2;
+        out[j] = r0;
+        out[N + j] = r1;
+        out[2 * N + j] = r2;
+    }
+}
+
+// Reference layout, int_to_ntt NTT.cpp:330-341: two 16-bit points per word.
+__global__ void split16_kernel(uint64_t* __restrict__ T, size_t N, const uint32_t* __restrict__ A, size_t AL)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t w = i >> 1;
+        uint64_t v = 0;
+        if (w < AL) v = (i & 1) ? (A[w] >> 16) : (A[w] & 0xffffu);
+        T[i] = v;
+    }
+}
+
+// ---- coefficient -> word conversion ----------------------------------------
+constexpr int kCvtThreads = 256;
+constexpr int kCvtLPT = 2;  // 64-bit limbs per thread
+constexpr size_t kCvtLPC = (size_t)kCvtThreads * kCvtLPT;
+constexpr size_t kCvtWPC = 2 * kCvtLPC;
+
+struct Crt3Consts {
+    uint64_t p[3], pinv[3];
+    uint64_t scale[3];     // R^2 N^-1 mod p_q: undoes the pointwise R^-1 and the unscaled inverse
+    uint64_t inv01_m;      // Montgomery form of p0^-1 mod p1
+    uint64_t p0_mod_p2_m;  // Montgomery form of p0 mod p2
+    uint64_t inv012_m;     // Montgomery form of (p0 p1)^-1 mod p2
+    uint64_t p0p1_lo, p0p1_hi;
+};
+
+// Garner's CRT: x = r0 + p0 (v1 + p1 v2), 0 <= x < p0 p1 p2, as three limbs.
+__device__ __forceinline__ void crt3(const Crt3Consts& C, uint64_t y0, uint64_t y1, uint64_t y2, uint64_t& l0,
+                                     uint64_t& l1, uint64_t& l2)
+{
+    const uint64_t r0 = mont_mul(y0, C.scale[0], C.p[0], C.pinv[0]);
+    const uint64_t r1 = mont_mul(y1, C.scale[1], C.p[1], C.pinv[1]);
+    const uint64_t r2 = mont_mul(y2, C.scale[2], C.p[2], C.pinv[2]);
+    const uint64_t r0m1 = r0 >= C.p[1] ? r0 - C.p[1] : r0;
+    const uint64_t v1 = mont_mul(sub_mod(r1, r0m1, C.p[1]), C.inv01_m, C.p[1], C.pinv[1]);
+    const uint64_t r0m2 = r0 >= C.p[2] ? r0 - C.p[2] : r0;
+    uint64_t t = sub_mod(r2, r0m2, C.p[2]);
+    t = sub_mod(t, mont_mul(v1, C.p0_mod_p2_m, C.p[2], C.pinv[2]), C.p[2]);
+    const uint64_t v2 = mont_mul(t, C.inv012_m, C.p[2], C.pinv[2]);
+    // p0 * v1 + r0
+    uint64_t a0 = C.p[0] * v1, a1 = mulhi64(C.p[0], v1);
+    a0 += r0;
+    a1 += (a0 < r0);
+    // (p0 p1) * v2
+    const uint64_t b0 = C.p0p1_lo * v2;
+    uint64_t b1 = mulhi64(C.p0p1_lo, v2);
+    const uint64_t t1 = C.p0p1_hi * v2;
+    uint64_t b2 = mulhi64(C.p0p1_hi, v2);
+    b1 += t1;
+    b2 += (b1 < t1);
+    l0 = a0 + b0;
+    const uint64_t c0 = l0 < b0;
+    uint64_t s1 = a1 + b1;
+    uint64_t c1 = s1 < b1;
+    s1 += c0;
+    c1 += (s1 < c0);
+    l1 = s1;
+    l2 = b2 + c1;
+}
+
+// Shared tail of both conversions: limb digits (T = D_i + C_(i-1)) -> words
+// with in-block carry resolution; writes the CTA's (G, P).
+__device__ __forceinline__ void limbs_to_words(const uint64_t (&dig)[kCvtLPT], const uint32_t (&gen)[kCvtLPT],
+                                               size_t first_limb, uint32_t* z, size_t zw, uint32_t* agg)
+{
+    uint32_t gp = kGPIdentity;
+#pragma unroll
+    for (int u = 0; u < kCvtLPT; u++) {
+        const uint32_t lo = (uint32_t)dig[u], hi = (uint32_t)(dig[u] >> 32);
+        gp = gp_combine(gp, (uint32_t)(lo == 0xffffffffu) << 1);
+        gp = gp_combine(gp, gen[u] | ((uint32_t)(hi == 0xffffffffu) << 1));
+    }
+    uint32_t total;
+    uint32_t cin = block_gp_scan(gp, &total) & 1u;
+#pragma unroll
+    for (int u = 0; u < kCvtLPT; u++) {
+        const size_t w = 2 * (first_limb + u);
+        const uint32_t lo = (uint32_t)dig[u], hi = (uint32_t)(dig[u] >> 32);
+        if (w < zw) z[w] = lo + cin;
+        cin = (uint32_t)(lo == 0xffffffffu) & cin;
+        if (w + 1 < zw) z[w + 1] = hi + cin;
+        cin = gen[u] | ((uint32_t)(hi == 0xffffffffu) & cin);
+    }
+    if (threadIdx.x == 0) agg[blockIdx.x] = total;
+}
+
+__device__ __forceinline__ void add128(uint64_t& lo, uint64_t& hi, uint64_t v)
+{
+    lo += v;
+    hi += (lo < v);
+}
+
+// Three-prime residues Y[q * N + j] -> words.  Limb i (64 bits) collects
+// x_i.l0 + x_(i-1).l1 + x_(i-2).l2 (< 3 * 2^64).
+__global__ void __launch_bounds__(kCvtThreads) crt3_k1(const uint64_t* __restrict__ Y, size_t N, size_t ncoef,
+                                                       Crt3Consts C, uint32_t* __restrict__ z, size_t zw,
+                                                       uint32_t* agg)
+{
+    __shared__ uint64_t xs[(kCvtLPC + 3) * 3];
+    const int64_t i0 = (int64_t)blockIdx.x * (int64_t)kCvtLPC;
+    for (int t = threadIdx.x; t < (int)kCvtLPC + 3; t += blockDim.x) {
+        const int64_t j = i0 - 3 + t;
+        uint64_t l0 = 0, l1 = 0, l2 = 0;
+        if (j >= 0 && (size_t)j < ncoef) crt3(C, Y[j], Y[N + j], Y[2 * N + j], l0, l1, l2);
+        xs[3 * t] = l0;
+        xs[3 * t + 1] = l1;
+        xs[3 * t + 2] = l2;
+    }
+    __syncthreads();
+    uint64_t dig[kCvtLPT];
+    uint32_t gen[kCvtLPT];
+#pragma unroll
+    for (int u = 0; u < kCvtLPT; u++) {
+        const int li = threadIdx.x * kCvtLPT + u + 3;  // xs slot of coefficient i
+        uint64_t slo = xs[3 * li], shi = 0;
+        add128(slo, shi, xs[3 * (li - 1) + 1]);
+        add128(slo, shi, xs[3 * (li - 2) + 2]);
+        uint64_t plo = xs[3 * (li - 1)], phi = 0;
+        add128(plo, phi, xs[3 * (li - 2) + 1]);
+        add128(plo, phi, xs[3 * (li - 3) + 2]);
+        const uint64_t d = slo + phi;
+        dig[u] = d;
+        gen[u] = d < slo;
+    }
+    limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw, agg);
+}
+
+// Coefficients c_j at bit offsets bits * j (8 <= bits <= 16) -> words.  Limb
+// i (bits [64i, 64i+64)) collects lo64(c_j << r_j) for the j with
+// floor(bits j / 64) == i and hi64(c_j << r_j) for those with i - 1, where
+// r_j = bits j mod 64.  A loader supplies c_j (< 2^64).
+constexpr int kStageMax = (int)(64 * (kCvtLPC + 2) / 8 + 2);
+
+__device__ __forceinline__ int64_t first_coef(int64_t limb, int bits)
+{
+    return limb <= 0 ? 0 : (64 * limb + bits - 1) / bits;
+}
+
+__device__ __forceinline__ void limb_sum(const uint64_t* cs, int64_t jlo, int64_t limb, int bits, uint64_t& lo,
+                                         uint64_t& hi)
+{
+    lo = 0;
+    hi = 0;
+    if (limb < 0) return;
+    const int64_t a = first_coef(limb - 1, bits), b = first_coef(limb, bits), c = first_coef(limb + 1, bits);
+    if (limb >= 1)
+        for (int64_t j = a; j < b; j++) {
+            const int r = (int)((bits * j) & 63);
+            if (r) add128(lo, hi, cs[j - jlo] >> (64 - r));
+        }
+    for (int64_t j = b; j < c; j++) add128(lo, hi, cs[j - jlo] << ((bits * j) & 63));
+}
+
+struct NttCoefLoader {
+    const uint64_t* c;
+    uint64_t scale, p, pinv;
+    __device__ __forceinline__ uint64_t operator()(size_t j, double&) const
+    {
+        uint64_t v = c[j];
+        return scale ? mont_mul(v, scale, p, pinv) : v;
+    }
+};
+
+struct FftCoefLoader {
+    const double2* T;
+    double scale;
+    __device__ __forceinline__ uint64_t operator()(size_t j, double& emax) const
+    {
+        const double f = T[j].x * scale;
+        const double r = rint(f);
+        const double e = fabs(f - r);
+        if (e > emax) emax = e;
+        return r > 0 ? (uint64_t)r : 0;
+    }
+};
+
+template <class Loader>
+__global__ void __launch_bounds__(kCvtThreads) coefbits_k1(Loader ld, size_t ncoef, int bits,
+                                                           uint32_t* __restrict__ z, size_t zw, uint32_t* agg,
+                                                           unsigned long long* err_bits)
+{
+    __shared__ uint64_t cs[kStageMax];
+    const int64_t i0 = (int64_t)blockIdx.x * (int64_t)kCvtLPC;
+    const int64_t jlo = first_coef(i0 - 2, bits), jhi = first_coef(i0 + (int64_t)kCvtLPC, bits);
+    double emax = 0.0;
+    for (int64_t t = threadIdx.x; t < jhi - jlo; t += blockDim.x) {
+        const int64_t j = jlo + t;
+        cs[t] = (j < (int64_t)ncoef) ? ld((size_t)j, emax) : 0;
+    }
+    if (err_bits) {
+#pragma unroll
+        for (int off = 16; off; off >>= 1) emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, off));
+        if ((threadIdx.x & 31) == 0 && emax > 0.0) atomicMax(err_bits, (unsigned long long)__double_as_longlong(emax));
+    }
+    __syncthreads();
+    uint64_t dig[kCvtLPT];
+    uint32_t gen[kCvtLPT];
+#pragma unroll
+    for (int u = 0; u < kCvtLPT; u++) {
+        const int64_t i = i0 + threadIdx.x * kCvtLPT + u;
+        uint64_t slo, shi, plo, phi;
+        limb_sum(cs, jlo, i, bits, slo, shi);
+        limb_sum(cs, jlo, i - 1, bits, plo, phi);
+        const uint64_t d = slo + phi;
+        dig[u] = d;
+        gen[u] = d < slo;
+    }
+    limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw, agg);
+}
+
+static void finish_scan(uint32_t* z, size_t zw, uint32_t* agg, size_t nctas, cudaStream_t s)
+{
+    carry_scan_aggregates(agg, nctas, nullptr, s);
+    carry_ripple(z, zw, kCvtWPC, agg, nctas, kCarryAdd, s);
+}
+
+void coef16_to_words(const uint64_t* c, size_t ncoef, uint64_t scale_mont, uint64_t p, uint64_t pinv_neg,
+                     uint32_t* z, size_t zw, cudaStream_t s)
+{
+    if (zw == 0) return;
+    const size_t nlimbs = (zw + 1) / 2;
+    const size_t nctas = (nlimbs + kCvtLPC - 1) / kCvtLPC;
+    DevBuf<uint32_t> agg(nctas, s);
+    ProfScope ps(KC_CRT, 8.0 * (double)ncoef + 4.0 * (double)zw, s);
+    coefbits_k1<NttCoefLoader><<<(unsigned)nctas, kCvtThreads, 0, s>>>(
+        NttCoefLoader{c, scale_mont, p, pinv_neg}, ncoef, 16, z, zw, agg.get(), nullptr);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+    finish_scan(z, zw, agg.get(), nctas, s);
+}
+
+double fft_coef_to_words(const double2* T, size_t ncoef, double scale, int bits, uint32_t* z, size_t zw,
+                         cudaStream_t s)
+{
+    PIC_REQUIRE(bits >= 8 && bits <= 16, PIC_ERR_INVALID, "FFT piece width out of range");
+    if (zw == 0) return 0.0;
+    const size_t nlimbs = (zw + 1) / 2;
+    const size_t nctas = (nlimbs + kCvtLPC - 1) / kCvtLPC;
+    DevBuf<uint32_t> agg(nctas, s);
+    DevBuf<unsigned long long> err(1, s);
+    PIC_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(unsigned long long), s));
+    ProfScope ps(KC_CRT, 16.0 * (double)ncoef + 4.0 * (double)zw, s);
+    coefbits_k1<FftCoefLoader><<<(unsigned)nctas, kCvtThreads, 0, s>>>(FftCoefLoader{T, scale}, ncoef, bits, z,
+                                                                        zw, agg.get(), err.get());
+    PIC_CHECK_LAUNCH();
+    count_launch();
+    finish_scan(z, zw, agg.get(), nctas, s);
+    unsigned long long eb = 0;
+    read_words((uint32_t*)&eb, (const uint32_t*)err.get(), 2, s);
+    double e;
+    memcpy(&e, &eb, sizeof e);
+    return e;
+}
+
+// Scale folded into the CRT: R^(depth+1) N^-1 undoes `depth` pointwise
+// Montgomery products (each contributes R^-1) and the unscaled inverse (N).
+static Crt3Consts make_crt3(int k, int depth)
+{
+    Crt3Consts C;
+    const uint64_t N = (uint64_t)1 << k;
+    for (int q = 0; q < 3; q++) {
+        const uint64_t p = kProductPrimes[q];
+        const Mod64 m = make_mod(p);
+        C.p[q] = p;
+        C.pinv[q] = m.pinv_neg;
+        uint64_t sc = host_powmod(N % p, p - 2, p);
+        for (int d = 0; d < depth; d++) sc = to_mont(sc, p);
+        C.scale[q] = to_mont(sc, p);  // mont_mul(y, scale) = y * R^(depth+1) N^-1
+    }
+    const uint64_t p0 = C.p[0], p1 = C.p[1], p2 = C.p[2];
+    C.inv01_m = to_mont(host_powmod(p0 % p1, p1 - 2, p1), p1);
+    C.p0_mod_p2_m = to_mont(p0 % p2, p2);
+    const uint64_t p01m2 = host_mulmod(p0 % p2, p1 % p2, p2);
+    C.inv012_m = to_mont(host_powmod(p01m2, p2 - 2, p2), p2);
+    const unsigned __int128 p01 = (unsigned __int128)p0 * p1;
+    C.p0p1_lo = (uint64_t)p01;
+    C.p0p1_hi = (uint64_t)(p01 >> 64);
+    return C;
+}
+
+static NttBatch ntt3_batch(uint64_t* data, int k)
+{
+    NttBatch bat;
+    bat.data = data;
+    bat.stride = (size_t)1 << k;
+    bat.count = 3;
+    bat.per_prime = 1;
+    for (int q = 0; q < 3; q++) bat.prime[q] = prime_tables(kProductPrimes[q]).dev;
+    return bat;
+}
+
+void ntt3_forward_operand(uint64_t* out, int k, const uint32_t* a, size_t na, cudaStream_t s)
+{
+    const size_t N = (size_t)1 << k;
+    ProfScope ps(KC_SPLIT, 4.0 * (double)na + 24.0 * (double)N, s);
+    split3_kernel<<<grid_for(N, 256), 256, 0, s>>>(out, a, na, N, kProductPrimes[0], kProductPrimes[1],
+                                                   kProductPrimes[2]);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+    ntt_forward_dif(ntt3_batch(out, k), k, s);
+}
+
+void ntt3_pointwise(uint64_t* a, const uint64_t* b, int k, cudaStream_t s)
+{
+    ntt_pointwise_mont(ntt3_batch(a, k), b, k, s);
+}
+
+void ntt3_inverse_to_words(uint64_t* y, int k, size_t ncoef, int depth, uint32_t* z, size_t zw, cudaStream_t s)
+{
+    ntt_inverse_dit(ntt3_batch(y, k), k, s);
+    const Crt3Consts C = make_crt3(k, depth);
+    const size_t nlimbs = (zw + 1) / 2;
+    const size_t nctas = (nlimbs + kCvtLPC - 1) / kCvtLPC;
+    DevBuf<uint32_t> agg(nctas, s);
+    ProfScope ps(KC_CRT, 24.0 * (double)ncoef + 4.0 * (double)zw, s);
+    crt3_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(y, (size_t)1 << k, ncoef, C, z, zw, agg.get());
+    PIC_CHECK_LAUNCH();
+    count_launch();
+    finish_scan(z, zw, agg.get(), nctas, s);
+}
+
+// ---- products ----------------------------------------------------------------
+void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s)
+{
+    const size_t zw = na + nb;
+    const size_t pa = (na + 1) / 2, pb = (nb + 1) / 2;
+    const size_t ncoef = pa + pb - 1;
+    int k = ceil_log2(ncoef);
+    if (k < 1) k = 1;
+    PIC_REQUIRE(k <= 30, PIC_ERR_LENGTH, "product too long for the three-prime NTT (2^30 points)");
+    const size_t N = (size_t)1 << k;
+    const bool square = (a == b && na == nb);
+    DevBuf<uint64_t> A(3 * N, s);
+    DevBuf<uint64_t> B(square ? 0 : 3 * N, s);
+    ntt3_forward_operand(A.get(), k, a, na, s);
+    if (!square) ntt3_forward_operand(B.get(), k, b, nb, s);
+    ntt3_pointwise(A.get(), square ? A.get() : B.get(), k, s);
+    ntt3_inverse_to_words(A.get(), k, ncoef, 1, z, zw, s);
+}
+
+void mul_ntt_ref(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s)
+{
+    const size_t zw = na + nb;
+    int k = ceil_log2(4 * zw);  // BigFloat.cpp:380-385
+    PIC_REQUIRE(k <= 32, PIC_ERR_LENGTH, "product too long for the reference layout");
+    const size_t N = (size_t)1 << k;
+    const uint64_t p = reference_prime(k);
+    const PrimeDev P = prime_tables(p).dev;
+    const bool square = (a == b && na == nb);
+    NttBatch bat;
+    bat.stride = N;
+    bat.count = 1;
+    bat.per_prime = 1;
+    bat.prime[0] = P;
+    DevBuf<uint64_t> A(N, s), B(square ? 0 : N, s);
+    split16_kernel<<<grid_for(N, 256), 256, 0, s>>>(A.get(), N, a, na);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+    bat.data = A.get();
+    ntt_forward_dif(bat, k, s);
+    if (!square) {
+        split16_kernel<<<grid_for(N, 256), 256, 0, s>>>(B.get(), N, b, nb);
+        PIC_CHECK_LAUNCH();
+        count_launch();
+        NttBatch bb = bat;
+        bb.data = B.get();
+        ntt_forward_dif(bb, k, s);
+    }
+    ntt_pointwise_mont(bat, square ? A.get() : B.get(), k, s);
+    ntt_inverse_dit(bat, k, s);
+    const uint64_t ninv = host_powmod(N % p, p - 2, p);
+    coef16_to_words(A.get(), 2 * zw, to_mont(to_mont(ninv, p), p), p, P.pinv_neg, z, zw, s);
+}
+
+// ---- schoolbook ----------------------------------------------------------------
+// One CTA per product.  Phase 1: column sums v_c = sum a_i b_(c-i) as 96-bit
+// (3 words) in shared memory, columns dealt round-robin.  Phase 2: each thread
+// owns kSchWPT consecutive output words: S_w = v_w.0 + v_(w-1).1 + v_(w-2).2.
+constexpr int kSchThreads = 256;
+constexpr int kSchWPT = (int)(kSchoolMaxWords / kSchThreads);
+
+__global__ void __launch_bounds__(kSchThreads) school_kernel(uint32_t* __restrict__ z, const uint32_t* __restrict__ a,
+                                                             uint32_t na, const uint32_t* __restrict__ b, uint32_t nb)
+{
+    extern __shared__ uint32_t sm[];
+    uint32_t* sa = sm;
+    uint32_t* sb = sa + na;
+    uint32_t* col = sb + nb;  // 3 words per column, columns 0 .. na+nb-1
+    const uint32_t zw = na + nb;
+    for (uint32_t i = threadIdx.x; i < na; i += blockDim.x) sa[i] = a[i];
+    for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) sb[i] = b[i];
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < zw; c += blockDim.x) {
+        uint64_t lo = 0;
+        uint32_t hi = 0;
+        const uint32_t i_lo = c + 1 > nb ? c + 1 - nb : 0;
+        const uint32_t i_hi = c < na - 1 ? c : na - 1;
+        for (uint32_t i = i_lo; i <= i_hi && c + 1 < zw + 1; i++) {
+            const uint64_t pr = (uint64_t)sa[i] * sb[c - i];
+            lo += pr;
+            hi += (lo < pr);
+        }
+        if (i_lo > i_hi) { lo = 0; hi = 0; }
+        col[3 * c] = (uint32_t)lo;
+        col[3 * c + 1] = (uint32_t)(lo >> 32);
+        col[3 * c + 2] = hi;
+    }
+    __syncthreads();
+    uint32_t d[kSchWPT], gg[kSchWPT];
+    uint32_t gp = kGPIdentity;
+    const uint32_t w0 = threadIdx.x * kSchWPT;
+#pragma unroll 4
+    for (int u = 0; u < kSchWPT; u++) {
+        const uint32_t w = w0 + u;
+        uint32_t dig = 0, g = 0;
+        if (w < zw) {
+            uint64_t sw = col[3 * w];
+            uint64_t sp = 0;
+            if (w >= 1) { sw += col[3 * (w - 1) + 1]; sp += col[3 * (w - 1)]; }
+            if (w >= 2) { sw += col[3 * (w - 2) + 2]; sp += col[3 * (w - 2) + 1]; }
+            if (w >= 3) sp += col[3 * (w - 3) + 2];
+            const uint64_t t = (sw & 0xffffffffu) + (sp >> 32);
+            dig = (uint32_t)t;
+            g = (uint32_t)(t >> 32);
+        }
+        d[u] = dig;
+        gg[u] = g;
+        gp = gp_combine(gp, g | ((uint32_t)(dig == 0xffffffffu) << 1));
+    }
+    uint32_t total;
+    uint32_t cin = block_gp_scan(gp, &total) & 1u;
+#pragma unroll 4
+    for (int u = 0; u < kSchWPT; u++) {
+        const uint32_t w = w0 + u;
+        if (w < zw) z[w] = d[u] + cin;
+        cin = gg[u] | ((uint32_t)(d[u] == 0xffffffffu) & cin);
+    }
+}
+
+void mul_school(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s)
+{
+    PIC_REQUIRE(na + nb <= kSchoolMaxWords, PIC_ERR_INVALID, "schoolbook product too long");
+    const size_t smem = (na + nb) * 4 + (na + nb) * 12;
+    if (smem > 48 * 1024)
+        PIC_CUDA(cudaFuncSetAttribute(school_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ProfScope ps(KC_SCHOOL, 4.0 * (double)(2 * (na + nb)), s);
+    school_kernel<<<1, kSchThreads, smem, s>>>(z, a, (uint32_t)na, b, (uint32_t)nb);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+}
+
+// ---- dispatch ------------------------------------------------------------------
+int mul_auto_mode(size_t na, size_t nb)
+{
+    const size_t mn = na < nb ? na : nb;
+    if (na + nb <= kSchoolMaxWords && (mn <= 48 || na + nb <= 256)) return PIC_MUL_SCHOOL;
+    return PIC_MUL_NTT3;
+}
+
+static std::atomic<uint64_t> g_fft_err_bits{0};
+double fft_last_max_err()
+{
+    uint64_t b = g_fft_err_bits.load();
+    double d;
+    memcpy(&d, &b, sizeof d);
+    return d;
+}
+void fft_note_max_err(double e)
+{
+    uint64_t b;
+    memcpy(&b, &e, sizeof b);
+    g_fft_err_bits.store(b);
+}
+
+void mul_dispatch(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int mode,
+                  cudaStream_t s)
+{
+    PIC_REQUIRE(na > 0 && nb > 0, PIC_ERR_INVALID, "empty operand");
+    if (mode == PIC_MUL_AUTO) mode = mul_auto_mode(na, nb);
+    switch (mode) {
+    case PIC_MUL_SCHOOL:
+        if (na + nb <= kSchoolMaxWords) {
+            mul_school(z, a, na, b, nb, s);
+            return;
+        }
+        mul_ntt3(z, a, na, b, nb, s);
+        return;
+    case PIC_MUL_NTT_REF: mul_ntt_ref(z, a, na, b, nb, s); return;
+    case PIC_MUL_NTT3: mul_ntt3(z, a, na, b, nb, s); return;
+    case PIC_MUL_FFT: {
+        double e = 0;
+        if (!mul_fft(z, a, na, b, nb, s, &e)) mul_ntt3(z, a, na, b, nb, s);
+        return;
+    }
+    default: throw Error(PIC_ERR_INVALID, "unknown multiply mode");
+    }
+}
+
+void mul_batch(const pic_mul_desc* d, size_t count, int mode, cudaStream_t s)
+{
+    for (size_t i = 0; i < count; i++) {
+        PIC_REQUIRE(d[i].z && d[i].a && d[i].b && d[i].na && d[i].nb, PIC_ERR_INVALID, "bad product descriptor");
+        mul_dispatch(d[i].z, d[i].a, (size_t)d[i].na, d[i].b, (size_t)d[i].nb, mode, s);
+    }
+}
+
+// ---- reference-API conversions ---------------------------------------------------
+void int_to_ntt_dev(uint64_t* T, int k, const uint32_t* A, size_t AL, cudaStream_t s)
+{
+    const size_t N = (size_t)1 << k;
+    PIC_REQUIRE(2 * AL <= N, PIC_ERR_LENGTH, "FFT length is too small.");
+    split16_kernel<<<grid_for(N, 256), 256, 0, s>>>(T, N, A, AL);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+}
+
+void ntt_to_int_dev(const uint64_t* T, int k, uint32_t* A, size_t AL, cudaStream_t s)
+{
+    const size_t N = (size_t)1 << k;
+    PIC_REQUIRE(N >= 2 * AL, PIC_ERR_LENGTH, "FFT length is too small.");  // NTT.cpp:352-353
+    coef16_to_words(T, 2 * AL, 0, 0, 0, A, AL, s);
+}
+
+}  // namespace pic

@@ -1,0 +1,57 @@
+// Exact big-integer products on the device (the inner product of
+// BigFloat::mul, BigFloat.cpp:413-487): z[0 .. na+nb) = a * b.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ntt.cuh"
+#include "piculator_b200.h"
+
+namespace pic {
+
+// Three-prime NTT: 64-bit pieces, primes kProductPrimes, Garner CRT.
+void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s);
+// The reference's own layout: 16-bit points in u64, one prime (the
+// reference's prime for k), length 2^k >= 4 (na + nb) (BigFloat.cpp:380-385).
+void mul_ntt_ref(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s);
+// One CTA per product, column sums in shared memory (na + nb <= kSchoolMax).
+constexpr size_t kSchoolMaxWords = 4096;
+void mul_school(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s);
+// FP64 FFT product; returns false (and leaves z undefined) when the largest
+// rounding distance exceeded 0.25, so the caller can recompute exactly.
+bool mul_fft(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s,
+             double* max_err);
+
+// Three-prime building blocks (also used by transform-domain operands):
+// split + forward into out[3 * 2^k]; pointwise a *= b (adds one R^-1);
+// inverse + CRT + carry of coefficients [0, ncoef) into zw words, undoing
+// `depth` Montgomery factors.
+void ntt3_forward_operand(uint64_t* out, int k, const uint32_t* a, size_t na, cudaStream_t s);
+void ntt3_pointwise(uint64_t* a, const uint64_t* b, int k, cudaStream_t s);
+void ntt3_inverse_to_words(uint64_t* y, int k, size_t ncoef, int depth, uint32_t* z, size_t zw, cudaStream_t s);
+
+void mul_batch(const pic_mul_desc* d, size_t count, int mode, cudaStream_t s);
+
+// Dispatch on mode (PIC_MUL_*).
+void mul_dispatch(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int mode,
+                  cudaStream_t s);
+int mul_auto_mode(size_t na, size_t nb);
+
+// Reference-API conversions (NTT.cpp:330-369).
+void int_to_ntt_dev(uint64_t* T, int k, const uint32_t* A, size_t AL, cudaStream_t s);
+void ntt_to_int_dev(const uint64_t* T, int k, uint32_t* A, size_t AL, cudaStream_t s);
+
+// Coefficients (already reduced, one prime, 16-bit positions) -> words, with
+// optional Montgomery rescale; shared by ntt_to_int_dev and mul_ntt_ref.
+void coef16_to_words(const uint64_t* c, size_t ncoef, uint64_t scale_mont, uint64_t p, uint64_t pinv_neg,
+                     uint32_t* z, size_t zw, cudaStream_t s);
+
+// FFT coefficients (real parts times scale, rounded) at b-bit positions ->
+// words; returns the largest rounding distance seen.  Synchronises.
+double fft_coef_to_words(const double2* T, size_t ncoef, double scale, int bits, uint32_t* z, size_t zw,
+                         cudaStream_t s);
+
+double fft_last_max_err();
+void fft_note_max_err(double e);
+
+}  // namespace pic

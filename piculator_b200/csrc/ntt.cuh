@@ -1,0 +1,88 @@
+// NTT engine: batched power-of-two number-theoretic transforms modulo
+// 64-bit primes (< 2^63) on sm_100a.
+//
+// Forward = decimation in frequency, natural order in, bit-reversed order out.
+// Inverse = decimation in time, bit-reversed in, natural out, unscaled.
+// A convolution therefore never permutes: forward, pointwise, inverse.  The
+// natural-order NTT of the reference (NNT::NTT, NTT.cpp:191-223) is forward +
+// one bit-reversal permutation.
+//
+// Large lengths use the four-/six-step decomposition N = N1 * N2 (* N3):
+// strided "column" passes (a size-N1 DIF over every column of an N1 x M tile,
+// W columns per CTA so every global access is a W*8-byte run, then the
+// inter-step twiddle w_(N1 M)^(col * k1)) and one contiguous "row" pass.  Each
+// pass reads and writes the array once; inside a pass the butterflies run in
+// radix-8 register groups with shared-memory exchanges between groups.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "modarith.cuh"
+
+namespace pic {
+
+constexpr int kInnerBits = 13;  // largest in-CTA sub-transform (2^13 points)
+constexpr int kMaxPrimesPerBatch = 3;
+
+// Device view of one prime's constants and twiddle tables.
+struct PrimeDev {
+    uint64_t p;
+    uint64_t pinv_neg;
+    uint64_t r2;
+    int K;        // outer tables cover roots of order 2^K
+    int S;        // outer split: e = hi * 2^S + lo
+    int IB;       // inner table order bits (min(K, kInnerBits))
+    const uint64_t* inner_fwd;  // (w, w') Shoup pairs, w = root_(2^IB)^i, i < 2^(IB-1)
+    const uint64_t* inner_inv;  // same for root^-1
+    const uint64_t* olo_fwd;    // Montgomery form root_(2^K)^i, i < 2^S
+    const uint64_t* ohi_fwd;    // Montgomery form root_(2^K)^(i 2^S), i < 2^(K-S)
+    const uint64_t* olo_inv;
+    const uint64_t* ohi_inv;
+};
+
+// Host-owned tables for one prime (built once, cached for the process).
+struct PrimeTables {
+    uint64_t p = 0, g = 0;
+    int adicity = 0;
+    PrimeDev dev{};
+};
+
+const PrimeTables& prime_tables(uint64_t p);
+
+// The reference's prime for transform length 2^k (NTT.cpp:125-158).
+uint64_t reference_prime(int k);
+// The reference's generator rule: smallest primitive root (NTT.cpp:104-123).
+uint64_t smallest_generator(uint64_t p);
+
+// The three 62-bit primes of the multi-prime product (c * 2^32 + 1).
+extern const uint64_t kProductPrimes[3];
+
+// A batch of transforms of length 2^k laid out at data + i * stride
+// (i < count); transform i uses prime[i / per_prime].
+struct NttBatch {
+    uint64_t* data;
+    size_t stride;
+    int count;
+    int per_prime;
+    PrimeDev prime[kMaxPrimesPerBatch];
+};
+
+void ntt_forward_dif(const NttBatch& b, int k, cudaStream_t s);
+void ntt_inverse_dit(const NttBatch& b, int k, cudaStream_t s);
+void ntt_bitreverse(const NttBatch& b, int k, cudaStream_t s);
+
+// out[i] = a[i] * b[i] * 2^-64 mod p over every transform of the batch
+// (b may equal a for squaring).
+void ntt_pointwise_mont(const NttBatch& a, const uint64_t* b, int k, cudaStream_t s);
+
+// T[i] = T[i] * A[i] mod p exactly (reference ntt_pointwise semantics).
+void ntt_pointwise_plain(uint64_t* T, const uint64_t* A, int k, const PrimeDev& P, cudaStream_t s);
+// T[i] = T[i] * n^-1 mod p.
+void ntt_scale_ninv(uint64_t* T, int k, const PrimeDev& P, cudaStream_t s);
+
+// Pass split used for length 2^k (for reporting / tests).
+std::vector<int> ntt_pass_bits(int k);
+
+}  // namespace pic

@@ -1,0 +1,205 @@
+// Context, memory and error plumbing (see common.cuh).
+#include <stdio.h>
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace pic {
+
+static Context g_ctx;
+static std::atomic<bool> g_init{false};
+static thread_local std::string t_last_error;
+
+void set_last_error(const std::string& s) { t_last_error = s; }
+const std::string& last_error() { return t_last_error; }
+
+void throw_cuda(cudaError_t e, const char* what, const char* file, int line)
+{
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    if (e == cudaErrorMemoryAllocation) throw Error(PIC_ERR_NO_MEMORY, buf);
+    throw Error(PIC_ERR_CUDA, buf);
+}
+
+Context& ctx() { return g_ctx; }
+bool initialized() { return g_init.load(); }
+
+void require_init()
+{
+    if (!g_init.load()) throw Error(PIC_ERR_NOT_INITIALIZED, "pic_init has not been called");
+}
+
+cudaStream_t resolve(pic_stream s) { return s ? (cudaStream_t)s : g_ctx.stream; }
+
+void init_context(int device)
+{
+    std::lock_guard<std::recursive_mutex> g(g_ctx.lock);
+    if (g_init.load()) {
+        PIC_REQUIRE(device == g_ctx.device, PIC_ERR_INVALID,
+                    "pic_init: library already initialised on another device");
+        return;
+    }
+    int n = 0;
+    PIC_CUDA(cudaGetDeviceCount(&n));
+    PIC_REQUIRE(device >= 0 && device < n, PIC_ERR_INVALID, "pic_init: no such device");
+    PIC_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    PIC_CUDA(cudaGetDeviceProperties(&prop, device));
+    PIC_REQUIRE(prop.major == 10, PIC_ERR_CUDA,
+                "pic_init: this build targets sm_100a (B200); device is " + std::string(prop.name));
+    g_ctx.device = device;
+    g_ctx.num_sms = prop.multiProcessorCount;
+    PIC_CUDA(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
+    cudaMemPool_t pool;
+    PIC_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thr = UINT64_MAX;
+    PIC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    g_ctx.pinned_words_cap = 1 << 16;
+    PIC_CUDA(cudaMallocHost((void**)&g_ctx.pinned_words, g_ctx.pinned_words_cap * sizeof(uint32_t)));
+    g_init.store(true);
+}
+
+void shutdown_context()
+{
+    std::lock_guard<std::recursive_mutex> g(g_ctx.lock);
+    if (!g_init.load()) return;
+    cudaStreamSynchronize(g_ctx.stream);
+    if (g_ctx.pinned_words) cudaFreeHost(g_ctx.pinned_words);
+    g_ctx.pinned_words = nullptr;
+    cudaStreamDestroy(g_ctx.stream);
+    g_ctx.stream = nullptr;
+    g_init.store(false);
+}
+
+void* dev_alloc(size_t bytes, cudaStream_t s)
+{
+    int f = g_ctx.fail_allocs.load();
+    while (f > 0) {
+        if (g_ctx.fail_allocs.compare_exchange_weak(f, f - 1))
+            throw Error(PIC_ERR_NO_MEMORY, "device allocation failed (injected)");
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        char buf[256];
+        snprintf(buf, sizeof buf, "cudaMallocAsync(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+        throw Error(PIC_ERR_NO_MEMORY, buf);
+    }
+    g_ctx.bytes_in_use.fetch_add(bytes);
+    return p;
+}
+
+void dev_free(void* p, size_t bytes, cudaStream_t s)
+{
+    if (!p) return;
+    cudaFreeAsync(p, s);
+    g_ctx.bytes_in_use.fetch_sub(bytes);
+}
+
+void read_words(uint32_t* host, const uint32_t* dev, size_t count, cudaStream_t s)
+{
+    if (count == 0) return;
+    if (count <= g_ctx.pinned_words_cap) {
+        std::lock_guard<std::recursive_mutex> g(g_ctx.lock);
+        PIC_CUDA(cudaMemcpyAsync(g_ctx.pinned_words, dev, count * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, s));
+        PIC_CUDA(cudaStreamSynchronize(s));
+        memcpy(host, g_ctx.pinned_words, count * sizeof(uint32_t));
+    } else {
+        PIC_CUDA(cudaMemcpyAsync(host, dev, count * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        PIC_CUDA(cudaStreamSynchronize(s));
+    }
+}
+
+// ---- live kernel timing ------------------------------------------------------
+namespace {
+struct ProfRec {
+    int cls;
+    double bytes;
+    cudaEvent_t a, b;
+};
+std::mutex g_prof_lock;
+std::atomic<bool> g_prof_on{false};
+std::vector<ProfRec> g_prof;
+std::vector<cudaEvent_t> g_ev_pool;
+cudaEvent_t take_event()
+{
+    if (g_ev_pool.empty()) {
+        cudaEvent_t e;
+        PIC_CUDA(cudaEventCreate(&e));
+        return e;
+    }
+    cudaEvent_t e = g_ev_pool.back();
+    g_ev_pool.pop_back();
+    return e;
+}
+}  // namespace
+
+const char* kernel_class_name(int c)
+{
+    static const char* names[KC_COUNT] = {"ntt_cols", "ntt_rows", "ntt_pointwise", "split", "crt_carry",
+                                          "carry_scan", "linear", "schoolbook", "fft_cols", "fft_rows",
+                                          "bsr_level", "other"};
+    return (c >= 0 && c < KC_COUNT) ? names[c] : "?";
+}
+
+bool profiling() { return g_prof_on.load(std::memory_order_relaxed); }
+
+ProfScope::ProfScope(KernelClass c, double bytes, cudaStream_t st) : s(st)
+{
+    if (!profiling()) return;
+    std::lock_guard<std::mutex> g(g_prof_lock);
+    ProfRec r{(int)c, bytes, take_event(), take_event()};
+    PIC_CUDA(cudaEventRecord(r.a, st));
+    slot = (int)g_prof.size();
+    g_prof.push_back(r);
+}
+
+ProfScope::~ProfScope()
+{
+    if (slot < 0) return;
+    std::lock_guard<std::mutex> g(g_prof_lock);
+    cudaEventRecord(g_prof[slot].b, s);
+}
+
+void profile_begin()
+{
+    std::lock_guard<std::mutex> g(g_prof_lock);
+    for (auto& r : g_prof) {
+        g_ev_pool.push_back(r.a);
+        g_ev_pool.push_back(r.b);
+    }
+    g_prof.clear();
+    g_prof_on.store(true);
+}
+
+int profile_end(pic_kernel_stat* out, int cap)
+{
+    g_prof_on.store(false);
+    std::lock_guard<std::mutex> g(g_prof_lock);
+    pic_kernel_stat acc[KC_COUNT];
+    memset(acc, 0, sizeof acc);
+    for (auto& r : g_prof) {
+        PIC_CUDA(cudaEventSynchronize(r.b));
+        float ms = 0;
+        PIC_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        acc[r.cls].launches++;
+        acc[r.cls].seconds += ms / 1000.0;
+        acc[r.cls].bytes += r.bytes;
+    }
+    int n = 0;
+    for (int c = 0; c < KC_COUNT; c++) {
+        if (!acc[c].launches) continue;
+        if (n < cap) {
+            out[n] = acc[c];
+            snprintf(out[n].name, sizeof out[n].name, "%s", kernel_class_name(c));
+        }
+        n++;
+    }
+    return n;
+}
+
+}  // namespace pic

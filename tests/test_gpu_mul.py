@@ -1,0 +1,131 @@
+"""Whole products (pic_mul / pic_mul_host / pic_mul_batch) vs the oracle,
+Python integers and the reference goldens."""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from oracle.ffi import random_words
+
+pytestmark = pytest.mark.gpu
+
+MODES = ["school", "ntt_ref", "ntt3", "fft", "auto"]
+
+
+def _md5(w):
+    return hashlib.md5(np.ascontiguousarray(w, dtype="<u4").tobytes()).hexdigest()
+
+
+def _int(w):
+    return int.from_bytes(np.ascontiguousarray(w, dtype="<u4").tobytes(), "little")
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("na,nb", [(1, 1), (1, 2), (2, 3), (7, 7), (31, 33), (64, 64), (100, 1),
+                                   (1, 257), (255, 256), (1000, 1000), (1023, 2000), (2047, 2049)])
+def test_products_vs_oracle(pic, oracle, mode, na, nb):
+    a = random_words(na * 7 + nb, na)
+    b = random_words(nb * 13 + na, nb)
+    z = pic.mul_host(a, b, mode)
+    assert np.array_equal(z, oracle.mul_words(a, b))
+
+
+@pytest.mark.parametrize("mode", ["ntt_ref", "ntt3", "fft", "auto"])
+@pytest.mark.parametrize("n", [5000, 1 << 14, 40000, 1 << 17])
+def test_products_vs_python_int(pic, mode, n):
+    a = random_words(n, n)
+    b = random_words(n + 1, n - 3)
+    z = pic.mul_host(a, b, mode)
+    assert _int(z) == _int(a) * _int(b)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_edge_products_golden(pic, golden, mode):
+    for rec in golden["products"]["edge"]:
+        n = rec["n"]
+        ones = np.full(n, 0xFFFFFFFF, dtype=np.uint32)
+        if rec["kind"] == "ones":
+            a, b = ones, ones
+        else:
+            a = np.zeros(n, dtype=np.uint32)
+            a[0] = 1
+            a[-1] = 1
+            b = ones
+        z = pic.mul_host(a, b, mode)
+        L = z.size - (1 if z[-1] == 0 else 0)
+        assert L == rec["L"] and _md5(z[:L]) == rec["md5"]
+
+
+@pytest.mark.parametrize("lg", [12, 16, 20])
+@pytest.mark.parametrize("mode", ["ntt_ref", "ntt3", "fft", "auto"])
+def test_isolated_products_golden(pic, golden, lg, mode):
+    rec = [r for r in golden["products"]["isolated"] if r["log2n"] == lg][0]
+    n = 1 << lg
+    z = pic.mul_host(random_words(42, n), random_words(43, n), mode)
+    L = z.size - (1 if z[-1] == 0 else 0)
+    assert L == rec["L"] and _md5(z[:L]) == rec["md5"]
+
+
+@pytest.mark.parametrize("lg", [22, 24])
+def test_large_products_fingerprint(pic, lg):
+    """Mod-prime fingerprints where Python-int products would be slow:
+    z mod q == (a mod q)(b mod q) mod q for several 61-bit primes, and the
+    NTT forms agree word for word."""
+    n = 1 << lg
+    a, b = random_words(42, n), random_words(43, n)
+    z3 = pic.mul_host(a, b, "ntt3")
+    zr = pic.mul_host(a, b, "ntt_ref")
+    assert np.array_equal(z3, zr)
+    ia, ib, iz = _int(a), _int(b), _int(z3)
+    for q in (2 ** 61 - 1, 2305843009213693921, 1000000007):
+        assert iz % q == (ia % q) * (ib % q) % q
+
+
+def test_all_ones_max_carry_chain(pic):
+    # (B^n - 1)^2 = B^2n - 2 B^n + 1: the longest possible carry chains
+    for n in (3, 4097, 1 << 16, (1 << 18) + 5):
+        ones = np.full(n, 0xFFFFFFFF, dtype=np.uint32)
+        for mode in ("ntt3", "ntt_ref", "fft"):
+            z = pic.mul_host(ones, ones, mode)
+            assert z[0] == 1 and np.all(z[1:n] == 0)
+            assert z[n] == 0xFFFFFFFE and np.all(z[n + 1:] == 0xFFFFFFFF)
+
+
+def test_squaring_same_pointer(pic, torch_cuda, oracle):
+    torch = torch_cuda
+    a = random_words(77, 3000)
+    ta = torch.from_numpy(a.view(np.int32)).cuda()
+    z = torch.zeros(6000, dtype=torch.int32, device="cuda")
+    for mode in ("ntt3", "ntt_ref", "fft", "school"):
+        z.zero_()
+        pic.mul_dev(z.data_ptr(), ta.data_ptr(), 3000, ta.data_ptr(), 3000, mode,
+                    torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert np.array_equal(z.cpu().numpy().view(np.uint32), oracle.mul_words(a, a))
+
+
+def test_mul_batch_uneven(pic, torch_cuda, oracle):
+    torch = torch_cuda
+    rng = np.random.default_rng(7)
+    sizes = [(int(x), int(y)) for x, y in rng.integers(1, 3000, (40, 2))]
+    ops, descs = [], []
+    for i, (na, nb) in enumerate(sizes):
+        a, b = random_words(2 * i, na), random_words(2 * i + 1, nb)
+        ta = torch.from_numpy(a.view(np.int32)).cuda()
+        tb = torch.from_numpy(b.view(np.int32)).cuda()
+        tz = torch.zeros(na + nb, dtype=torch.int32, device="cuda")
+        ops.append((a, b, ta, tb, tz))
+        descs.append((tz.data_ptr(), ta.data_ptr(), na, tb.data_ptr(), nb))
+    pic.mul_batch_dev(descs, "auto", torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    for a, b, _, _, tz in ops:
+        assert np.array_equal(tz.cpu().numpy().view(np.uint32), oracle.mul_words(a, b))
+
+
+def test_fft_error_is_logged(pic):
+    a, b = random_words(1, 1 << 15), random_words(2, 1 << 15)
+    pic.mul_host(a, b, "fft")
+    e = pic.lib().pic_fft_last_max_err()
+    assert 0.0 < e < 0.25

@@ -1,0 +1,33 @@
+"""Whole pi runs: pi.txt byte for byte against the reference's own output."""
+from __future__ import annotations
+
+import hashlib
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("digits", [10_000, 100_000, 1_000_000])
+@pytest.mark.parametrize("form", ["chosen", "plain"])
+def test_pi_matches_reference(pic, golden, digits, form):
+    if form == "plain" and digits > 100_000:
+        pytest.skip("plain form at 1M digits is covered by the benchmark")
+    text, st = pic.pi_hex(digits, pic.PI_CHOSEN if form == "chosen" else pic.PI_PLAIN)
+    g = golden["pi"][str(digits)]
+    assert len(text) == g["bytes"]
+    assert text[:80].decode() == g["head"]
+    assert text[-80:].decode() == g["tail"]
+    assert hashlib.md5(text).hexdigest() == g["md5"]
+    assert st["terms"] > 0 and st["kernel_launches"] > 0
+
+
+@pytest.mark.slow
+def test_pi_10m_matches_reference(pic, golden):
+    text, st = pic.pi_hex(10_000_000, pic.PI_CHOSEN)
+    assert hashlib.md5(text).hexdigest() == golden["pi"]["10000000"]["md5"]
+
+
+def test_pi_oracle_agrees_small(pic, oracle):
+    text, _ = pic.pi_hex(20_000, pic.PI_CHOSEN)
+    assert text == oracle.pi_hex(20_000)
