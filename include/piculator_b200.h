@@ -200,6 +200,21 @@ pic_status pic_pi_hex(uint64_t decimal_digits, int mode, char* out, size_t cap,
 pic_status pic_pi_compute(uint64_t decimal_digits, int mode, pic_bf* out,
                           pic_pi_stats* stats);
 
+/* Binary splitting over [a, b) at precision p (Pi_BSR, PI.h:64-136): the
+ * batched form (PIC_PI_CHOSEN) or the node-by-node recursion (PIC_PI_PLAIN).
+ * Both give the reference's P, Q, R word for word. */
+pic_status pic_bsr(uint32_t a, uint32_t b, size_t p, int mode, pic_bf* P, pic_bf* Q,
+                   pic_bf* R);
+
+/* Tuning knobs (the size-class thresholds the autotuner sets). */
+enum {
+    PIC_TUNE_BSR_SCHOOL_MAX = 0, /* children up to this many words: CTA schoolbook merge */
+    PIC_TUNE_MUL_SCHOOL_MAX = 1, /* products up to this many words: schoolbook in AUTO */
+    PIC_TUNE_MUL_FFT_MAX = 2     /* products up to this many words: FP64 FFT in AUTO (0: never) */
+};
+pic_status pic_set_tuning(int knob, int64_t value);
+int64_t pic_get_tuning(int knob);
+
 /* Sizes Pi() derives from the digit count (PI.h:141-144). */
 pic_status pic_pi_sizes(uint64_t decimal_digits, uint64_t* hex_digits,
                         uint64_t* p_words, uint64_t* terms);

@@ -120,6 +120,10 @@ _SIGS = {
     "pic_transform_free": ([C.c_void_p], C.c_int),
     "pic_pi_hex": ([C.c_uint64, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t),
                     C.POINTER(PiStats)], C.c_int),
+    "pic_bsr": ([C.c_uint32, C.c_uint32, C.c_size_t, C.c_int, C.POINTER(C.c_void_p),
+                 C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)], C.c_int),
+    "pic_set_tuning": ([C.c_int, C.c_int64], C.c_int),
+    "pic_get_tuning": ([C.c_int], C.c_int64),
     "pic_pi_sizes": ([C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                       C.POINTER(C.c_uint64)], C.c_int),
 }
@@ -302,6 +306,24 @@ class Transform:
         out = C.c_void_p()
         check(lib().pic_transform_to_bf(C.byref(out), self.h))
         return DeviceBigFloat(out.value)
+
+
+TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX = range(3)
+
+
+def set_tuning(knob: int, value: int) -> None:
+    check(lib().pic_set_tuning(knob, value))
+
+
+def get_tuning(knob: int) -> int:
+    return int(lib().pic_get_tuning(knob))
+
+
+def bsr(a: int, b: int, p: int, form: int = 0):
+    """Binary splitting over [a, b) at precision p: (P, Q, R) DeviceBigFloats."""
+    hp, hq, hr = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    check(lib().pic_bsr(a, b, p, form, C.byref(hp), C.byref(hq), C.byref(hr)))
+    return DeviceBigFloat(hp.value), DeviceBigFloat(hq.value), DeviceBigFloat(hr.value)
 
 
 # ---- pi ----------------------------------------------------------------------------

@@ -1,12 +1,946 @@
-// Batched binary splitting.
+// Batched Chudnovsky binary splitting (Pi_BSR, PI.h:64-136).
+//
+// The recursion tree splits [a, b) at m = (a + b) / 2, so every node at depth d
+// has length floor(T / 2^d) or ceil(T / 2^d).  Below the depth where a merge
+// could truncate (operands longer than p + 2 words or an add window wider than
+// p + 2, BigFloat.cpp:337-366 and :196-200), every value is an exact integer
+// and every merge is exact arithmetic: P = P0 Q1 + P1 R0, Q = Q0 Q1,
+// R = R0 R1.  Those depths are evaluated level by level, all nodes of a depth
+// in a few launches, with every value resident in HBM in fixed-capacity slots:
+//   * bottom depth (node lengths 1 or 2): one thread per node, leaf formulas
+//     (PI.h:67-88) and the two-leaf merge in registers;
+//   * short children: one CTA per parent, schoolbook column sums and
+//     carry-lookahead scans in shared memory;
+//   * long children: batched three-prime NTT, each child transformed once and
+//     reused by the two products that need it (the transform-domain reuse that
+//     Transform.h was written for), CRT + carry per product, then a batched
+//     signed add for P.
+// The few top levels, where truncation happens, run through BigFloat exactly
+// as the reference does.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "bigfloat.hpp"
 #include "bsr.cuh"
+#include "carry.cuh"
+#include "common.cuh"
+#include "mul.cuh"
+#include "ntt.cuh"
 #include "pi.cuh"
 
 namespace pic {
 
+// ---------------------------------------------------------------------------
+// Per-depth storage.
+struct Slots {
+    size_t count = 0;
+    uint32_t cap = 0;
+    DevBuf<uint32_t> w;    // count x cap words
+    DevBuf<uint32_t> len;  // count lengths (words, no leading zeros)
+};
+
+struct Level {
+    size_t count = 0;
+    Slots P, Q, R;
+    DevBuf<uint8_t> sign;  // P's sign: 1 = positive or zero
+    DevBuf<uint32_t> bnd;  // count + 1 boundaries a_0 < a_1 < ... < a_count = b
+};
+
+static void alloc_slots(Slots& s, size_t count, uint32_t cap, cudaStream_t st)
+{
+    s.count = count;
+    s.cap = cap;
+    s.w = DevBuf<uint32_t>(count * (size_t)cap, st);
+    s.len = DevBuf<uint32_t>(count, st);
+}
+
+// Bits of Q(a,b) for any node of length <= n with b <= T: sum of log2 Q_j
+// (PI.h:77-79), and likewise R (PI.h:81-84); |P| / Q <= sum |P_j| / Q_j
+// <= n (0.09 + 3.6e-6 T) (R_j < Q_j makes the ratio subadditive).
+static void slot_caps(double n, double T, uint32_t& cP, uint32_t& cQ, uint32_t& cR)
+{
+    const double lq = log2(10939058860032000.0) + 3.0 * log2(T + 1.0);
+    const double lr = log2(72.0) + 3.0 * log2(T + 1.0);
+    const double bq = n * lq, br = n * lr;
+    const double bp = bq + log2(n * (0.0895 + 3.6e-6 * T) + 1.0) + 1.0;
+    cQ = (uint32_t)ceil(bq / 32.0) + 2;
+    cR = (uint32_t)ceil(br / 32.0) + 2;
+    cP = (uint32_t)ceil(bp / 32.0) + 2;
+}
+
+// ---------------------------------------------------------------------------
+// Boundaries: child 2i = [a, m), child 2i+1 = [m, b), m = (a + b) / 2 (PI.h:90).
+__global__ void split_bounds_kernel(const uint32_t* __restrict__ pb, size_t count, uint32_t* __restrict__ cb)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t a = pb[i], b = pb[i + 1];
+        cb[2 * i] = a;
+        cb[2 * i + 1] = (uint32_t)((a + b) / 2);
+        if (i == count - 1) cb[2 * count] = b;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Small fixed-size multiword helpers (registers).
+template <int N>
+struct SW {
+    uint32_t w[N];
+    int n;  // used words, canonical (top nonzero) or 0
+};
+
+template <int N>
+__device__ __forceinline__ void sw_set(SW<N>& x, uint64_t v)
+{
+#pragma unroll
+    for (int i = 0; i < N; i++) x.w[i] = 0;
+    x.w[0] = (uint32_t)v;
+    if (N > 1) x.w[1] = (uint32_t)(v >> 32);
+    x.n = (v >> 32) ? 2 : (v ? 1 : 0);
+}
+
+// x *= m (m a 32-bit word), the reference's mul(uint32_t) (BigFloat.cpp:156-183).
+template <int N>
+__device__ __forceinline__ void sw_mul_u32(SW<N>& x, uint32_t m)
+{
+    uint64_t carry = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        if (i < x.n) {
+            carry += (uint64_t)x.w[i] * m;
+            x.w[i] = (uint32_t)carry;
+            carry >>= 32;
+        }
+    }
+    if (carry && x.n < N) x.w[x.n++] = (uint32_t)carry;
+}
+
+template <int NA, int NB, int NZ>
+__device__ __forceinline__ void sw_mul(const SW<NA>& a, const SW<NB>& b, SW<NZ>& z)
+{
+#pragma unroll
+    for (int i = 0; i < NZ; i++) z.w[i] = 0;
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+        if (i >= a.n) continue;
+        uint64_t carry = 0;
+#pragma unroll
+        for (int j = 0; j < NB; j++) {
+            if (j >= b.n) continue;
+            carry += (uint64_t)a.w[i] * b.w[j] + z.w[i + j];
+            z.w[i + j] = (uint32_t)carry;
+            carry >>= 32;
+        }
+        if (i + b.n < NZ) z.w[i + b.n] = (uint32_t)carry;
+    }
+    int n = (a.n && b.n) ? a.n + b.n : 0;
+    if (n > NZ) n = NZ;
+    while (n > 0 && z.w[n - 1] == 0) n--;
+    z.n = n;
+}
+
+template <int N>
+__device__ __forceinline__ int sw_cmp(const SW<N>& a, const SW<N>& b)
+{
+    for (int i = N - 1; i >= 0; i--) {
+        if (a.w[i] != b.w[i]) return a.w[i] < b.w[i] ? -1 : 1;
+    }
+    return 0;
+}
+
+// Signed sum: (sa, a) + (sb, b) -> (sz, z), the reference's add with
+// sign dispatch (BigFloat.cpp:288-305) on exact integers.
+template <int N>
+__device__ __forceinline__ void sw_signed_add(bool sa, const SW<N>& a, bool sb, const SW<N>& b, bool& sz, SW<N>& z)
+{
+    if (sa == sb) {
+        uint64_t c = 0;
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            c += (uint64_t)a.w[i] + b.w[i];
+            z.w[i] = (uint32_t)c;
+            c >>= 32;
+        }
+        sz = sa;
+    } else {
+        const int c = sw_cmp(a, b);
+        const SW<N>& big = c >= 0 ? a : b;
+        const SW<N>& sml = c >= 0 ? b : a;
+        uint32_t br = 0;
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            const uint64_t d = (uint64_t)big.w[i] - sml.w[i] - br;
+            z.w[i] = (uint32_t)d;
+            br = (uint32_t)(d >> 63);
+        }
+        sz = c > 0 ? sa : (c < 0 ? sb : true);
+    }
+    int n = N;
+    while (n > 0 && z.w[n - 1] == 0) n--;
+    z.n = n;
+    if (n == 0) sz = true;
+}
+
+// Leaf b (PI.h:67-88).
+struct LeafV {
+    SW<6> P;
+    bool sP;
+    SW<5> Q;
+    SW<4> R;
+};
+
+__device__ __forceinline__ void leaf(uint32_t b, LeafV& v)
+{
+    sw_set(v.P, (uint64_t)b * 545140134ull + 13591409ull);
+    sw_mul_u32(v.P, 2 * b - 1);
+    sw_mul_u32(v.P, 6 * b - 5);
+    sw_mul_u32(v.P, 6 * b - 1);
+    v.sP = (b % 2) == 0;
+    sw_set(v.Q, b);
+    sw_mul_u32(v.Q, b);
+    sw_mul_u32(v.Q, b);
+    sw_mul_u32(v.Q, 26726400u);
+    sw_mul_u32(v.Q, 409297880u);
+    sw_set(v.R, 2 * b - 1);
+    sw_mul_u32(v.R, 6 * b - 5);
+    sw_mul_u32(v.R, 6 * b - 1);
+}
+
+template <int N>
+__device__ __forceinline__ void store_sw(const SW<N>& x, uint32_t* slot, uint32_t cap, uint32_t* len)
+{
+    for (int i = 0; i < (int)cap && i < N; i++) slot[i] = x.w[i];
+    *len = (uint32_t)x.n;
+}
+
+// Bottom depth: nodes of length 1 (a leaf) or 2 (two leaves merged).
+__global__ void bottom_kernel(const uint32_t* __restrict__ bnd, size_t count,
+                              uint32_t* Pw, uint32_t* Plen, uint8_t* Psign, uint32_t cP, uint32_t* Qw,
+                              uint32_t* Qlen, uint32_t cQ, uint32_t* Rw, uint32_t* Rlen, uint32_t cR)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t a = bnd[i], b = bnd[i + 1];
+        if (b - a == 1) {
+            LeafV v;
+            leaf(b, v);
+            store_sw(v.P, Pw + i * cP, cP, Plen + i);
+            Psign[i] = v.sP ? 1 : 0;
+            store_sw(v.Q, Qw + i * cQ, cQ, Qlen + i);
+            store_sw(v.R, Rw + i * cR, cR, Rlen + i);
+        } else {
+            LeafV l, r;
+            leaf(a + 1, l);
+            leaf(a + 2, r);
+            SW<12> t1, t2, P;
+            sw_mul(l.P, r.Q, t1);  // P0 Q1
+            sw_mul(r.P, l.R, t2);  // P1 R0
+            bool sP;
+            sw_signed_add(l.sP, t1, r.sP, t2, sP, P);
+            SW<10> Q;
+            SW<8> R;
+            sw_mul(l.Q, r.Q, Q);
+            sw_mul(l.R, r.R, R);
+            store_sw(P, Pw + i * cP, cP, Plen + i);
+            Psign[i] = sP ? 1 : 0;
+            store_sw(Q, Qw + i * cQ, cQ, Qlen + i);
+            store_sw(R, Rw + i * cR, cR, Rlen + i);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CTA-per-parent schoolbook merge.
+//
+// Shared-memory helpers; every thread of the block must call them.
+
+// z[0..na+nb) = a * b; col must hold 3 (na + nb) words.  Returns the length
+// without leading zeros (0 if either operand is empty).
+__device__ uint32_t cta_mul(const uint32_t* a, uint32_t na, const uint32_t* b, uint32_t nb, uint32_t* z,
+                            uint32_t* col)
+{
+    if (na == 0 || nb == 0) {
+        __syncthreads();
+        return 0;
+    }
+    const uint32_t zw = na + nb;
+    for (uint32_t c = threadIdx.x; c < zw; c += blockDim.x) {
+        uint64_t lo = 0;
+        uint32_t hi = 0;
+        if (c + 1 < zw) {
+            const uint32_t i_lo = c + 1 > nb ? c + 1 - nb : 0;
+            const uint32_t i_hi = c < na - 1 ? c : na - 1;
+            for (uint32_t i = i_lo; i <= i_hi; i++) {
+                const uint64_t pr = (uint64_t)a[i] * b[c - i];
+                lo += pr;
+                hi += (lo < pr);
+            }
+        }
+        col[3 * c] = (uint32_t)lo;
+        col[3 * c + 1] = (uint32_t)(lo >> 32);
+        col[3 * c + 2] = hi;
+    }
+    __syncthreads();
+    // each thread owns a contiguous run of output words
+    const uint32_t per = (zw + blockDim.x - 1) / blockDim.x;
+    const uint32_t w0 = threadIdx.x * per, w1 = min(w0 + per, zw);
+    auto digit = [&](uint32_t w, uint32_t& g) -> uint32_t {
+        uint64_t sw = col[3 * w], sp = 0;
+        if (w >= 1) {
+            sw += col[3 * (w - 1) + 1];
+            sp += col[3 * (w - 1)];
+        }
+        if (w >= 2) {
+            sw += col[3 * (w - 2) + 2];
+            sp += col[3 * (w - 2) + 1];
+        }
+        if (w >= 3) sp += col[3 * (w - 3) + 2];
+        const uint64_t t = (sw & 0xffffffffu) + (sp >> 32);
+        g = (uint32_t)(t >> 32);
+        return (uint32_t)t;
+    };
+    uint32_t gp = kGPIdentity;
+    for (uint32_t w = w0; w < w1; w++) {
+        uint32_t g;
+        const uint32_t d = digit(w, g);
+        gp = gp_combine(gp, g | ((uint32_t)(d == 0xffffffffu) << 1));
+    }
+    uint32_t total;
+    uint32_t cin = block_gp_scan(gp, &total) & 1u;
+    for (uint32_t w = w0; w < w1; w++) {
+        uint32_t g;
+        const uint32_t d = digit(w, g);
+        z[w] = d + cin;
+        cin = g | ((uint32_t)(d == 0xffffffffu) & cin);
+    }
+    __syncthreads();
+    return z[zw - 1] == 0 ? zw - 1 : zw;
+}
+
+// Highest index < n with x[i] != 0, plus one (0 if none).
+__device__ uint32_t cta_top(const uint32_t* x, uint32_t n)
+{
+    __shared__ uint32_t s_top;
+    if (threadIdx.x == 0) s_top = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        if (x[i] != 0) atomicMax(&s_top, i + 1);
+    __syncthreads();
+    const uint32_t r = s_top;
+    __syncthreads();
+    return r;
+}
+
+// Signed sum of magnitudes (sa, a[0..na)) + (sb, b[0..nb)) into z (capacity
+// max(na, nb) + 1).  Returns the length; *sz the sign.  Exact arithmetic
+// with the reference's sign dispatch (BigFloat.cpp:288-305).
+__device__ uint32_t cta_signed_add(bool sa, const uint32_t* a, uint32_t na, bool sb, const uint32_t* b, uint32_t nb,
+                                   uint32_t* z, bool* sz)
+{
+    __shared__ int s_cmp;
+    const uint32_t n = max(na, nb);
+    auto A = [&](uint32_t i) -> uint32_t { return i < na ? a[i] : 0u; };
+    auto B = [&](uint32_t i) -> uint32_t { return i < nb ? b[i] : 0u; };
+    bool sub = sa != sb;
+    bool swap = false;
+    if (sub) {
+        // compare magnitudes: highest differing word decides
+        __shared__ uint32_t s_hi;
+        if (threadIdx.x == 0) s_hi = 0;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+            if (A(i) != B(i)) atomicMax(&s_hi, i + 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint32_t h = s_hi;
+            s_cmp = h == 0 ? 0 : (A(h - 1) > B(h - 1) ? 1 : -1);
+        }
+        __syncthreads();
+        const int c = s_cmp;
+        __syncthreads();
+        if (c == 0) {
+            *sz = true;
+            return 0;
+        }
+        swap = c < 0;
+    }
+    const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+    const uint32_t w0 = threadIdx.x * per, w1 = min(w0 + per, n);
+    uint32_t gp = kGPIdentity;
+    for (uint32_t i = w0; i < w1; i++) {
+        const uint32_t x = swap ? B(i) : A(i), y = swap ? A(i) : B(i);
+        uint32_t d, g, p;
+        if (!sub) {
+            const uint64_t s = (uint64_t)x + y;
+            d = (uint32_t)s;
+            g = (uint32_t)(s >> 32);
+            p = d == 0xffffffffu;
+        } else {
+            d = x - y;
+            g = x < y;
+            p = d == 0u;
+        }
+        gp = gp_combine(gp, g | (p << 1));
+    }
+    uint32_t total;
+    uint32_t cin = block_gp_scan(gp, &total) & 1u;
+    for (uint32_t i = w0; i < w1; i++) {
+        const uint32_t x = swap ? B(i) : A(i), y = swap ? A(i) : B(i);
+        if (!sub) {
+            const uint64_t s = (uint64_t)x + y;
+            const uint32_t d = (uint32_t)s;
+            z[i] = d + cin;
+            cin = (uint32_t)(s >> 32) | ((uint32_t)(d == 0xffffffffu) & cin);
+        } else {
+            const uint32_t d = x - y;
+            z[i] = d - cin;
+            cin = (uint32_t)(x < y) | ((uint32_t)(d == 0u) & cin);
+        }
+    }
+    __syncthreads();
+    uint32_t len;
+    if (!sub) {
+        if (threadIdx.x == 0) z[n] = total & 1u;
+        __syncthreads();
+        len = z[n] ? n + 1 : n;
+        *sz = sa;
+    } else {
+        len = cta_top(z, n);
+        *sz = swap ? sb : sa;
+        if (len == 0) *sz = true;
+    }
+    __syncthreads();
+    return len;
+}
+
+struct MergeArgs {
+    // children (depth d + 1)
+    const uint32_t *cPw, *cQw, *cRw, *cPl, *cQl, *cRl;
+    const uint8_t* cS;
+    uint32_t ccP, ccQ, ccR;
+    // parents (depth d)
+    uint32_t *pPw, *pQw, *pRw, *pPl, *pQl, *pRl;
+    uint8_t* pS;
+    uint32_t pcP, pcQ, pcR;
+    size_t count;  // parents
+};
+
+__global__ void __launch_bounds__(256) merge_school_kernel(MergeArgs m)
+{
+    extern __shared__ uint32_t sm[];
+    const size_t i = blockIdx.x;
+    const size_t L = 2 * i, R = 2 * i + 1;
+    const uint32_t nPL = m.cPl[L], nQL = m.cQl[L], nRL = m.cRl[L];
+    const uint32_t nPR = m.cPl[R], nQR = m.cQl[R], nRR = m.cRl[R];
+    const bool sL = m.cS[L] != 0, sR = m.cS[R] != 0;
+    uint32_t* PL = sm;
+    uint32_t* QL = PL + m.ccP;
+    uint32_t* RL = QL + m.ccQ;
+    uint32_t* PR = RL + m.ccR;
+    uint32_t* QR = PR + m.ccP;
+    uint32_t* RR = QR + m.ccQ;
+    uint32_t* t1 = RR + m.ccR;         // ccP + ccQ
+    uint32_t* t2 = t1 + m.ccP + m.ccQ; // ccP + ccR
+    uint32_t* col = t2 + m.ccP + m.ccR;  // 3 (ccP + ccQ) (the largest product)
+    for (uint32_t k = threadIdx.x; k < nPL; k += blockDim.x) PL[k] = m.cPw[L * m.ccP + k];
+    for (uint32_t k = threadIdx.x; k < nQL; k += blockDim.x) QL[k] = m.cQw[L * m.ccQ + k];
+    for (uint32_t k = threadIdx.x; k < nRL; k += blockDim.x) RL[k] = m.cRw[L * m.ccR + k];
+    for (uint32_t k = threadIdx.x; k < nPR; k += blockDim.x) PR[k] = m.cPw[R * m.ccP + k];
+    for (uint32_t k = threadIdx.x; k < nQR; k += blockDim.x) QR[k] = m.cQw[R * m.ccQ + k];
+    for (uint32_t k = threadIdx.x; k < nRR; k += blockDim.x) RR[k] = m.cRw[R * m.ccR + k];
+    __syncthreads();
+    // Q = QL QR, R = RL RR written straight to the parent slots via t1 staging
+    uint32_t nQ = cta_mul(QL, nQL, QR, nQR, t1, col);
+    for (uint32_t k = threadIdx.x; k < nQ; k += blockDim.x) m.pQw[i * m.pcQ + k] = t1[k];
+    uint32_t nR = cta_mul(RL, nRL, RR, nRR, t1, col);
+    for (uint32_t k = threadIdx.x; k < nR; k += blockDim.x) m.pRw[i * m.pcR + k] = t1[k];
+    __syncthreads();
+    // P = PL QR + PR RL (PI.h:110)
+    const uint32_t n1 = cta_mul(PL, nPL, QR, nQR, t1, col);
+    const uint32_t n2 = cta_mul(PR, nPR, RL, nRL, t2, col);
+    bool sP;
+    uint32_t* pz = col;  // reuse: max(n1, n2) + 1 <= 3 (ccP + ccQ)
+    const uint32_t nP = cta_signed_add(sL, t1, n1, sR, t2, n2, pz, &sP);
+    for (uint32_t k = threadIdx.x; k < nP; k += blockDim.x) m.pPw[i * m.pcP + k] = pz[k];
+    if (threadIdx.x == 0) {
+        m.pPl[i] = nP;
+        m.pQl[i] = nQ;
+        m.pRl[i] = nR;
+        m.pS[i] = sP ? 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Batched three-prime NTT merge.
+
+// Child slot -> residues: out[(q * n2 + c) * N + j] = piece j of child c0 + c.
+__global__ void slot_split_kernel(uint64_t* __restrict__ out, const uint32_t* __restrict__ w,
+                                  const uint32_t* __restrict__ len, uint32_t cap, size_t c0, size_t n2, int k,
+                                  uint64_t p0, uint64_t p1, uint64_t p2)
+{
+    const size_t N = (size_t)1 << k;
+    const size_t total = n2 * N;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
+        const size_t c = g >> k, j = g & (N - 1);
+        const uint32_t n = len[c0 + c];
+        const uint32_t* x = w + (c0 + c) * (size_t)cap;
+        uint64_t v = 0;
+        if (2 * j < n) {
+            v = x[2 * j];
+            if (2 * j + 1 < n) v |= (uint64_t)x[2 * j + 1] << 32;
+        }
+        uint64_t r0 = v, r1 = v, r2 = v;
+        while (r0 >= p0) r0 -= p0;
+        while (r1 >= p1) r1 -= p1;
+        while (r2 >= p2) r2 -= p2;
+        out[(0 * n2 + c) * N + j] = r0;
+        out[(1 * n2 + c) * N + j] = r1;
+        out[(2 * n2 + c) * N + j] = r2;
+    }
+}
+
+// For every parent i and prime q (arrays laid out [q][child][N]):
+//   T1 = PL QR -> P[2i], T2 = PR RL -> P[2i+1], Q = QL QR -> Q[2i], R = RL RR -> R[2i]
+__global__ void merge_pointwise_kernel(uint64_t* __restrict__ P, uint64_t* __restrict__ Q, uint64_t* __restrict__ R,
+                                       size_t npar, int k, Mod64 m0, Mod64 m1, Mod64 m2)
+{
+    const size_t N = (size_t)1 << k;
+    const size_t total = 3 * npar * N;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
+        const size_t q = g / (npar * N);
+        const size_t r = g - q * npar * N;
+        const size_t i = r >> k, j = r & (N - 1);
+        const Mod64& M = q == 0 ? m0 : (q == 1 ? m1 : m2);
+        const size_t base = q * 2 * npar;
+        const size_t L = (base + 2 * i) * N + j, Rr = (base + 2 * i + 1) * N + j;
+        const uint64_t pl = P[L], pr = P[Rr], ql = Q[L], qr = Q[Rr], rl = R[L], rr = R[Rr];
+        P[L] = mont_mul(pl, qr, M);
+        P[Rr] = mont_mul(pr, rl, M);
+        Q[L] = mont_mul(ql, qr, M);
+        R[L] = mont_mul(rl, rr, M);
+    }
+}
+
+// Product lengths: z = a b with na, nb from the children; 0 if either is 0.
+__global__ void product_len_kernel(const uint32_t* la, const uint32_t* lb, size_t c0, size_t npar, int a_off,
+                                   int b_off, uint32_t* zl)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < npar; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t na = la[2 * (c0 + i) + a_off], nb = lb[2 * (c0 + i) + b_off];
+        zl[i] = (na && nb) ? na + nb : 0;
+    }
+}
+
+__global__ void fix_top_kernel(const uint32_t* w, uint32_t cap, uint32_t* len, size_t n)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t l = len[i];
+        if (l && w[i * (size_t)cap + l - 1] == 0) len[i] = l - 1;
+    }
+}
+
+// CTA per parent: P = sL T1 + sR T2 over long operands, processed in chunks
+// of blockDim * 8 words with the carry carried between chunks.
+__global__ void __launch_bounds__(256) signed_add_kernel(const uint32_t* __restrict__ t1, const uint32_t* l1,
+                                                         uint32_t c1, const uint32_t* __restrict__ t2,
+                                                         const uint32_t* l2, uint32_t c2, const uint8_t* cS,
+                                                         size_t c0, uint32_t* __restrict__ Pw, uint32_t* Pl,
+                                                         uint8_t* Ps, uint32_t cP)
+{
+    const size_t i = blockIdx.x;
+    const uint32_t na = l1[i], nb = l2[i];
+    const bool sa = cS[2 * (c0 + i)] != 0, sb = cS[2 * (c0 + i) + 1] != 0;
+    const uint32_t* a = t1 + i * (size_t)c1;
+    const uint32_t* b = t2 + i * (size_t)c2;
+    uint32_t* z = Pw + (c0 + i) * (size_t)cP;
+    const uint32_t n = max(na, nb);
+    auto A = [&](uint32_t k) -> uint32_t { return k < na ? a[k] : 0u; };
+    auto B = [&](uint32_t k) -> uint32_t { return k < nb ? b[k] : 0u; };
+    const bool sub = sa != sb;
+    bool swap = false;
+    __shared__ uint32_t s_hi;
+    __shared__ uint32_t s_carry;
+    if (sub) {
+        if (threadIdx.x == 0) s_hi = 0;
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < n; k += blockDim.x)
+            if (A(k) != B(k)) atomicMax(&s_hi, k + 1);
+        __syncthreads();
+        const uint32_t h = s_hi;
+        if (h == 0) {
+            if (threadIdx.x == 0) {
+                Pl[c0 + i] = 0;
+                Ps[c0 + i] = 1;
+            }
+            return;
+        }
+        swap = A(h - 1) < B(h - 1);
+    }
+    constexpr int IPT = 8;
+    const uint32_t chunk = blockDim.x * IPT;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n; base += chunk) {
+        const uint32_t cin_chunk = s_carry;
+        const uint32_t w0 = base + threadIdx.x * IPT;
+        uint32_t gp = kGPIdentity;
+#pragma unroll
+        for (int u = 0; u < IPT; u++) {
+            const uint32_t k = w0 + u;
+            uint32_t d = 0, g = 0, p = 1;
+            if (k < n) {
+                const uint32_t x = swap ? B(k) : A(k), y = swap ? A(k) : B(k);
+                if (!sub) {
+                    const uint64_t s = (uint64_t)x + y;
+                    d = (uint32_t)s;
+                    g = (uint32_t)(s >> 32);
+                    p = d == 0xffffffffu;
+                } else {
+                    d = x - y;
+                    g = x < y;
+                    p = d == 0u;
+                }
+            }
+            gp = gp_combine(gp, g | (p << 1));
+        }
+        uint32_t total;
+        const uint32_t pre = block_gp_scan(gp, &total);
+        uint32_t cin = (pre & 1u) | (((pre >> 1) & 1u) & cin_chunk);
+#pragma unroll
+        for (int u = 0; u < IPT; u++) {
+            const uint32_t k = w0 + u;
+            if (k >= n) break;
+            const uint32_t x = swap ? B(k) : A(k), y = swap ? A(k) : B(k);
+            if (!sub) {
+                const uint64_t s = (uint64_t)x + y;
+                const uint32_t d = (uint32_t)s;
+                z[k] = d + cin;
+                cin = (uint32_t)(s >> 32) | ((uint32_t)(d == 0xffffffffu) & cin);
+            } else {
+                const uint32_t d = x - y;
+                z[k] = d - cin;
+                cin = (uint32_t)(x < y) | ((uint32_t)(d == 0u) & cin);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry = (total & 1u) | (((total >> 1) & 1u) & cin_chunk);
+        __syncthreads();
+    }
+    if (!sub) {
+        if (threadIdx.x == 0) {
+            const uint32_t c = s_carry;
+            if (c) z[n] = 1;
+            Pl[c0 + i] = n + (c ? 1 : 0);
+            Ps[c0 + i] = sa ? 1 : 0;
+        }
+        return;
+    }
+    // strip leading zeros after a subtraction
+    if (threadIdx.x == 0) s_hi = 0;
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x)
+        if (z[k] != 0) atomicMax(&s_hi, k + 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t l = s_hi;
+        Pl[c0 + i] = l;
+        Ps[c0 + i] = l == 0 ? 1 : ((swap ? sb : sa) ? 1 : 0);
+    }
+}
+
+static inline int ceil_log2_sz(size_t n)
+{
+    int k = 0;
+    while (((size_t)1 << k) < n) k++;
+    return k;
+}
+
+// The three primes' constants for the pointwise kernel.
+static Mod64 prime_mod(int q) { return make_mod(kProductPrimes[q]); }
+
+static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
+{
+    const uint32_t ccP = ch.P.cap, ccQ = ch.Q.cap, ccR = ch.R.cap;
+    const uint32_t cmax = std::max(ccP, std::max(ccQ, ccR));
+    // 64-bit pieces: a product of two <= cmax-word operands has <= cmax pieces
+    int k = ceil_log2_sz(cmax);
+    if (k < 1) k = 1;
+    PIC_REQUIRE(k <= 30, PIC_ERR_LENGTH, "binary-splitting node too long for the three-prime NTT");
+    const size_t N = (size_t)1 << k;
+    // bytes per parent: three child arrays (P, Q, R of both children) x 3 primes,
+    // plus the two word buffers for P's partial products
+    const size_t per_parent = 3 * 2 * 3 * N * sizeof(uint64_t) + 4 * (size_t)(2 * ccP + ccQ + ccR);
+    size_t chunk = mem_budget / per_parent;
+    if (chunk < 1) chunk = 1;
+    if (chunk > par.count) chunk = par.count;
+    const uint64_t P0 = kProductPrimes[0], P1 = kProductPrimes[1], P2 = kProductPrimes[2];
+    const Mod64 m0 = prime_mod(0), m1 = prime_mod(1), m2 = prime_mod(2);
+    const uint32_t c1 = ccP + ccQ, c2 = ccP + ccR;
+    for (size_t p0 = 0; p0 < par.count; p0 += chunk) {
+        const size_t np = std::min(chunk, par.count - p0);
+        const size_t nc = 2 * np, c0 = 2 * p0;
+        DevBuf<uint64_t> bP(3 * nc * N, s), bQ(3 * nc * N, s), bR(3 * nc * N, s);
+        const size_t tot = nc * N;
+        slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bP.get(), ch.P.w.get(), ch.P.len.get(), ccP, c0, nc, k,
+                                                             P0, P1, P2);
+        slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bQ.get(), ch.Q.w.get(), ch.Q.len.get(), ccQ, c0, nc, k,
+                                                             P0, P1, P2);
+        slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bR.get(), ch.R.w.get(), ch.R.len.get(), ccR, c0, nc, k,
+                                                             P0, P1, P2);
+        PIC_CHECK_LAUNCH();
+        count_launch(3);
+        NttBatch fb;
+        fb.stride = N;
+        fb.count = (int)(3 * nc);
+        fb.per_prime = (int)nc;
+        for (int q = 0; q < 3; q++) fb.prime[q] = prime_tables(kProductPrimes[q]).dev;
+        fb.data = bP.get();
+        ntt_forward_dif(fb, k, s);
+        fb.data = bQ.get();
+        ntt_forward_dif(fb, k, s);
+        fb.data = bR.get();
+        ntt_forward_dif(fb, k, s);
+        {
+            ProfScope ps(KC_NTT_POINTWISE, 3.0 * 3 * np * N * 80.0 / 8.0, s);
+            merge_pointwise_kernel<<<grid_for(3 * np * N, 256), 256, 0, s>>>(bP.get(), bQ.get(), bR.get(), np, k, m0,
+                                                                           m1, m2);
+            PIC_CHECK_LAUNCH();
+            count_launch();
+        }
+        // inverses: P holds T1, T2 for every parent (all items); Q, R the even items
+        NttBatch ib = fb;
+        ib.data = bP.get();
+        ntt_inverse_dit(ib, k, s);
+        NttBatch eb = fb;
+        eb.stride = 2 * N;
+        eb.count = (int)(3 * np);
+        eb.per_prime = (int)np;
+        eb.data = bQ.get();
+        ntt_inverse_dit(eb, k, s);
+        eb.data = bR.get();
+        ntt_inverse_dit(eb, k, s);
+        // CRT + carry into words
+        DevBuf<uint32_t> T1(np * c1, s), T2(np * c2, s), l1(np, s), l2(np, s);
+        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.Q.len.get(), p0, np, 0, 1, l1.get());
+        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.R.len.get(), p0, np, 1, 0, l2.get());
+        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.Q.len.get(), ch.Q.len.get(), p0, np, 0, 1,
+                                                             par.Q.len.get() + p0);
+        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.R.len.get(), ch.R.len.get(), p0, np, 0, 1,
+                                                             par.R.len.get() + p0);
+        PIC_CHECK_LAUNCH();
+        count_launch(4);
+        // T1: residues at bP items 2i (stride 2N), T2 at items 2i+1
+        const size_t pstride = nc * N;  // [prime][child][N]
+        ntt3_batch_to_words(bP.get(), 2 * N, pstride, np, k, T1.get(), c1, l1.get(), s);
+        ntt3_batch_to_words(bP.get() + N, 2 * N, pstride, np, k, T2.get(), c2, l2.get(), s);
+        ntt3_batch_to_words(bQ.get(), 2 * N, pstride, np, k, par.Q.w.get() + p0 * par.Q.cap, par.Q.cap,
+                            par.Q.len.get() + p0, s);
+        ntt3_batch_to_words(bR.get(), 2 * N, pstride, np, k, par.R.w.get() + p0 * par.R.cap, par.R.cap,
+                            par.R.len.get() + p0, s);
+        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(T1.get(), c1, l1.get(), np);
+        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(T2.get(), c2, l2.get(), np);
+        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(par.Q.w.get() + p0 * par.Q.cap, par.Q.cap,
+                                                         par.Q.len.get() + p0, np);
+        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(par.R.w.get() + p0 * par.R.cap, par.R.cap,
+                                                         par.R.len.get() + p0, np);
+        PIC_CHECK_LAUNCH();
+        count_launch(4);
+        {
+            ProfScope ps(KC_LINEAR, 12.0 * (double)np * (double)c1, s);
+            signed_add_kernel<<<(unsigned)np, 256, 0, s>>>(T1.get(), l1.get(), c1, T2.get(), l2.get(), c2,
+                                                          ch.sign.get(), p0, par.P.w.get(), par.P.len.get(),
+                                                          par.sign.get(), par.P.cap);
+            PIC_CHECK_LAUNCH();
+            count_launch();
+        }
+    }
+}
+
+static void merge_school(Level& ch, Level& par, cudaStream_t s)
+{
+    MergeArgs m;
+    m.cPw = ch.P.w.get();
+    m.cQw = ch.Q.w.get();
+    m.cRw = ch.R.w.get();
+    m.cPl = ch.P.len.get();
+    m.cQl = ch.Q.len.get();
+    m.cRl = ch.R.len.get();
+    m.cS = ch.sign.get();
+    m.ccP = ch.P.cap;
+    m.ccQ = ch.Q.cap;
+    m.ccR = ch.R.cap;
+    m.pPw = par.P.w.get();
+    m.pQw = par.Q.w.get();
+    m.pRw = par.R.w.get();
+    m.pPl = par.P.len.get();
+    m.pQl = par.Q.len.get();
+    m.pRl = par.R.len.get();
+    m.pS = par.sign.get();
+    m.pcP = par.P.cap;
+    m.pcQ = par.Q.cap;
+    m.pcR = par.R.cap;
+    m.count = par.count;
+    const size_t words = 2 * ((size_t)m.ccP + m.ccQ + m.ccR) + (m.ccP + m.ccQ) + (m.ccP + m.ccR) +
+                         3 * ((size_t)m.ccP + m.ccQ);
+    const size_t smem = words * sizeof(uint32_t);
+    PIC_REQUIRE(smem <= 200 * 1024, PIC_ERR_INVALID, "schoolbook merge tile too large");
+    if (smem > 48 * 1024)
+        PIC_CUDA(cudaFuncSetAttribute(merge_school_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const uint32_t cmax = std::max(m.ccP, std::max(m.ccQ, m.ccR));
+    const int threads = cmax <= 16 ? 32 : (cmax <= 64 ? 64 : (cmax <= 256 ? 128 : 256));
+    ProfScope ps(KC_BSR, 4.0 * (double)par.count * 2.0 * (m.ccP + m.ccQ + m.ccR), s);
+    merge_school_kernel<<<(unsigned)par.count, threads, smem, s>>>(m);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+}
+
+// Largest child capacity handled by the CTA schoolbook merge.
+static uint32_t g_school_max = 192;
+
+void bsr_set_school_threshold(uint32_t words) { g_school_max = words; }
+uint32_t bsr_school_threshold() { return g_school_max; }
+
+static void alloc_level(Level& L, size_t count, uint32_t cP, uint32_t cQ, uint32_t cR, cudaStream_t s)
+{
+    L.count = count;
+    alloc_slots(L.P, count, cP, s);
+    alloc_slots(L.Q, count, cQ, s);
+    alloc_slots(L.R, count, cR, s);
+    L.sign = DevBuf<uint8_t>(count, s);
+}
+
+// Recursion above the batched depth, exactly the reference's merges with
+// truncation (PI.h:93-112); nodes at `stop_depth` come from `top`.
+struct TopSource {
+    std::vector<BigFloat> P, Q, R;
+    size_t next = 0;
+};
+
+static void bsr_top(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, size_t p, int depth,
+                    int stop_depth, TopSource& src)
+{
+    if (depth == stop_depth) {
+        P = src.P[src.next];
+        Q = src.Q[src.next];
+        R = src.R[src.next];
+        src.next++;
+        return;
+    }
+    if (b - a == 1) {  // only reached when the whole tree is shallower than stop_depth
+        bsr_recursive(P, Q, R, a, b, p);
+        return;
+    }
+    const uint32_t m = (a + b) / 2;
+    BigFloat P0, Q0, R0, P1, Q1, R1;
+    bsr_top(P0, Q0, R0, a, m, p, depth + 1, stop_depth, src);
+    bsr_top(P1, Q1, R1, m, b, p, depth + 1, stop_depth, src);
+    P = P0.mul(Q1, p).add(P1.mul(R0, p), p);
+    Q = Q0.mul(Q1, p);
+    R = R0.mul(R1, p);
+}
+
 void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, size_t p)
 {
-    bsr_recursive(P, Q, R, a, b, p);
+    cudaStream_t s = ctx().stream;
+    const uint32_t T = b - a;
+    // bottom depth: node lengths <= 2
+    int Db = 0;
+    while ((((uint64_t)T + ((1ull << Db) - 1)) >> Db) > 2) Db++;
+    // top of the batched range: the shallowest depth whose merges cannot truncate
+    // (every operand <= p + 2 words and every add window <= p + 2)
+    int Dtop = Db;
+    for (int d = Db - 1; d >= 0; d--) {
+        const double nchild = ceil((double)T / (double)(1ull << (d + 1)));
+        uint32_t cP, cQ, cR;
+        slot_caps(nchild, (double)b, cP, cQ, cR);
+        if ((size_t)cP + cQ > p + 2 || (size_t)cP + cR > p + 2) break;
+        Dtop = d;
+    }
+    // the bottom kernel merges pairs of leaves exactly: that needs the
+    // reference's p + 2 window to hold two leaves (<= 6 + 5 words)
+    if (p < 16 || T < 4) {
+        bsr_recursive(P, Q, R, a, b, p);
+        return;
+    }
+    // boundaries, top down
+    std::vector<DevBuf<uint32_t>> bnd(Db + 1);
+    {
+        bnd[0] = DevBuf<uint32_t>(2, s);
+        const uint32_t h[2] = {a, b};
+        PIC_CUDA(cudaMemcpyAsync(bnd[0].get(), h, sizeof h, cudaMemcpyHostToDevice, s));
+        PIC_CUDA(cudaStreamSynchronize(s));
+        for (int d = 0; d < Db; d++) {
+            const size_t cnt = (size_t)1 << d;
+            bnd[d + 1] = DevBuf<uint32_t>(2 * cnt + 1, s);
+            split_bounds_kernel<<<grid_for(cnt, 256), 256, 0, s>>>(bnd[d].get(), cnt, bnd[d + 1].get());
+            PIC_CHECK_LAUNCH();
+            count_launch();
+        }
+    }
+    // bottom level
+    Level cur;
+    {
+        const size_t cnt = (size_t)1 << Db;
+        uint32_t cP, cQ, cR;
+        slot_caps(2.0, (double)b, cP, cQ, cR);
+        cP = std::max(cP, 12u);
+        cQ = std::max(cQ, 10u);
+        cR = std::max(cR, 8u);
+        alloc_level(cur, cnt, cP, cQ, cR, s);
+        ProfScope ps(KC_BSR, (double)cnt * 4.0 * (cP + cQ + cR), s);
+        bottom_kernel<<<grid_for(cnt, 128), 128, 0, s>>>(bnd[Db].get(), cnt, cur.P.w.get(), cur.P.len.get(),
+                                                         cur.sign.get(), cP, cur.Q.w.get(), cur.Q.len.get(), cQ,
+                                                         cur.R.w.get(), cur.R.len.get(), cR);
+        PIC_CHECK_LAUNCH();
+        count_launch();
+    }
+    // merge up to Dtop
+    size_t free_b = 0, total_b = 0;
+    PIC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    for (int d = Db - 1; d >= Dtop; d--) {
+        const size_t cnt = (size_t)1 << d;
+        const double n = ceil((double)T / (double)cnt);
+        uint32_t cP, cQ, cR;
+        slot_caps(n, (double)b, cP, cQ, cR);
+        // a parent slot must hold the exact products of its children's slots
+        cP = std::max(cP, std::max(cur.P.cap + cur.Q.cap, cur.P.cap + cur.R.cap) + 1);
+        cQ = std::max(cQ, 2 * cur.Q.cap);
+        cR = std::max(cR, 2 * cur.R.cap);
+        Level par;
+        alloc_level(par, cnt, cP, cQ, cR, s);
+        const uint32_t cmax = std::max(cur.P.cap, std::max(cur.Q.cap, cur.R.cap));
+        if (cmax <= g_school_max) merge_school(cur, par, s);
+        else merge_ntt(cur, par, s, std::max<size_t>(free_b / 4, (size_t)1 << 30));
+        cur = std::move(par);
+        bnd[d + 1].reset();
+    }
+    // hand the nodes at Dtop to the exact BigFloat recursion
+    const size_t cnt = cur.count;
+    std::vector<uint32_t> lP(cnt), lQ(cnt), lR(cnt);
+    std::vector<uint8_t> sg(cnt);
+    PIC_CUDA(cudaMemcpyAsync(lP.data(), cur.P.len.get(), cnt * 4, cudaMemcpyDeviceToHost, s));
+    PIC_CUDA(cudaMemcpyAsync(lQ.data(), cur.Q.len.get(), cnt * 4, cudaMemcpyDeviceToHost, s));
+    PIC_CUDA(cudaMemcpyAsync(lR.data(), cur.R.len.get(), cnt * 4, cudaMemcpyDeviceToHost, s));
+    PIC_CUDA(cudaMemcpyAsync(sg.data(), cur.sign.get(), cnt, cudaMemcpyDeviceToHost, s));
+    PIC_CUDA(cudaStreamSynchronize(s));
+    auto own = [&](Slots& sl) {
+        auto st = std::make_shared<WordStore>();
+        st->base = sl.w.ptr;
+        st->bytes = sizeof(uint32_t) * (sl.w.n ? sl.w.n : 1);
+        sl.w.ptr = nullptr;  // ownership moves to the WordStore
+        sl.w.n = 0;
+        return st;
+    };
+    auto sP = own(cur.P), sQ = own(cur.Q), sR = own(cur.R);
+    TopSource src;
+    src.P.reserve(cnt);
+    for (size_t i = 0; i < cnt; i++) {
+        src.P.push_back(BigFloat::from_device(sg[i] != 0, 0, sP, sP->base + i * cur.P.cap, lP[i]));
+        src.Q.push_back(BigFloat::from_device(true, 0, sQ, sQ->base + i * cur.Q.cap, lQ[i]));
+        src.R.push_back(BigFloat::from_device(true, 0, sR, sR->base + i * cur.R.cap, lR[i]));
+    }
+    bsr_top(P, Q, R, a, b, p, 0, Dtop, src);
 }
 
 }  // namespace pic

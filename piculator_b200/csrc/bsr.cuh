@@ -8,5 +8,7 @@ namespace pic {
 
 // Same P, Q, R as Pi_BSR(P, Q, R, a, b, p) word for word.
 void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, size_t p);
+void bsr_set_school_threshold(uint32_t words);
+uint32_t bsr_school_threshold();
 
 }  // namespace pic

@@ -11,6 +11,7 @@
 #include "fft.cuh"
 #include "mul.cuh"
 #include "ntt.cuh"
+#include "bsr.cuh"
 #include "pi.cuh"
 #include "transform.cuh"
 
@@ -510,6 +511,49 @@ pic_status pic_transform_free(pic_transform t)
 }
 
 // ---- Pi -------------------------------------------------------------------------
+pic_status pic_bsr(uint32_t a, uint32_t b, size_t p, int mode, pic_bf* P, pic_bf* Q, pic_bf* R)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(P);
+        PIC_REQ_PTR(Q);
+        PIC_REQ_PTR(R);
+        PIC_REQUIRE(b > a, PIC_ERR_INVALID, "empty range");
+        PIC_REQUIRE(mode == PIC_PI_CHOSEN || mode == PIC_PI_PLAIN, PIC_ERR_INVALID, "unknown mode");
+        BigFloat p_, q_, r_;
+        with_mode(mode == PIC_PI_PLAIN ? PIC_MUL_NTT_REF : PIC_MUL_AUTO, [&] {
+            if (mode == PIC_PI_PLAIN) bsr_recursive(p_, q_, r_, a, b, p);
+            else bsr_chosen(p_, q_, r_, a, b, p);
+        });
+        *P = wrap(std::move(p_));
+        *Q = wrap(std::move(q_));
+        *R = wrap(std::move(r_));
+    });
+}
+
+pic_status pic_set_tuning(int knob, int64_t value)
+{
+    return guarded([&] {
+        PIC_REQUIRE(value >= 0, PIC_ERR_INVALID, "tuning value must be >= 0");
+        switch (knob) {
+        case PIC_TUNE_BSR_SCHOOL_MAX: bsr_set_school_threshold((uint32_t)value); break;
+        case PIC_TUNE_MUL_SCHOOL_MAX: mul_set_thresholds(value, -1); break;
+        case PIC_TUNE_MUL_FFT_MAX: mul_set_thresholds(-1, value); break;
+        default: throw Error(PIC_ERR_INVALID, "unknown tuning knob");
+        }
+    });
+}
+
+int64_t pic_get_tuning(int knob)
+{
+    switch (knob) {
+    case PIC_TUNE_BSR_SCHOOL_MAX: return bsr_school_threshold();
+    case PIC_TUNE_MUL_SCHOOL_MAX: return mul_school_max();
+    case PIC_TUNE_MUL_FFT_MAX: return mul_fft_max();
+    }
+    return -1;
+}
+
 pic_status pic_pi_sizes(uint64_t d, uint64_t* hex_digits, uint64_t* p_words, uint64_t* terms)
 {
     return guarded([&] { pi_sizes(d, hex_digits, p_words, terms); });

@@ -32,6 +32,59 @@ void carry_scan_aggregates(uint32_t* agg, size_t nctas, uint32_t* final_carry, c
     count_launch();
 }
 
+__global__ void __launch_bounds__(256) carry_scan_seg_kernel(uint32_t* agg, size_t cpp)
+{
+    uint32_t* a = agg + blockIdx.x * cpp;
+    const size_t per = (cpp + blockDim.x - 1) / blockDim.x;
+    const size_t b = threadIdx.x * per, e = b + per < cpp ? b + per : cpp;
+    uint32_t acc = kGPIdentity;
+    for (size_t i = b; i < e; i++) acc = gp_combine(acc, a[i]);
+    uint32_t total;
+    const uint32_t pre = block_gp_scan(acc, &total);
+    uint32_t cin = pre & 1u;
+    for (size_t i = b; i < e; i++) {
+        const uint32_t gp = a[i];
+        a[i] = cin;
+        cin = (gp & 1u) | ((gp >> 1) & cin);
+    }
+}
+
+void carry_scan_segments(uint32_t* agg, size_t count, size_t cpp, cudaStream_t s)
+{
+    ProfScope ps(KC_CARRY, 8.0 * (double)(count * cpp), s);
+    carry_scan_seg_kernel<<<(unsigned)count, 256, 0, s>>>(agg, cpp);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+}
+
+__global__ void carry_ripple_batch_kernel(uint32_t* z, uint32_t zcap, const uint32_t* zlen, size_t wpc,
+                                          const uint32_t* cin, size_t cpp)
+{
+    if (cin[blockIdx.x] == 0) return;
+    const size_t prod = blockIdx.x / cpp, lc = blockIdx.x % cpp;
+    uint32_t* zz = z + prod * (size_t)zcap;
+    const size_t n = zlen[prod];
+    const size_t b = lc * wpc, e = b + wpc < n ? b + wpc : n;
+    __shared__ unsigned long long s_first;
+    if (threadIdx.x == 0) s_first = ~0ull;
+    __syncthreads();
+    for (size_t i = b + threadIdx.x; i < e; i += blockDim.x)
+        if (zz[i] != 0xffffffffu) atomicMin(&s_first, (unsigned long long)i);
+    __syncthreads();
+    const size_t f = (size_t)s_first;
+    for (size_t i = b + threadIdx.x; i < e && i < f; i += blockDim.x) zz[i] = 0;
+    if (threadIdx.x == 0 && f < e) zz[f] += 1u;
+}
+
+void carry_ripple_batch(uint32_t* z, uint32_t zcap, const uint32_t* zlen, size_t words_per_cta,
+                        const uint32_t* agg_cin, size_t count, size_t cpp, cudaStream_t s)
+{
+    ProfScope ps(KC_CARRY, 4.0 * (double)(count * cpp), s);
+    carry_ripple_batch_kernel<<<(unsigned)(count * cpp), 256, 0, s>>>(z, zcap, zlen, words_per_cta, agg_cin, cpp);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+}
+
 // ---- K3: ripple a carry-in of 1 through one CTA's words --------------------
 __global__ void carry_ripple_kernel(uint32_t* z, size_t n, size_t wpc, const uint32_t* cin, int mode)
 {
@@ -98,7 +151,7 @@ __global__ void __launch_bounds__(kLinThreads) addsub_k1(uint32_t* z, size_t TL,
         const uint32_t p = mode == kCarryAdd ? (dig == 0xffffffffu) : (dig == 0u);
         d[u] = dig;
         gg[u] = g;
-        gp = gp_combine(gp, g | (p << 1));
+        if (i < TL) gp = gp_combine(gp, g | (p << 1));  // padding is the scan identity
     }
     uint32_t total;
     uint32_t cin = block_gp_scan(gp, &total) & 1u;
@@ -142,7 +195,7 @@ __global__ void __launch_bounds__(kLinThreads) mulu32_k1(uint32_t* z, const uint
         }
         d[u] = dig;
         gg[u] = g;
-        gp = gp_combine(gp, g | ((uint32_t)(dig == 0xffffffffu) << 1));
+        if (i < L) gp = gp_combine(gp, g | ((uint32_t)(dig == 0xffffffffu) << 1));
     }
     uint32_t total;
     uint32_t cin = block_gp_scan(gp, &total) & 1u;

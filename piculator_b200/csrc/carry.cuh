@@ -78,4 +78,10 @@ void carry_scan_aggregates(uint32_t* agg, size_t nctas, uint32_t* final_carry, c
 void carry_ripple(uint32_t* z, size_t nwords, size_t words_per_cta, const uint32_t* agg_cin,
                   size_t nctas, CarryMode mode, cudaStream_t s);
 
+// Segmented forms for batches of products: `count` segments of `cpp` CTAs;
+// product i writes zlen[i] words at z + i * zcap.
+void carry_scan_segments(uint32_t* agg, size_t count, size_t cpp, cudaStream_t s);
+void carry_ripple_batch(uint32_t* z, uint32_t zcap, const uint32_t* zlen, size_t words_per_cta,
+                        const uint32_t* agg_cin, size_t count, size_t cpp, cudaStream_t s);
+
 }  // namespace pic

@@ -103,14 +103,15 @@ __device__ __forceinline__ void crt3(const Crt3Consts& C, uint64_t y0, uint64_t 
 // Shared tail of both conversions: limb digits (T = D_i + C_(i-1)) -> words
 // with in-block carry resolution; writes the CTA's (G, P).
 __device__ __forceinline__ void limbs_to_words(const uint64_t (&dig)[kCvtLPT], const uint32_t (&gen)[kCvtLPT],
-                                               size_t first_limb, uint32_t* z, size_t zw, uint32_t* agg)
+                                               size_t first_limb, uint32_t* z, size_t zw, uint32_t* agg_slot)
 {
     uint32_t gp = kGPIdentity;
 #pragma unroll
     for (int u = 0; u < kCvtLPT; u++) {
+        const size_t w = 2 * (first_limb + u);
         const uint32_t lo = (uint32_t)dig[u], hi = (uint32_t)(dig[u] >> 32);
-        gp = gp_combine(gp, (uint32_t)(lo == 0xffffffffu) << 1);
-        gp = gp_combine(gp, gen[u] | ((uint32_t)(hi == 0xffffffffu) << 1));
+        if (w < zw) gp = gp_combine(gp, (uint32_t)(lo == 0xffffffffu) << 1);
+        if (w + 1 < zw) gp = gp_combine(gp, gen[u] | ((uint32_t)(hi == 0xffffffffu) << 1));
     }
     uint32_t total;
     uint32_t cin = block_gp_scan(gp, &total) & 1u;
@@ -123,7 +124,7 @@ __device__ __forceinline__ void limbs_to_words(const uint64_t (&dig)[kCvtLPT], c
         if (w + 1 < zw) z[w + 1] = hi + cin;
         cin = gen[u] | ((uint32_t)(hi == 0xffffffffu) & cin);
     }
-    if (threadIdx.x == 0) agg[blockIdx.x] = total;
+    if (threadIdx.x == 0) *agg_slot = total;
 }
 
 __device__ __forceinline__ void add128(uint64_t& lo, uint64_t& hi, uint64_t v)
@@ -132,18 +133,20 @@ __device__ __forceinline__ void add128(uint64_t& lo, uint64_t& hi, uint64_t v)
     hi += (lo < v);
 }
 
-// Three-prime residues Y[q * N + j] -> words.  Limb i (64 bits) collects
-// x_i.l0 + x_(i-1).l1 + x_(i-2).l2 (< 3 * 2^64).
-__global__ void __launch_bounds__(kCvtThreads) crt3_k1(const uint64_t* __restrict__ Y, size_t N, size_t ncoef,
-                                                       Crt3Consts C, uint32_t* __restrict__ z, size_t zw,
-                                                       uint32_t* agg)
+// Three-prime residues y[q * pstride + j] -> words.  Limb i (64 bits)
+// collects x_i.l0 + x_(i-1).l1 + x_(i-2).l2 (< 3 * 2^64).  One CTA handles
+// limbs [i0, i0 + kCvtLPC) of one product.
+__device__ __forceinline__ void crt3_block(const uint64_t* __restrict__ Y, size_t pstride, size_t ncoef,
+                                           const Crt3Consts& C, uint32_t* __restrict__ z, size_t zw, int64_t i0,
+                                           uint32_t* agg_slot)
 {
     __shared__ uint64_t xs[(kCvtLPC + 3) * 3];
-    const int64_t i0 = (int64_t)blockIdx.x * (int64_t)kCvtLPC;
+    const int64_t climit = (int64_t)((zw + 1) / 2);  // limbs this product needs
     for (int t = threadIdx.x; t < (int)kCvtLPC + 3; t += blockDim.x) {
         const int64_t j = i0 - 3 + t;
         uint64_t l0 = 0, l1 = 0, l2 = 0;
-        if (j >= 0 && (size_t)j < ncoef) crt3(C, Y[j], Y[N + j], Y[2 * N + j], l0, l1, l2);
+        if (j >= 0 && (size_t)j < ncoef && j < climit)
+            crt3(C, Y[j], Y[pstride + j], Y[2 * pstride + j], l0, l1, l2);
         xs[3 * t] = l0;
         xs[3 * t + 1] = l1;
         xs[3 * t + 2] = l2;
@@ -164,7 +167,27 @@ __global__ void __launch_bounds__(kCvtThreads) crt3_k1(const uint64_t* __restric
         dig[u] = d;
         gen[u] = d < slo;
     }
-    limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw, agg);
+    limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw, agg_slot);
+}
+
+__global__ void __launch_bounds__(kCvtThreads) crt3_k1(const uint64_t* __restrict__ Y, size_t N, size_t ncoef,
+                                                       Crt3Consts C, uint32_t* __restrict__ z, size_t zw,
+                                                       uint32_t* agg)
+{
+    crt3_block(Y, N, ncoef, C, z, zw, (int64_t)blockIdx.x * (int64_t)kCvtLPC, agg + blockIdx.x);
+}
+
+// Batched: product i has residues at Y + i * istride (+ q * pstride), zlen[i]
+// words out at z + i * zcap; cpp CTAs per product.
+__global__ void __launch_bounds__(kCvtThreads) crt3_batch_k1(const uint64_t* __restrict__ Y, size_t istride,
+                                                             size_t pstride, size_t N, Crt3Consts C,
+                                                             uint32_t* __restrict__ z, uint32_t zcap,
+                                                             const uint32_t* __restrict__ zlen, size_t cpp,
+                                                             uint32_t* agg)
+{
+    const size_t prod = blockIdx.x / cpp, lc = blockIdx.x % cpp;
+    crt3_block(Y + prod * istride, pstride, N, C, z + prod * (size_t)zcap, zlen[prod],
+               (int64_t)lc * (int64_t)kCvtLPC, agg + blockIdx.x);
 }
 
 // Coefficients c_j at bit offsets bits * j (8 <= bits <= 16) -> words.  Limb
@@ -247,7 +270,7 @@ __global__ void __launch_bounds__(kCvtThreads) coefbits_k1(Loader ld, size_t nco
         dig[u] = d;
         gen[u] = d < slo;
     }
-    limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw, agg);
+    limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw, agg + blockIdx.x);
 }
 
 static void finish_scan(uint32_t* z, size_t zw, uint32_t* agg, size_t nctas, cudaStream_t s)
@@ -361,6 +384,25 @@ void ntt3_inverse_to_words(uint64_t* y, int k, size_t ncoef, int depth, uint32_t
     finish_scan(z, zw, agg.get(), nctas, s);
 }
 
+void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
+                         uint32_t zcap, const uint32_t* zlen, cudaStream_t s)
+{
+    if (count == 0) return;
+    const Crt3Consts C = make_crt3(k, 1);
+    const size_t cpp = (((size_t)zcap + 1) / 2 + kCvtLPC - 1) / kCvtLPC;
+    const size_t nctas = count * cpp;
+    DevBuf<uint32_t> agg(nctas, s);
+    {
+        ProfScope ps(KC_CRT, (24.0 * ((size_t)1 << k) + 4.0 * zcap) * (double)count, s);
+        crt3_batch_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(y, istride, pstride, (size_t)1 << k, C, z, zcap, zlen,
+                                                              cpp, agg.get());
+        PIC_CHECK_LAUNCH();
+        count_launch();
+    }
+    carry_scan_segments(agg.get(), count, cpp, s);
+    carry_ripple_batch(z, zcap, zlen, kCvtWPC, agg.get(), count, cpp, s);
+}
+
 // ---- products ----------------------------------------------------------------
 void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s)
 {
@@ -467,7 +509,7 @@ __global__ void __launch_bounds__(kSchThreads) school_kernel(uint32_t* __restric
         }
         d[u] = dig;
         gg[u] = g;
-        gp = gp_combine(gp, g | ((uint32_t)(dig == 0xffffffffu) << 1));
+        if (w < zw) gp = gp_combine(gp, g | ((uint32_t)(dig == 0xffffffffu) << 1));
     }
     uint32_t total;
     uint32_t cin = block_gp_scan(gp, &total) & 1u;
@@ -492,10 +534,23 @@ void mul_school(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, si
 }
 
 // ---- dispatch ------------------------------------------------------------------
+static int64_t g_school_max_words = 256;
+static int64_t g_fft_max_words = 0;
+
+void mul_set_thresholds(int64_t school_max, int64_t fft_max)
+{
+    if (school_max >= 0) g_school_max_words = school_max;
+    if (fft_max >= 0) g_fft_max_words = fft_max;
+}
+int64_t mul_school_max() { return g_school_max_words; }
+int64_t mul_fft_max() { return g_fft_max_words; }
+
 int mul_auto_mode(size_t na, size_t nb)
 {
     const size_t mn = na < nb ? na : nb;
-    if (na + nb <= kSchoolMaxWords && (mn <= 48 || na + nb <= 256)) return PIC_MUL_SCHOOL;
+    const size_t zw = na + nb;
+    if (zw <= kSchoolMaxWords && (mn <= 48 || (int64_t)zw <= g_school_max_words)) return PIC_MUL_SCHOOL;
+    if ((int64_t)zw <= g_fft_max_words) return PIC_MUL_FFT;
     return PIC_MUL_NTT3;
 }
 

@@ -30,12 +30,21 @@ void ntt3_forward_operand(uint64_t* out, int k, const uint32_t* a, size_t na, cu
 void ntt3_pointwise(uint64_t* a, const uint64_t* b, int k, cudaStream_t s);
 void ntt3_inverse_to_words(uint64_t* y, int k, size_t ncoef, int depth, uint32_t* z, size_t zw, cudaStream_t s);
 
+// Batched inverse output: product i's residues at y + i * istride + q * pstride
+// (length 2^k each, already inverse-transformed, one pointwise Montgomery
+// factor); zlen[i] words into z + i * zcap.
+void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
+                         uint32_t zcap, const uint32_t* zlen, cudaStream_t s);
+
 void mul_batch(const pic_mul_desc* d, size_t count, int mode, cudaStream_t s);
 
 // Dispatch on mode (PIC_MUL_*).
 void mul_dispatch(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int mode,
                   cudaStream_t s);
 int mul_auto_mode(size_t na, size_t nb);
+void mul_set_thresholds(int64_t school_max, int64_t fft_max);
+int64_t mul_school_max();
+int64_t mul_fft_max();
 
 // Reference-API conversions (NTT.cpp:330-369).
 void int_to_ntt_dev(uint64_t* T, int k, const uint32_t* A, size_t AL, cudaStream_t s);

@@ -1,0 +1,38 @@
+"""Batched binary splitting (bsr.cu) vs the oracle's Pi_BSR restatement:
+P, Q, R word for word, through both merge algorithms."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(0, 5, 100), (0, 4, 16), (0, 50, 10_000), (0, 706, 923), (17, 600, 5_000),
+         (0, 3000, 200), (0, 2000, 100_000), (1000, 1257, 50)]
+
+
+def _same(dev, want) -> bool:
+    got = dev.to_bf()
+    return (got.sign == want.sign and got.exp == want.exp and got.words.size == want.words.size
+            and np.array_equal(got.words, want.words))
+
+
+@pytest.mark.parametrize("a,b,p", CASES)
+@pytest.mark.parametrize("school_max", [192, 8])
+def test_bsr_vs_oracle(pic, oracle, a, b, p, school_max):
+    saved = pic.get_tuning(pic.TUNE_BSR_SCHOOL_MAX)
+    pic.set_tuning(pic.TUNE_BSR_SCHOOL_MAX, school_max)
+    try:
+        P, Q, R = pic.bsr(a, b, p, pic.PI_CHOSEN)
+    finally:
+        pic.set_tuning(pic.TUNE_BSR_SCHOOL_MAX, saved)
+    wP, wQ, wR = oracle.bsr(a, b, p)
+    assert _same(Q, wQ), "Q"
+    assert _same(R, wR), "R"
+    assert _same(P, wP), "P"
+
+
+def test_bsr_plain_form_vs_oracle(pic, oracle):
+    P, Q, R = pic.bsr(0, 300, 1000, pic.PI_PLAIN)
+    wP, wQ, wR = oracle.bsr(0, 300, 1000)
+    assert _same(P, wP) and _same(Q, wQ) and _same(R, wR)
