@@ -66,9 +66,11 @@ static void slot_caps(double n, double T, uint32_t& cP, uint32_t& cQ, uint32_t& 
     const double lr = log2(72.0) + 3.0 * log2(T + 1.0);
     const double bq = n * lq, br = n * lr;
     const double bp = bq + log2(n * (0.0895 + 3.6e-6 * T) + 1.0) + 1.0;
-    cQ = (uint32_t)ceil(bq / 32.0) + 2;
-    cR = (uint32_t)ceil(br / 32.0) + 2;
-    cP = (uint32_t)ceil(bp / 32.0) + 2;
+    // margins: a product's words (na + nb, top word possibly zero) and P's
+    // carry word fit in ceil(bound / 32) + 3 (+ 4 for P)
+    cQ = (uint32_t)ceil(bq / 32.0) + 3;
+    cR = (uint32_t)ceil(br / 32.0) + 3;
+    cP = (uint32_t)ceil(bp / 32.0) + 4;
 }
 
 // ---------------------------------------------------------------------------
@@ -903,15 +905,18 @@ void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, s
         const double n = ceil((double)T / (double)cnt);
         uint32_t cP, cQ, cR;
         slot_caps(n, (double)b, cP, cQ, cR);
-        // a parent slot must hold the exact products of its children's slots
-        cP = std::max(cP, std::max(cur.P.cap + cur.Q.cap, cur.P.cap + cur.R.cap) + 1);
-        cQ = std::max(cQ, 2 * cur.Q.cap);
-        cR = std::max(cR, 2 * cur.R.cap);
         Level par;
         alloc_level(par, cnt, cP, cQ, cR, s);
         const uint32_t cmax = std::max(cur.P.cap, std::max(cur.Q.cap, cur.R.cap));
-        if (cmax <= g_school_max) merge_school(cur, par, s);
+        TraceSpan span(s);
+        const bool school = cmax <= g_school_max;
+        if (school) merge_school(cur, par, s);
         else merge_ntt(cur, par, s, std::max<size_t>(free_b / 4, (size_t)1 << 30));
+        if (tracing())
+            fprintf(stderr,
+                    "{\"trace\": \"bsr_level\", \"depth\": %d, \"parents\": %zu, \"child_caps\": [%u, %u, %u], "
+                    "\"algo\": \"%s\", \"ms\": %.3f}\n",
+                    d, cnt, cur.P.cap, cur.Q.cap, cur.R.cap, school ? "school" : "ntt3", span.end_ms());
         cur = std::move(par);
         bnd[d + 1].reset();
     }
@@ -940,7 +945,11 @@ void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, s
         src.Q.push_back(BigFloat::from_device(true, 0, sQ, sQ->base + i * cur.Q.cap, lQ[i]));
         src.R.push_back(BigFloat::from_device(true, 0, sR, sR->base + i * cur.R.cap, lR[i]));
     }
+    TraceSpan tspan(s);
     bsr_top(P, Q, R, a, b, p, 0, Dtop, src);
+    if (tracing())
+        fprintf(stderr, "{\"trace\": \"bsr_top\", \"nodes\": %zu, \"depth\": %d, \"ms\": %.3f}\n", cnt, Dtop,
+                tspan.end_ms());
 }
 
 }  // namespace pic

@@ -113,6 +113,17 @@ struct ProfScope {
     ~ProfScope();
 };
 
+// Tracing: when the environment variable PIC_TRACE is set, phases print one
+// JSON line each to stderr with their device time.
+bool tracing();
+struct TraceSpan {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaStream_t s = nullptr;
+    TraceSpan(cudaStream_t st);
+    double end_ms();  // synchronises
+    ~TraceSpan();
+};
+
 inline unsigned grid_for(size_t n, unsigned block, unsigned cap = 148u * 32u)
 {
     size_t g = (n + block - 1) / block;

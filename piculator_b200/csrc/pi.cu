@@ -101,6 +101,10 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
         tm.mark();
         if (mode == PIC_PI_PLAIN) bsr_recursive(P, Q, R, 0, (uint32_t)terms, (size_t)p);
         else bsr_chosen(P, Q, R, 0, (uint32_t)terms, (size_t)p);
+        if (tracing()) {
+            PIC_CUDA(cudaStreamSynchronize(ctx().stream));
+            fprintf(stderr, "{\"trace\": \"bsr_done\"}\n");
+        }
         P = Q.mul(13591409u).add(P, (size_t)p);  // PI.h:180-181
         Q = Q.mul(4270934400u);
         tm.mark();

@@ -2,6 +2,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <stdlib.h>
+
 #include <vector>
 
 #include "common.cuh"
@@ -112,6 +114,37 @@ void read_words(uint32_t* host, const uint32_t* dev, size_t count, cudaStream_t 
         PIC_CUDA(cudaMemcpyAsync(host, dev, count * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         PIC_CUDA(cudaStreamSynchronize(s));
     }
+}
+
+// ---- tracing ---------------------------------------------------------------------
+bool tracing()
+{
+    static const bool on = getenv("PIC_TRACE") != nullptr;
+    return on;
+}
+
+TraceSpan::TraceSpan(cudaStream_t st) : s(st)
+{
+    if (!tracing()) return;
+    PIC_CUDA(cudaEventCreate(&a));
+    PIC_CUDA(cudaEventCreate(&b));
+    PIC_CUDA(cudaEventRecord(a, s));
+}
+
+double TraceSpan::end_ms()
+{
+    if (!a) return 0.0;
+    PIC_CUDA(cudaEventRecord(b, s));
+    PIC_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    PIC_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+}
+
+TraceSpan::~TraceSpan()
+{
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
 }
 
 // ---- live kernel timing ------------------------------------------------------
