@@ -131,6 +131,21 @@ typedef struct {
 pic_status pic_mul_batch(const pic_mul_desc* descs, size_t count, int mode,
                          pic_stream s);
 
+/* Allocation-free product.  No counterpart in the reference: this exists for
+ * callers that cannot allocate device memory when they multiply (an
+ * application that has given its device memory to its own pool, a
+ * latency-critical loop that must not take the allocator's locks or risk an
+ * out-of-memory failure mid-computation).  Same result as pic_mul, computed
+ * with the three-prime NTT in fixed storage compiled into the library
+ * (about 3.5 MiB per GPU, held until the process exits).  Limit:
+ * ceil(na/2) + ceil(nb/2) - 1 <= 65536 (about 131,000 product words);
+ * longer products return PIC_ERR_LENGTH.  Calls share that storage, so calls
+ * that overlap on the GPU race.  The first call on each device sets up the
+ * storage (resolving its device address, filling twiddle tables) and
+ * synchronises the stream: make that first call outside any stream capture. */
+pic_status pic_mul_noalloc(uint32_t* z, const uint32_t* a, size_t na,
+                           const uint32_t* b, size_t nb, pic_stream s);
+
 /* Host-buffer convenience: copies in, multiplies, copies out (synchronous). */
 pic_status pic_mul_host(uint32_t* z, const uint32_t* a, size_t na,
                         const uint32_t* b, size_t nb, int mode);

@@ -97,6 +97,7 @@ _SIGS = {
     "pic_fft_last_max_err": ([], C.c_double),
     "pic_mul": ([_U32P, _U32P, C.c_size_t, _U32P, C.c_size_t, C.c_int, _P], C.c_int),
     "pic_mul_batch": ([C.POINTER(MulDesc), C.c_size_t, C.c_int, _P], C.c_int),
+    "pic_mul_noalloc": ([_U32P, _U32P, C.c_size_t, _U32P, C.c_size_t, _P], C.c_int),
     "pic_mul_host": ([_U32P, _U32P, C.c_size_t, _U32P, C.c_size_t, C.c_int], C.c_int),
     "pic_bf_from_words": ([C.POINTER(C.c_void_p), C.c_int, C.c_int64, _U32P, C.c_size_t], C.c_int),
     "pic_bf_from_u32": ([C.POINTER(C.c_void_p), C.c_uint32, C.c_int], C.c_int),

@@ -304,6 +304,18 @@ pic_status pic_mul_batch(const pic_mul_desc* d, size_t count, int mode, pic_stre
     });
 }
 
+pic_status pic_mul_noalloc(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(z);
+        PIC_REQ_PTR(a);
+        PIC_REQ_PTR(b);
+        PIC_REQUIRE(na > 0 && nb > 0, PIC_ERR_INVALID, "empty operand");
+        mul_noalloc(z, a, na, b, nb, resolve(s));
+    });
+}
+
 pic_status pic_mul_host(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int mode)
 {
     return guarded([&] {

@@ -403,6 +403,30 @@ void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size
     carry_ripple_batch(z, zcap, zlen, kCvtWPC, agg.get(), count, cpp, s);
 }
 
+// Pieces used by the allocation-free product (noalloc.cu): the same split and
+// CRT + carry kernels, with every buffer supplied by the caller.
+void split3_into(uint64_t* out, int k, const uint32_t* a, size_t na, const uint64_t primes[3], cudaStream_t s)
+{
+    const size_t N = (size_t)1 << k;
+    split3_kernel<<<grid_for(N, 256), 256, 0, s>>>(out, a, na, N, primes[0], primes[1], primes[2]);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+}
+
+size_t crt3_scratch_ctas(size_t zw) { return ((zw + 1) / 2 + kCvtLPC - 1) / kCvtLPC; }
+
+void crt3_to_words_scratch(const uint64_t* y, int k, size_t ncoef, uint32_t* z, size_t zw, uint32_t* agg,
+                           cudaStream_t s)
+{
+    const Crt3Consts C = make_crt3(k, 1);
+    const size_t nctas = crt3_scratch_ctas(zw);
+    crt3_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(y, (size_t)1 << k, ncoef, C, z, zw, agg);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+    carry_scan_aggregates(agg, nctas, nullptr, s);
+    carry_ripple(z, zw, kCvtWPC, agg, nctas, kCarryAdd, s);
+}
+
 // ---- products ----------------------------------------------------------------
 void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s)
 {

@@ -37,6 +37,16 @@ void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size
                          uint32_t zcap, const uint32_t* zlen, cudaStream_t s);
 
 void mul_batch(const pic_mul_desc* d, size_t count, int mode, cudaStream_t s);
+// noalloc.cu: the three-prime product in fixed library storage (no allocation).
+void mul_noalloc(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s);
+
+// Caller-supplied-buffer forms of the three-prime pieces (noalloc.cu):
+// split3_into writes 3 * 2^k residues mod primes[0..2]; crt3_to_words_scratch
+// needs crt3_scratch_ctas(zw) words of `agg` and ncoef <= 2^k.
+void split3_into(uint64_t* out, int k, const uint32_t* a, size_t na, const uint64_t primes[3], cudaStream_t s);
+size_t crt3_scratch_ctas(size_t zw);
+void crt3_to_words_scratch(const uint64_t* y, int k, size_t ncoef, uint32_t* z, size_t zw, uint32_t* agg,
+                           cudaStream_t s);
 
 // Dispatch on mode (PIC_MUL_*).
 void mul_dispatch(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int mode,
