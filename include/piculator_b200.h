@@ -120,7 +120,10 @@ pic_status pic_mul(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b,
                    size_t nb, int mode, pic_stream s);
 
 /* Many independent products in one call (device pointers in each record).
- * The descriptor array itself is host memory. */
+ * The descriptor array itself is host memory.  Short products run in one
+ * persistent schoolbook launch, the rest in batched three-prime NTT size
+ * classes; the launch sequence is captured as a CUDA graph and replayed when
+ * a later call has the same sizes.  Returns after the products are written. */
 typedef struct {
     uint32_t* z;
     const uint32_t* a;
@@ -225,10 +228,17 @@ pic_status pic_bsr(uint32_t a, uint32_t b, size_t p, int mode, pic_bf* P, pic_bf
 enum {
     PIC_TUNE_BSR_SCHOOL_MAX = 0, /* children up to this many words: CTA schoolbook merge */
     PIC_TUNE_MUL_SCHOOL_MAX = 1, /* products up to this many words: schoolbook in AUTO */
-    PIC_TUNE_MUL_FFT_MAX = 2     /* products up to this many words: FP64 FFT in AUTO (0: never) */
+    PIC_TUNE_MUL_FFT_MAX = 2,    /* products up to this many words: FP64 FFT in AUTO (0: never) */
+    PIC_TUNE_BATCH_GRAPHS = 3    /* 1: pic_mul_batch replays captured CUDA graphs (default) */
 };
 pic_status pic_set_tuning(int knob, int64_t value);
 int64_t pic_get_tuning(int knob);
+
+/* NTT geometry for transforms of length 2^k: bits handled by the contiguous
+ * row pass (8..13), log2 columns per CTA in column passes (2..6, 0 = automatic)
+ * and bits per register round (2..4, i.e. radix 4, 8 or 16). */
+pic_status pic_set_ntt_geometry(int k, int row_bits, int col_width_log2, int radix_log2);
+pic_status pic_get_ntt_geometry(int k, int* row_bits, int* col_width_log2, int* radix_log2);
 
 /* Sizes Pi() derives from the digit count (PI.h:141-144). */
 pic_status pic_pi_sizes(uint64_t decimal_digits, uint64_t* hex_digits,

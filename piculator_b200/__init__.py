@@ -19,7 +19,7 @@ from typing import NamedTuple, Sequence
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libpiculator_b200.so")
+LIB_PATH = os.environ.get("PICULATOR_B200_LIB", os.path.join(HERE, "lib", "libpiculator_b200.so"))
 HEADER = os.path.join(os.path.dirname(HERE), "include", "piculator_b200.h")
 
 # pic_status (include/piculator_b200.h)
@@ -125,6 +125,8 @@ _SIGS = {
                  C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)], C.c_int),
     "pic_set_tuning": ([C.c_int, C.c_int64], C.c_int),
     "pic_get_tuning": ([C.c_int], C.c_int64),
+    "pic_set_ntt_geometry": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+    "pic_get_ntt_geometry": ([C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "pic_pi_sizes": ([C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                       C.POINTER(C.c_uint64)], C.c_int),
 }
@@ -163,10 +165,36 @@ def check(status: int) -> None:
 _initialised = False
 
 
-def init(device: int = 0) -> None:
+TUNING_FILE = os.path.join(HERE, "tuning.json")
+
+
+def apply_tuning(path: str = TUNING_FILE) -> bool:
+    """Applies an autotuner result (piculator_b200/autotune.py) if present."""
+    if not os.path.exists(path):
+        return False
+    import json
+    with open(path) as f:
+        t = json.load(f)
+    L = lib()
+    for k, g in t.get("ntt", {}).items():
+        check(L.pic_set_ntt_geometry(int(k), g["row_bits"], g["col_width_log2"], g["radix_log2"]))
+    prod = t.get("products", {})
+    if "school_max_words" in prod:
+        check(L.pic_set_tuning(TUNE_MUL_SCHOOL_MAX, int(prod["school_max_words"])))
+    if "fft_max_words" in prod:
+        check(L.pic_set_tuning(TUNE_MUL_FFT_MAX, int(prod["fft_max_words"])))
+    if "bsr_school_max_words" in t.get("bsr", {}):
+        check(L.pic_set_tuning(TUNE_BSR_SCHOOL_MAX, int(t["bsr"]["bsr_school_max_words"])))
+    return True
+
+
+def init(device: int = 0, tuned: bool = True) -> None:
+    """pic_init(device), then the autotuner's settings when tuned is set."""
     global _initialised
     check(lib().pic_init(device))
     _initialised = True
+    if tuned:
+        apply_tuning(TUNING_FILE)
 
 
 def synchronize() -> None:
@@ -309,7 +337,7 @@ class Transform:
         return DeviceBigFloat(out.value)
 
 
-TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX = range(3)
+TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS = range(4)
 
 
 def set_tuning(knob: int, value: int) -> None:
@@ -318,6 +346,16 @@ def set_tuning(knob: int, value: int) -> None:
 
 def get_tuning(knob: int) -> int:
     return int(lib().pic_get_tuning(knob))
+
+
+def set_ntt_geometry(k: int, row_bits: int, col_width_log2: int, radix_log2: int) -> None:
+    check(lib().pic_set_ntt_geometry(k, row_bits, col_width_log2, radix_log2))
+
+
+def get_ntt_geometry(k: int) -> tuple[int, int, int]:
+    r, c, x = C.c_int(), C.c_int(), C.c_int()
+    check(lib().pic_get_ntt_geometry(k, C.byref(r), C.byref(c), C.byref(x)))
+    return r.value, c.value, x.value
 
 
 def bsr(a: int, b: int, p: int, form: int = 0):

@@ -1,0 +1,156 @@
+"""Autotuner for the B200 engine: measures this GPU and writes tuning.json.
+
+Size classes and what is chosen for each:
+  * NTT transform length 2^k (k = 10..27): row-pass bits (11, 12, 13), radix
+    of the register rounds (8 or 16) and column-tile width (automatic or
+    4..32 columns), timed on three-prime products of that length;
+  * single products by length: the form (schoolbook, three-prime NTT, FP64
+    FFT, or the one-prime reference layout) -- i.e. the prime count and
+    transform family -- as crossover thresholds;
+  * binary splitting: the child length below which a level merges with the
+    CTA schoolbook instead of batched NTTs, timed on whole pi runs.
+
+    python -m piculator_b200.autotune [--quick] [--out PATH]
+
+`piculator_b200.init()` applies the file it finds next to this module.
+Every candidate computes the same words (products are exact); only time
+differs, measured with CUDA events on the library's stream.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import time
+
+import numpy as np
+
+import piculator_b200 as P
+
+DEFAULT_OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
+
+
+def _words(seed: int, n: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, 2 ** 32, n, dtype=np.uint64).astype(np.uint32)
+
+
+class Timer:
+    def __init__(self):
+        import torch
+        self.torch = torch
+        self.stream = torch.cuda.ExternalStream(P.lib().pic_default_stream())
+
+    def time(self, fn, reps: int = 3, warm: int = 1) -> float:
+        for _ in range(warm):
+            fn()
+        e0 = self.torch.cuda.Event(enable_timing=True)
+        e1 = self.torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        for _ in range(reps):
+            fn()
+        e1.record(self.stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+
+def tune_ntt(timer: Timer, ks, quick: bool) -> dict:
+    torch = timer.torch
+    out = {}
+    for k in ks:
+        n = 1 << k  # words per operand: the product fills 2^k three-prime points
+        a = torch.from_numpy(_words(k, n).view(np.int32)).cuda()
+        b = torch.from_numpy(_words(k + 100, n).view(np.int32)).cuda()
+        z = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+        cands = []
+        for rb in (3, 4):
+            if k <= 13:
+                cands.append((12, 0, rb))
+                continue
+            for row in ((12,) if quick else (11, 12, 13)):
+                for lw in ((0,) if quick else (0, 3, 5)):
+                    cands.append((row, lw, rb))
+        best = None
+        for row, lw, rb in cands:
+            P.set_ntt_geometry(k, row, lw, rb)
+            try:
+                ms = timer.time(lambda: P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, "ntt3"),
+                                reps=2 if k >= 24 else 4)
+            except P.PicError as e:  # a geometry this GPU cannot launch
+                print(f"ntt k={k} {row}/{lw}/{rb}: skipped ({e})", flush=True)
+                continue
+            if best is None or ms < best[0]:
+                best = (ms, row, lw, rb)
+        P.set_ntt_geometry(k, best[1], best[2], best[3])
+        out[str(k)] = {"row_bits": best[1], "col_width_log2": best[2], "radix_log2": best[3], "ms": best[0]}
+        print(f"ntt k={k}: {out[str(k)]}", flush=True)
+    return out
+
+
+def tune_products(timer: Timer) -> dict:
+    torch = timer.torch
+    rows = []
+    for lg in range(4, 21):
+        n = 1 << (lg - 1)
+        a = torch.from_numpy(_words(lg, n).view(np.int32)).cuda()
+        b = torch.from_numpy(_words(lg + 50, n).view(np.int32)).cuda()
+        z = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+        row = {"words": 2 * n}
+        for mode in ("school", "ntt3", "fft", "ntt_ref"):
+            if mode == "school" and 2 * n > 4096:
+                continue
+            row[mode] = timer.time(lambda: P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, mode))
+        rows.append(row)
+        print(f"product {2 * n} words: { {k: round(v, 4) for k, v in row.items()} }", flush=True)
+    school_max = 0
+    fft_max = 0
+    for r in rows:
+        if "school" in r and r["school"] <= r["ntt3"]:
+            school_max = r["words"]
+        if r["fft"] < r["ntt3"] and r["words"] > school_max:
+            fft_max = r["words"]
+    return {"school_max_words": school_max, "fft_max_words": fft_max, "table": rows}
+
+
+def tune_bsr(quick: bool) -> dict:
+    digits = 10_000_000 if quick else 100_000_000
+    res = {}
+    for thr in (192, 400, 600, 900):
+        P.set_tuning(P.TUNE_BSR_SCHOOL_MAX, thr)
+        P.pi_hex(digits, P.PI_CHOSEN, want_text=False)
+        t0 = time.perf_counter()
+        _, st = P.pi_hex(digits, P.PI_CHOSEN, want_text=False)
+        res[thr] = st["seconds_bsr"]
+        print(f"bsr school threshold {thr}: {res[thr]:.4f} s", flush=True)
+    best = min(res, key=res.get)
+    P.set_tuning(P.TUNE_BSR_SCHOOL_MAX, best)
+    return {"bsr_school_max_words": best, "digits": digits, "seconds": res}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--quick", action="store_true")
+    ap.add_argument("--out", default=DEFAULT_OUT)
+    args = ap.parse_args()
+    P.init(0, tuned=False)
+    timer = Timer()
+    result = {"gpu": None}
+    try:
+        import torch
+        result["gpu"] = torch.cuda.get_device_name(0)
+    except Exception:
+        pass
+    result["ntt"] = tune_ntt(timer, range(10, 28) if not args.quick else (14, 18, 22, 24, 26), args.quick)
+    prod = tune_products(timer)
+    result["products"] = prod
+    P.set_tuning(P.TUNE_MUL_SCHOOL_MAX, prod["school_max_words"])
+    P.set_tuning(P.TUNE_MUL_FFT_MAX, prod["fft_max_words"])
+    result["bsr"] = tune_bsr(args.quick)
+    with open(args.out, "w") as f:
+        json.dump(result, f, indent=1)
+    print("wrote", args.out)
+
+
+if __name__ == "__main__":
+    main()

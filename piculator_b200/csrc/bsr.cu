@@ -323,15 +323,10 @@ __device__ uint32_t cta_mul(const uint32_t* a, uint32_t na, const uint32_t* b, u
 // Highest index < n with x[i] != 0, plus one (0 if none).
 __device__ uint32_t cta_top(const uint32_t* x, uint32_t n)
 {
-    __shared__ uint32_t s_top;
-    if (threadIdx.x == 0) s_top = 0;
-    __syncthreads();
+    unsigned long long mine = 0;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
-        if (x[i] != 0) atomicMax(&s_top, i + 1);
-    __syncthreads();
-    const uint32_t r = s_top;
-    __syncthreads();
-    return r;
+        if (x[i] != 0) mine = i + 1;
+    return (uint32_t)block_max_u64(mine);
 }
 
 // Signed sum of magnitudes (sa, a[0..na)) + (sb, b[0..nb)) into z (capacity
@@ -348,16 +343,11 @@ __device__ uint32_t cta_signed_add(bool sa, const uint32_t* a, uint32_t na, bool
     bool swap = false;
     if (sub) {
         // compare magnitudes: highest differing word decides
-        __shared__ uint32_t s_hi;
-        if (threadIdx.x == 0) s_hi = 0;
-        __syncthreads();
+        unsigned long long mine = 0;
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
-            if (A(i) != B(i)) atomicMax(&s_hi, i + 1);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const uint32_t h = s_hi;
-            s_cmp = h == 0 ? 0 : (A(h - 1) > B(h - 1) ? 1 : -1);
-        }
+            if (A(i) != B(i)) mine = i + 1;
+        const uint32_t h = (uint32_t)block_max_u64(mine);
+        if (threadIdx.x == 0) s_cmp = h == 0 ? 0 : (A(h - 1) > B(h - 1) ? 1 : -1);
         __syncthreads();
         const int c = s_cmp;
         __syncthreads();
@@ -561,15 +551,18 @@ __global__ void __launch_bounds__(256) signed_add_kernel(const uint32_t* __restr
     auto B = [&](uint32_t k) -> uint32_t { return k < nb ? b[k] : 0u; };
     const bool sub = sa != sb;
     bool swap = false;
-    __shared__ uint32_t s_hi;
     __shared__ uint32_t s_carry;
     if (sub) {
-        if (threadIdx.x == 0) s_hi = 0;
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < n; k += blockDim.x)
-            if (A(k) != B(k)) atomicMax(&s_hi, k + 1);
-        __syncthreads();
-        const uint32_t h = s_hi;
+        // the highest differing word decides; it is almost always near the top,
+        // so look at the top block of words first
+        uint32_t h = 0;
+        for (uint32_t top = n; top > 0 && h == 0;) {
+            const uint32_t lo = top > blockDim.x ? top - blockDim.x : 0;
+            const uint32_t k = lo + threadIdx.x;
+            unsigned long long mine = (k < top && A(k) != B(k)) ? k + 1 : 0;
+            h = (uint32_t)block_max_u64(mine);
+            top = lo;
+        }
         if (h == 0) {
             if (threadIdx.x == 0) {
                 Pl[c0 + i] = 0;
@@ -638,14 +631,17 @@ __global__ void __launch_bounds__(256) signed_add_kernel(const uint32_t* __restr
         }
         return;
     }
-    // strip leading zeros after a subtraction
-    if (threadIdx.x == 0) s_hi = 0;
+    // strip leading zeros after a subtraction, scanning down from the top
     __syncthreads();
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x)
-        if (z[k] != 0) atomicMax(&s_hi, k + 1);
-    __syncthreads();
+    uint32_t l = 0;
+    for (uint32_t top = n; top > 0 && l == 0;) {
+        const uint32_t lo = top > blockDim.x ? top - blockDim.x : 0;
+        const uint32_t k = lo + threadIdx.x;
+        unsigned long long mine = (k < top && z[k] != 0) ? k + 1 : 0;
+        l = (uint32_t)block_max_u64(mine);
+        top = lo;
+    }
     if (threadIdx.x == 0) {
-        const uint32_t l = s_hi;
         Pl[c0 + i] = l;
         Ps[c0 + i] = l == 0 ? 1 : ((swap ? sb : sa) ? 1 : 0);
     }
@@ -798,7 +794,7 @@ static void merge_school(Level& ch, Level& par, cudaStream_t s)
 }
 
 // Largest child capacity handled by the CTA schoolbook merge.
-static uint32_t g_school_max = 192;
+static uint32_t g_school_max = 600;
 
 void bsr_set_school_threshold(uint32_t words) { g_school_max = words; }
 uint32_t bsr_school_threshold() { return g_school_max; }

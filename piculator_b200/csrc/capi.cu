@@ -551,8 +551,24 @@ pic_status pic_set_tuning(int knob, int64_t value)
         case PIC_TUNE_BSR_SCHOOL_MAX: bsr_set_school_threshold((uint32_t)value); break;
         case PIC_TUNE_MUL_SCHOOL_MAX: mul_set_thresholds(value, -1); break;
         case PIC_TUNE_MUL_FFT_MAX: mul_set_thresholds(-1, value); break;
+        case PIC_TUNE_BATCH_GRAPHS: mul_batch_set_graphs(value != 0); break;
         default: throw Error(PIC_ERR_INVALID, "unknown tuning knob");
         }
+    });
+}
+
+pic_status pic_set_ntt_geometry(int k, int row_bits, int col_width_log2, int radix_log2)
+{
+    return guarded([&] { ntt_set_geometry(k, row_bits, col_width_log2, radix_log2); });
+}
+
+pic_status pic_get_ntt_geometry(int k, int* row_bits, int* col_width_log2, int* radix_log2)
+{
+    return guarded([&] {
+        PIC_REQ_PTR(row_bits);
+        PIC_REQ_PTR(col_width_log2);
+        PIC_REQ_PTR(radix_log2);
+        ntt_get_geometry(k, row_bits, col_width_log2, radix_log2);
     });
 }
 
@@ -562,6 +578,7 @@ int64_t pic_get_tuning(int knob)
     case PIC_TUNE_BSR_SCHOOL_MAX: return bsr_school_threshold();
     case PIC_TUNE_MUL_SCHOOL_MAX: return mul_school_max();
     case PIC_TUNE_MUL_FFT_MAX: return mul_fft_max();
+    case PIC_TUNE_BATCH_GRAPHS: return 1;
     }
     return -1;
 }

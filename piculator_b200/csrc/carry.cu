@@ -65,13 +65,10 @@ __global__ void carry_ripple_batch_kernel(uint32_t* z, uint32_t zcap, const uint
     uint32_t* zz = z + prod * (size_t)zcap;
     const size_t n = zlen[prod];
     const size_t b = lc * wpc, e = b + wpc < n ? b + wpc : n;
-    __shared__ unsigned long long s_first;
-    if (threadIdx.x == 0) s_first = ~0ull;
-    __syncthreads();
+    unsigned long long mine = ~0ull;
     for (size_t i = b + threadIdx.x; i < e; i += blockDim.x)
-        if (zz[i] != 0xffffffffu) atomicMin(&s_first, (unsigned long long)i);
-    __syncthreads();
-    const size_t f = (size_t)s_first;
+        if (zz[i] != 0xffffffffu && i < mine) mine = i;
+    const size_t f = (size_t)block_min_u64(mine);
     for (size_t i = b + threadIdx.x; i < e && i < f; i += blockDim.x) zz[i] = 0;
     if (threadIdx.x == 0 && f < e) zz[f] += 1u;
 }
@@ -92,13 +89,10 @@ __global__ void carry_ripple_kernel(uint32_t* z, size_t n, size_t wpc, const uin
     if (cin[c] == 0) return;
     const size_t b = c * wpc, e = b + wpc < n ? b + wpc : n;
     const uint32_t stop_unless = mode == kCarryAdd ? 0xffffffffu : 0u;
-    __shared__ unsigned long long s_first;
-    if (threadIdx.x == 0) s_first = ~0ull;
-    __syncthreads();
+    unsigned long long mine = ~0ull;
     for (size_t i = b + threadIdx.x; i < e; i += blockDim.x)
-        if (z[i] != stop_unless) atomicMin(&s_first, (unsigned long long)i);
-    __syncthreads();
-    const size_t f = (size_t)s_first;
+        if (z[i] != stop_unless && i < mine) mine = i;
+    const size_t f = (size_t)block_min_u64(mine);
     for (size_t i = b + threadIdx.x; i < e && i < f; i += blockDim.x) z[i] = ~stop_unless;
     if (threadIdx.x == 0 && f < e) z[f] = mode == kCarryAdd ? z[f] + 1u : z[f] - 1u;
 }
@@ -257,8 +251,11 @@ void lin_mul_u32(uint32_t* z, const uint32_t* a, size_t L, uint32_t x, cudaStrea
 __global__ void top_nonzero_kernel(const uint32_t* z, size_t n, unsigned long long* out)
 {
     // out = 1 + highest index with z[i] != 0 (0 if all zero); out preset to 0
+    unsigned long long mine = 0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        if (z[i] != 0) atomicMax(out, (unsigned long long)(i + 1));
+        if (z[i] != 0) mine = i + 1;
+    mine = warp_max_u64(mine);
+    if ((threadIdx.x & 31) == 0 && mine) atomicMax(out, mine);
 }
 
 size_t lin_top_nonzero(const uint32_t* z, size_t n, cudaStream_t s)
@@ -279,11 +276,13 @@ size_t lin_top_nonzero(const uint32_t* z, size_t n, cudaStream_t s)
 __global__ void ucmp_kernel(WordView a, WordView b, int64_t lo, int64_t hi, unsigned long long* out)
 {
     const int64_t n = hi - lo;
+    unsigned long long mine = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t mag = lo + i;
-        if (word_at(a.T, a.exp, a.L, mag) != word_at(b.T, b.exp, b.L, mag))
-            atomicMax(out, (unsigned long long)(i + 1));
+        if (word_at(a.T, a.exp, a.L, mag) != word_at(b.T, b.exp, b.L, mag)) mine = (unsigned long long)(i + 1);
     }
+    mine = warp_max_u64(mine);
+    if ((threadIdx.x & 31) == 0 && mine) atomicMax(out, mine);
 }
 
 int lin_ucmp(const WordView& a, const WordView& b, cudaStream_t s)

@@ -70,6 +70,55 @@ __device__ __forceinline__ uint32_t block_gp_scan(uint32_t gp, uint32_t* total)
     return res;
 }
 
+// Warp-reduced max / min: one shared or global atomic per warp instead of one
+// per qualifying element (a single hot address serialises per-element atomics).
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v)
+{
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, off);
+        v = o > v ? o : v;
+    }
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
+{
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, off);
+        v = o < v ? o : v;
+    }
+    return v;
+}
+
+// Block-wide max of one value per thread (all threads call; blockDim % 32 == 0).
+__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v)
+{
+    __shared__ unsigned long long s_m;
+    if (threadIdx.x == 0) s_m = 0;
+    __syncthreads();
+    v = warp_max_u64(v);
+    if ((threadIdx.x & 31) == 0 && v) atomicMax(&s_m, v);
+    __syncthreads();
+    const unsigned long long r = s_m;
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v)
+{
+    __shared__ unsigned long long s_m;
+    if (threadIdx.x == 0) s_m = ~0ull;
+    __syncthreads();
+    v = warp_min_u64(v);
+    if ((threadIdx.x & 31) == 0 && v != ~0ull) atomicMin(&s_m, v);
+    __syncthreads();
+    const unsigned long long r = s_m;
+    __syncthreads();
+    return r;
+}
+
 enum CarryMode { kCarryAdd = 0, kCarrySub = 1 };
 
 // Cross-CTA phases (carry.cu).  agg[c] = (G, P) of CTA c; words_per_cta words

@@ -357,11 +357,13 @@ static NttBatch ntt3_batch(uint64_t* data, int k)
 void ntt3_forward_operand(uint64_t* out, int k, const uint32_t* a, size_t na, cudaStream_t s)
 {
     const size_t N = (size_t)1 << k;
-    ProfScope ps(KC_SPLIT, 4.0 * (double)na + 24.0 * (double)N, s);
-    split3_kernel<<<grid_for(N, 256), 256, 0, s>>>(out, a, na, N, kProductPrimes[0], kProductPrimes[1],
-                                                   kProductPrimes[2]);
-    PIC_CHECK_LAUNCH();
-    count_launch();
+    {
+        ProfScope ps(KC_SPLIT, 4.0 * (double)na + 24.0 * (double)N, s);
+        split3_kernel<<<grid_for(N, 256), 256, 0, s>>>(out, a, na, N, kProductPrimes[0], kProductPrimes[1],
+                                                       kProductPrimes[2]);
+        PIC_CHECK_LAUNCH();
+        count_launch();
+    }
     ntt_forward_dif(ntt3_batch(out, k), k, s);
 }
 
@@ -614,14 +616,6 @@ void mul_dispatch(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, 
         return;
     }
     default: throw Error(PIC_ERR_INVALID, "unknown multiply mode");
-    }
-}
-
-void mul_batch(const pic_mul_desc* d, size_t count, int mode, cudaStream_t s)
-{
-    for (size_t i = 0; i < count; i++) {
-        PIC_REQUIRE(d[i].z && d[i].a && d[i].b && d[i].na && d[i].nb, PIC_ERR_INVALID, "bad product descriptor");
-        mul_dispatch(d[i].z, d[i].a, (size_t)d[i].na, d[i].b, (size_t)d[i].nb, mode, s);
     }
 }
 

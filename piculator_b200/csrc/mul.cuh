@@ -36,7 +36,10 @@ void ntt3_inverse_to_words(uint64_t* y, int k, size_t ncoef, int depth, uint32_t
 void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
                          uint32_t zcap, const uint32_t* zlen, cudaStream_t s);
 
+// batch.cu: persistent schoolbook + binned three-prime NTT, replayed from a
+// CUDA graph when the sizes repeat.
 void mul_batch(const pic_mul_desc* d, size_t count, int mode, cudaStream_t s);
+void mul_batch_set_graphs(bool on);
 // noalloc.cu: the three-prime product in fixed library storage (no allocation).
 void mul_noalloc(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s);
 

@@ -128,6 +128,7 @@ static const NoallocDevice& noalloc_setup(cudaStream_t s)
         P.K = kNoallocK;
         P.S = kNoallocS;
         P.IB = kInnerBits;
+        P.lazy = 1;  // the three product primes are below 2^62
         P.inner_fwd = t;
         P.inner_inv = t + 2 * kInnerPairs;
         P.olo_fwd = t + 4 * kInnerPairs;

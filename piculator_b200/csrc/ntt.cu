@@ -126,6 +126,7 @@ const PrimeTables& prime_tables(uint64_t p)
     d.K = K;
     d.S = S;
     d.IB = IB;
+    d.lazy = p < (1ull << 62) ? 1 : 0;
     d.inner_fwd = upload(inf);
     d.inner_inv = upload(ini);
     d.olo_fwd = upload(lof);
@@ -136,18 +137,49 @@ const PrimeTables& prime_tables(uint64_t p)
     return *t;
 }
 
+// Per-length geometry (tunable; pic_set_ntt_geometry): row-pass bits, column
+// tile width (log2 columns per CTA, 0 = automatic) and bits per register round
+// (radix 2^rbits).
+struct Geometry {
+    int row_bits = 12;
+    int col_lw = 0;
+    int rbits = 3;
+};
+static Geometry g_geom[33];
+
+void ntt_set_geometry(int k, int row_bits, int col_lw, int rbits)
+{
+    PIC_REQUIRE(k >= 1 && k <= 32, PIC_ERR_INVALID, "k out of range");
+    PIC_REQUIRE(row_bits >= 8 && row_bits <= kInnerBits, PIC_ERR_INVALID, "row bits out of range (8..13)");
+    PIC_REQUIRE(col_lw >= 0 && col_lw <= 6, PIC_ERR_INVALID, "column width out of range (0..6)");
+    PIC_REQUIRE(rbits >= 2 && rbits <= 4, PIC_ERR_INVALID, "radix bits out of range (2..4)");
+    g_geom[k].row_bits = row_bits;
+    g_geom[k].col_lw = col_lw;
+    g_geom[k].rbits = rbits;
+}
+
+void ntt_get_geometry(int k, int* row_bits, int* col_lw, int* rbits)
+{
+    const Geometry& g = g_geom[k < 1 ? 1 : (k > 32 ? 32 : k)];
+    *row_bits = g.row_bits;
+    *col_lw = g.col_lw;
+    *rbits = g.rbits;
+}
+
 std::vector<int> ntt_pass_bits(int k)
 {
+    // One in-CTA pass up to 2^13 points; then column passes of at most 11
+    // bits (balanced) and the row pass.
     std::vector<int> bits;
     if (k <= kInnerBits) {
         bits.push_back(k);
         return bits;
     }
-    const int row = 12, colmax = 10;
+    const int row = g_geom[k].row_bits, colmax = 11;
     int rest = k - row;
-    int ncol = (rest + colmax - 1) / colmax;
+    const int ncol = (rest + colmax - 1) / colmax;
     for (int i = 0; i < ncol; i++) {
-        int b = rest / (ncol - i) + ((rest % (ncol - i)) ? 1 : 0);
+        const int b = rest / (ncol - i) + ((rest % (ncol - i)) ? 1 : 0);
         bits.push_back(b);
         rest -= b;
     }
@@ -155,102 +187,224 @@ std::vector<int> ntt_pass_bits(int k)
     return bits;
 }
 
+// Column tile width for a column pass of 2^lc rows: enough columns that a CTA
+// holds >= 4096 points (every thread busy in every radix-8 round), at least 4
+// (a 32-byte DRAM sector per row), at most 64.
+static int col_width_log2(int lc)
+{
+    int lw = 12 - lc;
+    if (lw < 2) lw = 2;
+    if (lw > 6) lw = 6;
+    return lw;
+}
+
+// Compile-time kernel variants (chosen by measurement; see the profiles):
+// PIC_NTT_PREFETCH loads a radix group's twiddles before its butterflies,
+// PIC_NTT_SWIZZLE XOR-swizzles the row kernel's shared-memory layout.
+#ifndef PIC_NTT_PREFETCH
+#define PIC_NTT_PREFETCH 0
+#endif
+#ifndef PIC_NTT_SWIZZLE
+#define PIC_NTT_SWIZZLE 1
+#endif
+
 // ---------------------------------------------------------------------------
-// In-CTA transform: radix-2^B register groups, shared-memory exchanges.
+// Butterflies.  Strict: operands and results in [0, p).  Lazy (Harvey 2014,
+// primes below 2^62 so 4p < 2^64): operands and results in [0, 2p); the Shoup
+// product is left in [0, 2p) without its final correction.
+
+template <bool LAZY>
+__device__ __forceinline__ void bfly_dif(uint64_t& a, uint64_t& b, uint64_t w, uint64_t ws, uint64_t p)
+{
+    if (LAZY) {
+        const uint64_t p2 = 2 * p;
+        uint64_t x = a + b;
+        x = x >= p2 ? x - p2 : x;
+        const uint64_t t = a + p2 - b;
+        b = t * w - mulhi64(t, ws) * p;
+        a = x;
+    } else {
+        const uint64_t x = a, y = b;
+        a = add_mod(x, y, p);
+        b = shoup_mul(sub_mod(x, y, p), w, ws, p);
+    }
+}
+
+// Butterfly with a unit twiddle (the h = 1 level): no multiplication.
+template <bool LAZY>
+__device__ __forceinline__ void bfly_unit(uint64_t& a, uint64_t& b, uint64_t p)
+{
+    if (LAZY) {
+        const uint64_t p2 = 2 * p;
+        uint64_t x = a + b;
+        x = x >= p2 ? x - p2 : x;
+        uint64_t y = a + p2 - b;
+        y = y >= p2 ? y - p2 : y;
+        a = x;
+        b = y;
+    } else {
+        const uint64_t x = a, y = b;
+        a = add_mod(x, y, p);
+        b = sub_mod(x, y, p);
+    }
+}
+
+template <bool LAZY>
+__device__ __forceinline__ void bfly_dit(uint64_t& a, uint64_t& b, uint64_t w, uint64_t ws, uint64_t p)
+{
+    if (LAZY) {
+        const uint64_t p2 = 2 * p;
+        const uint64_t u = b * w - mulhi64(b, ws) * p;
+        uint64_t x = a + u;
+        x = x >= p2 ? x - p2 : x;
+        uint64_t y = a + p2 - u;
+        y = y >= p2 ? y - p2 : y;
+        a = x;
+        b = y;
+    } else {
+        const uint64_t x = a, y = shoup_mul(b, w, ws, p);
+        a = add_mod(x, y, p);
+        b = sub_mod(x, y, p);
+    }
+}
 
 // One group of 2^B elements at positions base + j + m * 2^lst of a sub-block
-// of size 2^(lst + B); performs the B butterfly levels of that sub-block.
-template <int B, bool INV>
-__device__ __forceinline__ void group_levels(uint64_t (&x)[1 << B], int j, int lst, const PrimeDev& P)
+// of size 2^(lst + B); performs the B butterfly levels of that sub-block.  All
+// 2^B - 1 twiddle pairs of the group are loaded before the first butterfly so
+// their latencies overlap.
+template <int B, bool INV, bool LAZY>
+__device__ __forceinline__ void group_levels(uint64_t (&x)[1 << B], int j, int lst, uint64_t p, int IB,
+                                             const uint64_t* __restrict__ tw)
 {
-    const uint64_t p = P.p;
-    const uint64_t* __restrict__ tw = INV ? P.inner_inv : P.inner_fwd;
+    constexpr int NT = (1 << B) - 1;
+    ulonglong2 w[NT];
+    const bool unit_last = lst == 0;  // the h = 1 level has every twiddle equal to 1
+#if PIC_NTT_PREFETCH
+#pragma unroll
+    for (int l = 0; l < B; l++) {
+        const int hm = 1 << (B - 1 - l);
+        const int off = (1 << B) - (1 << (B - l));
+        if (l == B - 1 && unit_last) continue;
+        const int shift = IB - (B - l) - lst;  // root of order 2h = 2^(B-l+lst)
+#pragma unroll
+        for (int u = 0; u < hm; u++)
+            w[off + u] = __ldg(reinterpret_cast<const ulonglong2*>(tw) + ((j + (u << lst)) << shift));
+    }
+#define PIC_TW(l, u) w[(1 << B) - (1 << (B - (l))) + (u)]
+#else
+#define PIC_TW(l, u) \
+    __ldg(reinterpret_cast<const ulonglong2*>(tw) + ((j + ((u) << lst)) << (IB - (B - (l)) - lst)))
+#endif
     if (!INV) {
 #pragma unroll
         for (int l = 0; l < B; l++) {
             const int hm = 1 << (B - 1 - l);
-            const int shift = P.IB - (B - l) - lst;  // root of order 2h = 2^(B-l+lst)
+            if (l == B - 1 && unit_last) {
+#pragma unroll
+                for (int m = 0; m < (1 << B); m += 2) bfly_unit<LAZY>(x[m], x[m + 1], p);
+                continue;
+            }
 #pragma unroll
             for (int m = 0; m < (1 << B); m++) {
                 if (m & hm) continue;
-                const int t = j + ((m & (hm - 1)) << lst);
-                const int ti = t << shift;
-                const uint64_t w = __ldg(tw + 2 * ti), ws = __ldg(tw + 2 * ti + 1);
-                const uint64_t a = x[m], b = x[m + hm];
-                x[m] = add_mod(a, b, p);
-                x[m + hm] = shoup_mul(sub_mod(a, b, p), w, ws, p);
+                const ulonglong2 t = PIC_TW(l, m & (hm - 1));
+                bfly_dif<LAZY>(x[m], x[m + hm], t.x, t.y, p);
             }
         }
     } else {
 #pragma unroll
         for (int l = B - 1; l >= 0; l--) {
             const int hm = 1 << (B - 1 - l);
-            const int shift = P.IB - (B - l) - lst;
+            if (l == B - 1 && unit_last) {
+#pragma unroll
+                for (int m = 0; m < (1 << B); m += 2) bfly_unit<LAZY>(x[m], x[m + 1], p);
+                continue;
+            }
 #pragma unroll
             for (int m = 0; m < (1 << B); m++) {
                 if (m & hm) continue;
-                const int t = j + ((m & (hm - 1)) << lst);
-                const int ti = t << shift;
-                const uint64_t w = __ldg(tw + 2 * ti), ws = __ldg(tw + 2 * ti + 1);
-                const uint64_t a = x[m], b = shoup_mul(x[m + hm], w, ws, p);
-                x[m] = add_mod(a, b, p);
-                x[m + hm] = sub_mod(a, b, p);
+                const ulonglong2 t = PIC_TW(l, m & (hm - 1));
+                bfly_dit<LAZY>(x[m], x[m + hm], t.x, t.y, p);
             }
         }
     }
+#undef PIC_TW
+    (void)w;
 }
 
-template <int B, bool INV>
-__device__ __forceinline__ void run_group(uint64_t* __restrict__ ptr, int base, int j, int lst, int es,
-                                          const PrimeDev& P)
+// Row layout swizzle: XOR bits 4..7 of an element's index into bits 0..3, a
+// bijection on every row that spreads the small-stride rounds over all
+// shared-memory banks.
+__device__ __forceinline__ int swz(int e)
+{
+#if PIC_NTT_SWIZZLE
+    return e ^ ((e >> 4) & 15);
+#else
+    return e;
+#endif
+}
+
+template <int B, bool INV, bool LAZY, bool SWZ>
+__device__ __forceinline__ void run_group(uint64_t* __restrict__ ptr, int base, int j, int lst, int les,
+                                          uint64_t p, int IB, const uint64_t* tw)
 {
     uint64_t x[1 << B];
 #pragma unroll
-    for (int m = 0; m < (1 << B); m++) x[m] = ptr[(size_t)(base + (m << lst)) * es];
-    group_levels<B, INV>(x, j, lst, P);
+    for (int m = 0; m < (1 << B); m++) {
+        const int e = base + (m << lst);
+        x[m] = ptr[SWZ ? swz(e) : (e << les)];
+    }
+    group_levels<B, INV, LAZY>(x, j, lst, p, IB, tw);
 #pragma unroll
-    for (int m = 0; m < (1 << B); m++) ptr[(size_t)(base + (m << lst)) * es] = x[m];
+    for (int m = 0; m < (1 << B); m++) {
+        const int e = base + (m << lst);
+        ptr[SWZ ? swz(e) : (e << les)] = x[m];
+    }
 }
 
-// nt transforms of size 2^logn in shared memory; element m of transform t
-// lives at s[t * ts + m * es].  tr_fast picks which index consecutive threads
-// walk (transforms for column tiles, elements for rows).
-template <bool INV>
-__device__ void cta_ntt(uint64_t* s, int logn, int nt, int es, int ts, bool tr_fast, const PrimeDev& P)
+// 2^lnt transforms of size 2^logn in shared memory; element m of transform t
+// lives at s[(t << lts) + (m << les)] (SWZ: s[(t << lts) + swz(m)], les = 0).
+// tr_fast: consecutive threads walk transforms (column tiles), else elements
+// (rows).
+template <bool INV, bool LAZY, bool SWZ, int rb>
+__device__ void cta_ntt(uint64_t* s, int logn, int lnt, int les, int lts, bool tr_fast, uint64_t p, int IB,
+                        const uint64_t* tw)
 {
-    const int nfull = logn / 3, rem = logn % 3;
+    const int nfull = logn / rb, rem = logn % rb;
     const int nr = nfull + (rem ? 1 : 0);
     for (int ri = 0; ri < nr; ri++) {
         const int r = INV ? (nr - 1 - ri) : ri;
-        const int b = (r < nfull) ? 3 : rem;
-        const int lB = logn - 3 * r;  // log2 sub-block size
+        const int b = (r < nfull) ? rb : rem;
+        const int lB = logn - rb * r;  // log2 sub-block size
         const int lst = lB - b;       // log2 stride inside the group
         const int lgpt = logn - b;    // log2 groups per transform
-        const int G = nt << lgpt;
+        const int G = 1 << (lnt + lgpt);
         for (int g = threadIdx.x; g < G; g += blockDim.x) {
             int tr, gi;
             if (tr_fast) {
-                tr = g % nt;
-                gi = g / nt;
+                tr = g & ((1 << lnt) - 1);
+                gi = g >> lnt;
             } else {
                 tr = g >> lgpt;
                 gi = g & ((1 << lgpt) - 1);
             }
-            const int sb = gi >> lst, j = gi & ((1 << lst) - 1);
-            const int base = (sb << lB) + j;
-            uint64_t* ptr = s + (size_t)tr * ts;
-            if (b == 3) run_group<3, INV>(ptr, base, j, lst, es, P);
-            else if (b == 2) run_group<2, INV>(ptr, base, j, lst, es, P);
-            else run_group<1, INV>(ptr, base, j, lst, es, P);
+            const int j = gi & ((1 << lst) - 1);
+            const int base = ((gi >> lst) << lB) + j;
+            uint64_t* ptr = s + (tr << lts);
+            if (rb >= 4 && b == 4) run_group<(rb >= 4 ? 4 : 1), INV, LAZY, SWZ>(ptr, base, j, lst, les, p, IB, tw);
+            else if (b == 3) run_group<3, INV, LAZY, SWZ>(ptr, base, j, lst, les, p, IB, tw);
+            else if (b == 2) run_group<2, INV, LAZY, SWZ>(ptr, base, j, lst, les, p, IB, tw);
+            else run_group<1, INV, LAZY, SWZ>(ptr, base, j, lst, les, p, IB, tw);
         }
         __syncthreads();
     }
 }
 
-__device__ __forceinline__ const PrimeDev& prime_of(const NttBatch& B, int i)
+// Constant-index selection keeps the prime's fields in registers (a dynamic
+// index into the kernel's parameter array would spill the array to local memory).
+__device__ __forceinline__ PrimeDev pick_prime(const NttBatch& B, int tr)
 {
-    int q = i / B.per_prime;
-    return B.prime[q];
+    return tr < B.per_prime ? B.prime[0] : (tr < 2 * B.per_prime ? B.prime[1] : B.prime[2]);
 }
 
 // Root of unity w_(2^lM)^e in Montgomery form from the two-level tables.
@@ -264,56 +418,53 @@ __device__ __forceinline__ uint64_t outer_root(const PrimeDev& P, uint64_t e, in
     return mont_mul(__ldg(th + hi), __ldg(tl + lo), P.p, P.pinv_neg);
 }
 
-// Contiguous row pass: rows of 2^lr elements; rpc rows per CTA.
-template <bool INV>
-__global__ void __launch_bounds__(512) ntt_rows_kernel(NttBatch B, int k, int lr, int rpc)
+// Contiguous row pass: rows of 2^lr elements; 2^lrpc rows per CTA.
+template <bool INV, bool LAZY, int RB>
+__global__ void __launch_bounds__(512) ntt_rows_kernel(NttBatch B, int k, int lr, int lrpc)
 {
     extern __shared__ uint64_t smem[];
-    const int n = 1 << lr;
-    const size_t rows_per_tr = (size_t)1 << (k - lr);
-    const size_t row0 = (size_t)blockIdx.x * rpc;
-    const int tr0 = (int)(row0 / rows_per_tr);
-    const PrimeDev& P = prime_of(B, tr0);
-    // load rpc rows (contiguous when rows belong to the same transform)
-    for (int idx = threadIdx.x; idx < rpc * n; idx += blockDim.x) {
-        const size_t row = row0 + idx / n;
-        const int e = idx % n;
-        const size_t tr = row / rows_per_tr, rr = row % rows_per_tr;
-        smem[idx] = B.data[tr * B.stride + (rr << lr) + e];
+    const int lrow = k - lr;  // log2 rows per transform
+    const size_t row0 = (size_t)blockIdx.x << lrpc;
+    const int tr0 = (int)(row0 >> lrow);
+    const PrimeDev P = pick_prime(B, tr0);
+    const int tot = 1 << (lrpc + lr);
+    const size_t rmask = ((size_t)1 << lrow) - 1;
+    const int emask = (1 << lr) - 1;
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        const size_t row = row0 + (idx >> lr);
+        smem[(idx & ~emask) + swz(idx & emask)] =
+            B.data[(row >> lrow) * B.stride + ((row & rmask) << lr) + (idx & emask)];
     }
     __syncthreads();
-    cta_ntt<INV>(smem, lr, rpc, 1, n, false, P);
-    for (int idx = threadIdx.x; idx < rpc * n; idx += blockDim.x) {
-        const size_t row = row0 + idx / n;
-        const int e = idx % n;
-        const size_t tr = row / rows_per_tr, rr = row % rows_per_tr;
-        B.data[tr * B.stride + (rr << lr) + e] = smem[idx];
+    cta_ntt<INV, LAZY, true, RB>(smem, lr, lrpc, 0, lr, false, P.p, P.IB, INV ? P.inner_inv : P.inner_fwd);
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        const size_t row = row0 + (idx >> lr);
+        B.data[(row >> lrow) * B.stride + ((row & rmask) << lr) + (idx & emask)] =
+            smem[(idx & ~emask) + swz(idx & emask)];
     }
 }
 
 // Strided column pass.  The transform is a sequence of 2^lpre outer blocks of
 // 2^(k-lpre) elements; each outer block is an N1 x M tile (N1 = 2^lc rows,
-// M = 2^(k-lpre-lc) columns, row-major).  A CTA owns W columns of one tile.
-template <bool INV>
-__global__ void __launch_bounds__(256) ntt_cols_kernel(NttBatch B, int k, int lpre, int lc, int W)
+// M = 2^(k-lpre-lc) columns, row-major).  A CTA owns 2^lw columns of one tile.
+template <bool INV, bool LAZY, int RB>
+__global__ void __launch_bounds__(256) ntt_cols_kernel(NttBatch B, int k, int lpre, int lc, int lw)
 {
     extern __shared__ uint64_t smem[];
     const int lM = k - lpre - lc;
-    const size_t M = (size_t)1 << lM;
-    const size_t tiles_per_block = M / W;
-    const size_t ctas_per_tr = tiles_per_block << lpre;
+    const int ltiles = lM - lw;  // log2 tiles per outer block
     const size_t cta = blockIdx.x;
-    const int tr = (int)(cta / ctas_per_tr);
-    const size_t rem = cta % ctas_per_tr;
-    const size_t ob = rem / tiles_per_block;
-    const size_t c0 = (rem % tiles_per_block) * W;
-    const PrimeDev& P = prime_of(B, tr);
+    const int tr = (int)(cta >> (ltiles + lpre));
+    const size_t rem = cta & (((size_t)1 << (ltiles + lpre)) - 1);
+    const size_t ob = rem >> ltiles;
+    const size_t c0 = (rem & (((size_t)1 << ltiles) - 1)) << lw;
+    const PrimeDev P = pick_prime(B, tr);
     uint64_t* base = B.data + (size_t)tr * B.stride + (ob << (k - lpre)) + c0;
-    const int N1 = 1 << lc;
+    const int tot = 1 << (lc + lw);
     const int lblock = k - lpre;  // twiddle root order 2^lblock
-
-    for (int idx = threadIdx.x; idx < N1 * W; idx += blockDim.x) {
-        const int m = idx / W, w = idx % W;
+    const int wmask = (1 << lw) - 1;
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        const int m = idx >> lw, w = idx & wmask;
         uint64_t v = base[((size_t)m << lM) + w];
         if (INV) {
             const uint64_t k1 = __brev((unsigned)m) >> (32 - lc);
@@ -322,9 +473,9 @@ __global__ void __launch_bounds__(256) ntt_cols_kernel(NttBatch B, int k, int lp
         smem[idx] = v;
     }
     __syncthreads();
-    cta_ntt<INV>(smem, lc, W, W, 1, true, P);
-    for (int idx = threadIdx.x; idx < N1 * W; idx += blockDim.x) {
-        const int m = idx / W, w = idx % W;
+    cta_ntt<INV, LAZY, false, RB>(smem, lc, lw, lw, 0, true, P.p, P.IB, INV ? P.inner_inv : P.inner_fwd);
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        const int m = idx >> lw, w = idx & wmask;
         uint64_t v = smem[idx];
         if (!INV) {
             const uint64_t k1 = __brev((unsigned)m) >> (32 - lc);
@@ -334,54 +485,78 @@ __global__ void __launch_bounds__(256) ntt_cols_kernel(NttBatch B, int k, int lp
     }
 }
 
-static constexpr int kColW = 8;
+template <typename K>
+static void set_smem(K kern, size_t smem)
+{
+    if (smem > 48 * 1024) PIC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+}
 
 static void launch_rows(bool inv, const NttBatch& b, int k, int lr, cudaStream_t s)
 {
-    const int n = 1 << lr;
-    int rpc = 1;
+    int lrpc = 0;
     if (lr == k) {
         // several whole transforms per CTA when short, never straddling primes
-        rpc = (1 << 11) / n;
-        if (rpc < 1) rpc = 1;
-        while (rpc > 1 && (b.per_prime % rpc)) rpc >>= 1;
+        lrpc = 11 - lr;
+        if (lrpc < 0) lrpc = 0;
+        while (lrpc > 0 && (b.per_prime & ((1 << lrpc) - 1))) lrpc--;
     }
     const size_t rows = (size_t)b.count << (k - lr);
-    const size_t grid = rows / rpc;
+    const size_t grid = rows >> lrpc;
     ProfScope ps(KC_NTT_ROWS, 16.0 * (double)b.count * (double)((size_t)1 << k), s);
-    const size_t smem = (size_t)rpc * n * sizeof(uint64_t);
-    int threads = (rpc * n) / 8;
+    const size_t smem = sizeof(uint64_t) << (lrpc + lr);
+    const int rb = g_geom[k].rbits;
+    int threads = 1 << (lrpc + lr - rb);
     if (threads < 32) threads = 32;
     if (threads > 512) threads = 512;
-    if (inv) {
-        if (smem > 48 * 1024)
-            PIC_CUDA(cudaFuncSetAttribute(ntt_rows_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        ntt_rows_kernel<true><<<(unsigned)grid, threads, smem, s>>>(b, k, lr, rpc);
+    const bool lazy = b.prime[0].lazy != 0;
+#define PIC_ROWS(I, Z, R)                                                                        \
+    do {                                                                                       \
+        set_smem(ntt_rows_kernel<I, Z, R>, smem);                                              \
+        ntt_rows_kernel<I, Z, R><<<(unsigned)grid, threads, smem, s>>>(b, k, lr, lrpc);        \
+    } while (0)
+    if (rb == 4) {
+        if (inv) { if (lazy) PIC_ROWS(true, true, 4); else PIC_ROWS(true, false, 4); }
+        else { if (lazy) PIC_ROWS(false, true, 4); else PIC_ROWS(false, false, 4); }
+    } else if (rb == 2) {
+        if (inv) { if (lazy) PIC_ROWS(true, true, 2); else PIC_ROWS(true, false, 2); }
+        else { if (lazy) PIC_ROWS(false, true, 2); else PIC_ROWS(false, false, 2); }
     } else {
-        if (smem > 48 * 1024)
-            PIC_CUDA(cudaFuncSetAttribute(ntt_rows_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        ntt_rows_kernel<false><<<(unsigned)grid, threads, smem, s>>>(b, k, lr, rpc);
+        if (inv) { if (lazy) PIC_ROWS(true, true, 3); else PIC_ROWS(true, false, 3); }
+        else { if (lazy) PIC_ROWS(false, true, 3); else PIC_ROWS(false, false, 3); }
     }
+#undef PIC_ROWS
     PIC_CHECK_LAUNCH();
     count_launch();
 }
 
 static void launch_cols(bool inv, const NttBatch& b, int k, int lpre, int lc, cudaStream_t s)
 {
-    const int W = kColW;
-    const size_t M = (size_t)1 << (k - lpre - lc);
-    const size_t grid = (size_t)b.count * (M / W) << lpre;
-    const size_t smem = ((size_t)W << lc) * sizeof(uint64_t);
+    int lw = g_geom[k].col_lw ? g_geom[k].col_lw : col_width_log2(lc);
+    const int rb = g_geom[k].rbits;
+    const int lM = k - lpre - lc;
+    if (lc + lw > kInnerBits) lw = kInnerBits - lc;  // tile <= 2^13 points (64 KB)
+    if (lw < 2) lw = 2;
+    if (lw > lM) lw = lM;
+    const size_t grid = (size_t)b.count << (lM - lw + lpre);
+    const size_t smem = sizeof(uint64_t) << (lc + lw);
     ProfScope ps(KC_NTT_COLS, 16.0 * (double)b.count * (double)((size_t)1 << k), s);
-    if (inv) {
-        if (smem > 48 * 1024)
-            PIC_CUDA(cudaFuncSetAttribute(ntt_cols_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        ntt_cols_kernel<true><<<(unsigned)grid, 256, smem, s>>>(b, k, lpre, lc, W);
+    const bool lazy = b.prime[0].lazy != 0;
+#define PIC_COLS(I, Z, R)                                                                          \
+    do {                                                                                         \
+        set_smem(ntt_cols_kernel<I, Z, R>, smem);                                                \
+        ntt_cols_kernel<I, Z, R><<<(unsigned)grid, 256, smem, s>>>(b, k, lpre, lc, lw);          \
+    } while (0)
+    if (rb == 4) {
+        if (inv) { if (lazy) PIC_COLS(true, true, 4); else PIC_COLS(true, false, 4); }
+        else { if (lazy) PIC_COLS(false, true, 4); else PIC_COLS(false, false, 4); }
+    } else if (rb == 2) {
+        if (inv) { if (lazy) PIC_COLS(true, true, 2); else PIC_COLS(true, false, 2); }
+        else { if (lazy) PIC_COLS(false, true, 2); else PIC_COLS(false, false, 2); }
     } else {
-        if (smem > 48 * 1024)
-            PIC_CUDA(cudaFuncSetAttribute(ntt_cols_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        ntt_cols_kernel<false><<<(unsigned)grid, 256, smem, s>>>(b, k, lpre, lc, W);
+        if (inv) { if (lazy) PIC_COLS(true, true, 3); else PIC_COLS(true, false, 3); }
+        else { if (lazy) PIC_COLS(false, true, 3); else PIC_COLS(false, false, 3); }
     }
+#undef PIC_COLS
     PIC_CHECK_LAUNCH();
     count_launch();
 }
@@ -392,8 +567,10 @@ static void check_batch(const NttBatch& b, int k)
     PIC_REQUIRE(b.count > 0 && b.per_prime > 0 && b.count <= b.per_prime * kMaxPrimesPerBatch,
                 PIC_ERR_INVALID, "bad NTT batch");
     PIC_REQUIRE(b.stride >= ((size_t)1 << k), PIC_ERR_INVALID, "NTT batch stride too small");
-    for (int q = 0; q * b.per_prime < b.count; q++)
+    for (int q = 0; q * b.per_prime < b.count; q++) {
         PIC_REQUIRE(b.prime[q].K >= k, PIC_ERR_INVALID, "prime has no root of unity of this order");
+        PIC_REQUIRE(b.prime[q].lazy == b.prime[0].lazy, PIC_ERR_INVALID, "mixed lazy/strict primes in one batch");
+    }
 }
 
 void ntt_forward_dif(const NttBatch& b, int k, cudaStream_t s)
@@ -452,7 +629,7 @@ __global__ void pointwise_mont_kernel(NttBatch B, const uint64_t* __restrict__ o
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total;
          g += (size_t)gridDim.x * blockDim.x) {
         const size_t tr = g >> k, i = g & (n - 1);
-        const PrimeDev& P = prime_of(B, (int)tr);
+        const PrimeDev P = pick_prime(B, (int)tr);
         uint64_t* d = B.data + tr * B.stride + i;
         *d = mont_mul(*d, other[tr * B.stride + i], P.p, P.pinv_neg);
     }

@@ -2,6 +2,8 @@
 // 64-bit primes (< 2^63) on sm_100a.
 //
 // Forward = decimation in frequency, natural order in, bit-reversed order out.
+// For primes below 2^62 outputs are only reduced to [0, 2p) (lazy butterflies);
+// the Montgomery consumers (pointwise products, CRT) accept that range.
 // Inverse = decimation in time, bit-reversed in, natural out, unscaled.
 // A convolution therefore never permutes: forward, pointwise, inverse.  The
 // natural-order NTT of the reference (NNT::NTT, NTT.cpp:191-223) is forward +
@@ -34,6 +36,7 @@ struct PrimeDev {
     int K;        // outer tables cover roots of order 2^K
     int S;        // outer split: e = hi * 2^S + lo
     int IB;       // inner table order bits (min(K, kInnerBits))
+    int lazy;     // 1 when 4p < 2^64: transforms keep values in [0, 2p)
     const uint64_t* inner_fwd;  // (w, w') Shoup pairs, w = root_(2^IB)^i, i < 2^(IB-1)
     const uint64_t* inner_inv;  // same for root^-1
     const uint64_t* olo_fwd;    // Montgomery form root_(2^K)^i, i < 2^S
@@ -84,5 +87,9 @@ void ntt_scale_ninv(uint64_t* T, int k, const PrimeDev& P, cudaStream_t s);
 
 // Pass split used for length 2^k (for reporting / tests).
 std::vector<int> ntt_pass_bits(int k);
+// Tunable geometry per length (row-pass bits 8..13, column tile log2 width
+// 0..6 with 0 = automatic, bits per register round 2..4).
+void ntt_set_geometry(int k, int row_bits, int col_lw, int rbits);
+void ntt_get_geometry(int k, int* row_bits, int* col_lw, int* rbits);
 
 }  // namespace pic

@@ -184,6 +184,8 @@ bool profiling() { return g_prof_on.load(std::memory_order_relaxed); }
 ProfScope::ProfScope(KernelClass c, double bytes, cudaStream_t st) : s(st)
 {
     if (!profiling()) return;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return;
     std::lock_guard<std::mutex> g(g_prof_lock);
     ProfRec r{(int)c, bytes, take_event(), take_event()};
     PIC_CUDA(cudaEventRecord(r.a, st));
