@@ -229,7 +229,8 @@ enum {
     PIC_TUNE_BSR_SCHOOL_MAX = 0, /* children up to this many words: CTA schoolbook merge */
     PIC_TUNE_MUL_SCHOOL_MAX = 1, /* products up to this many words: schoolbook in AUTO */
     PIC_TUNE_MUL_FFT_MAX = 2,    /* products up to this many words: FP64 FFT in AUTO (0: never) */
-    PIC_TUNE_BATCH_GRAPHS = 3    /* 1: pic_mul_batch replays captured CUDA graphs (default) */
+    PIC_TUNE_BATCH_GRAPHS = 3,   /* 1: pic_mul_batch replays captured CUDA graphs (default) */
+    PIC_TUNE_BSR_WRAP = 4        /* 1: binary-splitting NTT merges use wrapped products (default) */
 };
 pic_status pic_set_tuning(int knob, int64_t value);
 int64_t pic_get_tuning(int knob);

@@ -337,7 +337,7 @@ class Transform:
         return DeviceBigFloat(out.value)
 
 
-TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS = range(4)
+TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS, TUNE_BSR_WRAP = range(5)
 
 
 def set_tuning(knob: int, value: int) -> None:

@@ -466,10 +466,11 @@ __global__ void __launch_bounds__(256) merge_school_kernel(MergeArgs m)
 // ---------------------------------------------------------------------------
 // Batched three-prime NTT merge.
 
-// Child slot -> residues: out[(q * n2 + c) * N + j] = piece j of child c0 + c.
+// Child slot -> residues: out[(q * n2 + c) * ostride + j] = piece first + j of
+// child c0 + c, for j < 2^k (pieces past the child's length are zero).
 __global__ void slot_split_kernel(uint64_t* __restrict__ out, const uint32_t* __restrict__ w,
                                   const uint32_t* __restrict__ len, uint32_t cap, size_t c0, size_t n2, int k,
-                                  uint64_t p0, uint64_t p1, uint64_t p2)
+                                  size_t ostride, size_t first, uint64_t p0, uint64_t p1, uint64_t p2)
 {
     const size_t N = (size_t)1 << k;
     const size_t total = n2 * N;
@@ -477,25 +478,27 @@ __global__ void slot_split_kernel(uint64_t* __restrict__ out, const uint32_t* __
         const size_t c = g >> k, j = g & (N - 1);
         const uint32_t n = len[c0 + c];
         const uint32_t* x = w + (c0 + c) * (size_t)cap;
+        const size_t wi = 2 * (first + j);
         uint64_t v = 0;
-        if (2 * j < n) {
-            v = x[2 * j];
-            if (2 * j + 1 < n) v |= (uint64_t)x[2 * j + 1] << 32;
+        if (wi < n) {
+            v = x[wi];
+            if (wi + 1 < n) v |= (uint64_t)x[wi + 1] << 32;
         }
         uint64_t r0 = v, r1 = v, r2 = v;
         while (r0 >= p0) r0 -= p0;
         while (r1 >= p1) r1 -= p1;
         while (r2 >= p2) r2 -= p2;
-        out[(0 * n2 + c) * N + j] = r0;
-        out[(1 * n2 + c) * N + j] = r1;
-        out[(2 * n2 + c) * N + j] = r2;
+        out[(0 * n2 + c) * ostride + j] = r0;
+        out[(1 * n2 + c) * ostride + j] = r1;
+        out[(2 * n2 + c) * ostride + j] = r2;
     }
 }
 
-// For every parent i and prime q (arrays laid out [q][child][N]):
+// For every parent i and prime q (arrays laid out [q][child][stride], the
+// transforms of length 2^k at the start of each item):
 //   T1 = PL QR -> P[2i], T2 = PR RL -> P[2i+1], Q = QL QR -> Q[2i], R = RL RR -> R[2i]
 __global__ void merge_pointwise_kernel(uint64_t* __restrict__ P, uint64_t* __restrict__ Q, uint64_t* __restrict__ R,
-                                       size_t npar, int k, Mod64 m0, Mod64 m1, Mod64 m2)
+                                       size_t npar, int k, size_t stride, Mod64 m0, Mod64 m1, Mod64 m2)
 {
     const size_t N = (size_t)1 << k;
     const size_t total = 3 * npar * N;
@@ -505,12 +508,42 @@ __global__ void merge_pointwise_kernel(uint64_t* __restrict__ P, uint64_t* __res
         const size_t i = r >> k, j = r & (N - 1);
         const Mod64& M = q == 0 ? m0 : (q == 1 ? m1 : m2);
         const size_t base = q * 2 * npar;
-        const size_t L = (base + 2 * i) * N + j, Rr = (base + 2 * i + 1) * N + j;
+        const size_t L = (base + 2 * i) * stride + j, Rr = (base + 2 * i + 1) * stride + j;
         const uint64_t pl = P[L], pr = P[Rr], ql = Q[L], qr = Q[Rr], rl = R[L], rr = R[Rr];
         P[L] = mont_mul(pl, qr, M);
         P[Rr] = mont_mul(pr, rl, M);
         Q[L] = mont_mul(ql, qr, M);
         R[L] = mont_mul(rl, rr, M);
+    }
+}
+
+// Wrapped products.  A product of two operands of at most s pieces has
+// L = 2s - 1 coefficients c_0..c_(L-1).  When L exceeds the main transform
+// length Nm (but s <= Nm), the cyclic product of length Nm holds
+// c_j + c_(Nm+j) for j < W = L - Nm.  The W top coefficients depend only on
+// the operands' top W pieces (indices >= t0 = Nm - s + 1): the product of
+// those pieces, d, gives c_(Nm+j) = d_(W-1+j), and its cyclic length
+// T >= 2W - 1 keeps those indices free of wrap.  For each of the W positions:
+//   y[j] <- y[j] - h (kept nonnegative by adding 2p), y[Nm + j] <- h,
+// with h = d_(W-1+j) * Nm / T so that both halves carry the same scale Nm.
+// y items have stride ystride >= Nm + W; tail items have stride T.  `item`
+// selects which children hold products (all for P, the even ones for Q, R).
+__global__ void wrap_fix_kernel(uint64_t* __restrict__ y, size_t ystride, const uint64_t* __restrict__ tail,
+                                size_t T, size_t nitems, size_t item_mul, size_t nchild, size_t Nm, size_t W,
+                                Mod64 m0, Mod64 m1, Mod64 m2, uint64_t c0, uint64_t c1, uint64_t c2)
+{
+    const size_t total = 3 * nitems * W;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
+        const size_t q = g / (nitems * W);
+        const size_t r = g - q * nitems * W;
+        const size_t it = r / W, j = r - it * W;
+        const Mod64& M = q == 0 ? m0 : (q == 1 ? m1 : m2);
+        const uint64_t cT = q == 0 ? c0 : (q == 1 ? c1 : c2);
+        const size_t child = q * nchild + it * item_mul;
+        const uint64_t h = mont_mul(tail[child * T + W - 1 + j], cT, M);  // < p
+        uint64_t* yi = y + child * ystride;
+        yi[j] = yi[j] + 2 * M.p - h;  // < 4p < 2^64: the CRT reduces any 64-bit input
+        yi[Nm + j] = h;
     }
 }
 
@@ -657,67 +690,166 @@ static inline int ceil_log2_sz(size_t n)
 // The three primes' constants for the pointwise kernel.
 static Mod64 prime_mod(int q) { return make_mod(kProductPrimes[q]); }
 
+static bool g_wrap = true;
+
+// Parameters of one level's batched NTT merge.  Every operand has at most
+// smax = ceil(cmax / 2) 64-bit pieces, every product at most L = 2 smax - 1
+// coefficients.  Plain form: one transform of length 2^ceil_log2(L).  Wrapped
+// form (when L sits just above a power of two): main length Nm = 2^(k-1) plus
+// a tail product of length T >= 2W - 1 over the top W = L - Nm pieces.
+struct MergeShape {
+    int k = 0;          // main transform bits
+    size_t N = 0;       // main length
+    size_t stride = 0;  // item stride of the main arrays (>= N + W)
+    bool wrap = false;
+    int kt = 0;         // tail transform bits
+    size_t T = 0, W = 0, t0 = 0;
+};
+
+static MergeShape merge_shape(uint32_t cmax)
+{
+    MergeShape m;
+    const size_t smax = ((size_t)cmax + 1) / 2;
+    const size_t L = smax ? 2 * smax - 1 : 1;
+    int k = ceil_log2_sz(L);
+    if (k < 2) k = 2;
+    PIC_REQUIRE(k <= 30, PIC_ERR_LENGTH, "binary-splitting node too long for the three-prime NTT");
+    m.k = k;
+    m.N = (size_t)1 << k;
+    m.stride = m.N;
+    const size_t Nm = m.N / 2;
+    if (g_wrap && k >= 4 && smax <= Nm && L > Nm) {
+        const size_t W = L - Nm;
+        int kt = ceil_log2_sz(2 * W - 1);
+        if (kt < 2) kt = 2;
+        if (((size_t)1 << kt) <= Nm / 2) {
+            m.wrap = true;
+            m.k = k - 1;
+            m.N = Nm;
+            m.W = W;
+            m.kt = kt;
+            m.T = (size_t)1 << kt;
+            m.t0 = Nm - smax + 1;
+            m.stride = Nm + ((W + 15) & ~(size_t)15);
+        }
+    }
+    return m;
+}
+
 static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
 {
     const uint32_t ccP = ch.P.cap, ccQ = ch.Q.cap, ccR = ch.R.cap;
     const uint32_t cmax = std::max(ccP, std::max(ccQ, ccR));
-    // 64-bit pieces: a product of two <= cmax-word operands has <= cmax pieces
-    int k = ceil_log2_sz(cmax);
-    if (k < 1) k = 1;
-    PIC_REQUIRE(k <= 30, PIC_ERR_LENGTH, "binary-splitting node too long for the three-prime NTT");
-    const size_t N = (size_t)1 << k;
-    // bytes per parent: three child arrays (P, Q, R of both children) x 3 primes,
-    // plus the two word buffers for P's partial products
-    const size_t per_parent = 3 * 2 * 3 * N * sizeof(uint64_t) + 4 * (size_t)(2 * ccP + ccQ + ccR);
+    const MergeShape sh = merge_shape(cmax);
+    const int k = sh.k;
+    const size_t N = sh.N, ST = sh.stride, T = sh.T;
+    // bytes per parent: three child arrays (P, Q, R of both children) x 3 primes
+    // (main and tail), plus the two word buffers for P's partial products
+    const size_t per_parent =
+        3 * 2 * 3 * (ST + T) * sizeof(uint64_t) + 4 * (size_t)(2 * ccP + ccQ + ccR);
     size_t chunk = mem_budget / per_parent;
     if (chunk < 1) chunk = 1;
     if (chunk > par.count) chunk = par.count;
     const uint64_t P0 = kProductPrimes[0], P1 = kProductPrimes[1], P2 = kProductPrimes[2];
     const Mod64 m0 = prime_mod(0), m1 = prime_mod(1), m2 = prime_mod(2);
     const uint32_t c1 = ccP + ccQ, c2 = ccP + ccR;
+    // tail scale Nm / T in Montgomery form (mont_mul(x, c) = x Nm / T)
+    uint64_t cT[3] = {0, 0, 0};
+    if (sh.wrap)
+        for (int q = 0; q < 3; q++) cT[q] = to_mont((uint64_t)(N / T), kProductPrimes[q]);
+    const size_t ncoef = sh.wrap ? N + sh.W : N;
     for (size_t p0 = 0; p0 < par.count; p0 += chunk) {
         const size_t np = std::min(chunk, par.count - p0);
         const size_t nc = 2 * np, c0 = 2 * p0;
-        DevBuf<uint64_t> bP(3 * nc * N, s), bQ(3 * nc * N, s), bR(3 * nc * N, s);
-        const size_t tot = nc * N;
-        slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bP.get(), ch.P.w.get(), ch.P.len.get(), ccP, c0, nc, k,
-                                                             P0, P1, P2);
-        slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bQ.get(), ch.Q.w.get(), ch.Q.len.get(), ccQ, c0, nc, k,
-                                                             P0, P1, P2);
-        slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bR.get(), ch.R.w.get(), ch.R.len.get(), ccR, c0, nc, k,
-                                                             P0, P1, P2);
-        PIC_CHECK_LAUNCH();
-        count_launch(3);
+        DevBuf<uint64_t> bP(3 * nc * ST, s), bQ(3 * nc * ST, s), bR(3 * nc * ST, s);
+        DevBuf<uint64_t> tP(sh.wrap ? 3 * nc * T : 0, s), tQ(sh.wrap ? 3 * nc * T : 0, s),
+            tR(sh.wrap ? 3 * nc * T : 0, s);
+        {
+            const size_t tot = nc * N;
+            ProfScope ps(KC_SPLIT, 3.0 * (4.0 * (double)nc * cmax + 24.0 * (double)tot), s);
+            slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bP.get(), ch.P.w.get(), ch.P.len.get(), ccP, c0, nc,
+                                                                 k, ST, 0, P0, P1, P2);
+            slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bQ.get(), ch.Q.w.get(), ch.Q.len.get(), ccQ, c0, nc,
+                                                                 k, ST, 0, P0, P1, P2);
+            slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bR.get(), ch.R.w.get(), ch.R.len.get(), ccR, c0, nc,
+                                                                 k, ST, 0, P0, P1, P2);
+            PIC_CHECK_LAUNCH();
+            count_launch(3);
+            if (sh.wrap) {
+                const size_t tt = nc * T;
+                slot_split_kernel<<<grid_for(tt, 256), 256, 0, s>>>(tP.get(), ch.P.w.get(), ch.P.len.get(), ccP, c0,
+                                                                    nc, sh.kt, T, sh.t0, P0, P1, P2);
+                slot_split_kernel<<<grid_for(tt, 256), 256, 0, s>>>(tQ.get(), ch.Q.w.get(), ch.Q.len.get(), ccQ, c0,
+                                                                    nc, sh.kt, T, sh.t0, P0, P1, P2);
+                slot_split_kernel<<<grid_for(tt, 256), 256, 0, s>>>(tR.get(), ch.R.w.get(), ch.R.len.get(), ccR, c0,
+                                                                    nc, sh.kt, T, sh.t0, P0, P1, P2);
+                PIC_CHECK_LAUNCH();
+                count_launch(3);
+            }
+        }
         NttBatch fb;
-        fb.stride = N;
+        fb.stride = ST;
         fb.count = (int)(3 * nc);
         fb.per_prime = (int)nc;
         for (int q = 0; q < 3; q++) fb.prime[q] = prime_tables(kProductPrimes[q]).dev;
-        fb.data = bP.get();
-        ntt_forward_dif(fb, k, s);
-        fb.data = bQ.get();
-        ntt_forward_dif(fb, k, s);
-        fb.data = bR.get();
-        ntt_forward_dif(fb, k, s);
+        NttBatch tb = fb;
+        tb.stride = T;
+        for (uint64_t* d : {bP.get(), bQ.get(), bR.get()}) {
+            fb.data = d;
+            ntt_forward_dif(fb, k, s);
+        }
+        if (sh.wrap)
+            for (uint64_t* d : {tP.get(), tQ.get(), tR.get()}) {
+                tb.data = d;
+                ntt_forward_dif(tb, sh.kt, s);
+            }
         {
-            ProfScope ps(KC_NTT_POINTWISE, 3.0 * 3 * np * N * 80.0 / 8.0, s);
-            merge_pointwise_kernel<<<grid_for(3 * np * N, 256), 256, 0, s>>>(bP.get(), bQ.get(), bR.get(), np, k, m0,
-                                                                           m1, m2);
+            ProfScope ps(KC_NTT_POINTWISE, 3.0 * 3 * np * (double)(N + T) * 80.0 / 8.0, s);
+            merge_pointwise_kernel<<<grid_for(3 * np * N, 256), 256, 0, s>>>(bP.get(), bQ.get(), bR.get(), np, k, ST,
+                                                                           m0, m1, m2);
+            if (sh.wrap)
+                merge_pointwise_kernel<<<grid_for(3 * np * T, 256), 256, 0, s>>>(tP.get(), tQ.get(), tR.get(), np,
+                                                                               sh.kt, T, m0, m1, m2);
             PIC_CHECK_LAUNCH();
-            count_launch();
+            count_launch(sh.wrap ? 2 : 1);
         }
         // inverses: P holds T1, T2 for every parent (all items); Q, R the even items
-        NttBatch ib = fb;
-        ib.data = bP.get();
-        ntt_inverse_dit(ib, k, s);
-        NttBatch eb = fb;
-        eb.stride = 2 * N;
-        eb.count = (int)(3 * np);
-        eb.per_prime = (int)np;
-        eb.data = bQ.get();
-        ntt_inverse_dit(eb, k, s);
-        eb.data = bR.get();
-        ntt_inverse_dit(eb, k, s);
+        {
+            NttBatch ib = fb;
+            ib.data = bP.get();
+            ntt_inverse_dit(ib, k, s);
+            NttBatch eb = fb;
+            eb.stride = 2 * ST;
+            eb.count = (int)(3 * np);
+            eb.per_prime = (int)np;
+            eb.data = bQ.get();
+            ntt_inverse_dit(eb, k, s);
+            eb.data = bR.get();
+            ntt_inverse_dit(eb, k, s);
+        }
+        if (sh.wrap) {
+            NttBatch ib = tb;
+            ib.data = tP.get();
+            ntt_inverse_dit(ib, sh.kt, s);
+            NttBatch eb = tb;
+            eb.stride = 2 * T;
+            eb.count = (int)(3 * np);
+            eb.per_prime = (int)np;
+            eb.data = tQ.get();
+            ntt_inverse_dit(eb, sh.kt, s);
+            eb.data = tR.get();
+            ntt_inverse_dit(eb, sh.kt, s);
+            ProfScope ps(KC_NTT_POINTWISE, 3.0 * 4 * np * (double)sh.W * 24.0, s);
+            const size_t W = sh.W;
+            wrap_fix_kernel<<<grid_for(3 * nc * W, 256), 256, 0, s>>>(bP.get(), ST, tP.get(), T, nc, 1, nc, N, W, m0,
+                                                                      m1, m2, cT[0], cT[1], cT[2]);
+            wrap_fix_kernel<<<grid_for(3 * np * W, 256), 256, 0, s>>>(bQ.get(), ST, tQ.get(), T, np, 2, nc, N, W, m0,
+                                                                      m1, m2, cT[0], cT[1], cT[2]);
+            wrap_fix_kernel<<<grid_for(3 * np * W, 256), 256, 0, s>>>(bR.get(), ST, tR.get(), T, np, 2, nc, N, W, m0,
+                                                                      m1, m2, cT[0], cT[1], cT[2]);
+            PIC_CHECK_LAUNCH();
+            count_launch(3);
+        }
         // CRT + carry into words
         DevBuf<uint32_t> T1(np * c1, s), T2(np * c2, s), l1(np, s), l2(np, s);
         product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.Q.len.get(), p0, np, 0, 1, l1.get());
@@ -728,14 +860,14 @@ static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
                                                              par.R.len.get() + p0);
         PIC_CHECK_LAUNCH();
         count_launch(4);
-        // T1: residues at bP items 2i (stride 2N), T2 at items 2i+1
-        const size_t pstride = nc * N;  // [prime][child][N]
-        ntt3_batch_to_words(bP.get(), 2 * N, pstride, np, k, T1.get(), c1, l1.get(), s);
-        ntt3_batch_to_words(bP.get() + N, 2 * N, pstride, np, k, T2.get(), c2, l2.get(), s);
-        ntt3_batch_to_words(bQ.get(), 2 * N, pstride, np, k, par.Q.w.get() + p0 * par.Q.cap, par.Q.cap,
-                            par.Q.len.get() + p0, s);
-        ntt3_batch_to_words(bR.get(), 2 * N, pstride, np, k, par.R.w.get() + p0 * par.R.cap, par.R.cap,
-                            par.R.len.get() + p0, s);
+        // T1: residues at bP items 2i (stride 2 ST), T2 at items 2i+1
+        const size_t pstride = nc * ST;  // [prime][child][ST]
+        ntt3_batch_to_words(bP.get(), 2 * ST, pstride, np, k, T1.get(), c1, l1.get(), s, ncoef);
+        ntt3_batch_to_words(bP.get() + ST, 2 * ST, pstride, np, k, T2.get(), c2, l2.get(), s, ncoef);
+        ntt3_batch_to_words(bQ.get(), 2 * ST, pstride, np, k, par.Q.w.get() + p0 * par.Q.cap, par.Q.cap,
+                            par.Q.len.get() + p0, s, ncoef);
+        ntt3_batch_to_words(bR.get(), 2 * ST, pstride, np, k, par.R.w.get() + p0 * par.R.cap, par.R.cap,
+                            par.R.len.get() + p0, s, ncoef);
         fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(T1.get(), c1, l1.get(), np);
         fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(T2.get(), c2, l2.get(), np);
         fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(par.Q.w.get() + p0 * par.Q.cap, par.Q.cap,
@@ -797,6 +929,8 @@ static void merge_school(Level& ch, Level& par, cudaStream_t s)
 static uint32_t g_school_max = 600;
 
 void bsr_set_school_threshold(uint32_t words) { g_school_max = words; }
+void bsr_set_wrap(bool on) { g_wrap = on; }
+bool bsr_wrap() { return g_wrap; }
 uint32_t bsr_school_threshold() { return g_school_max; }
 
 static void alloc_level(Level& L, size_t count, uint32_t cP, uint32_t cQ, uint32_t cR, cudaStream_t s)

@@ -10,5 +10,9 @@ namespace pic {
 void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, size_t p);
 void bsr_set_school_threshold(uint32_t words);
 uint32_t bsr_school_threshold();
+// Wrapped products in the NTT merges (main transform at the smaller power of
+// two plus a short tail product); on by default.
+void bsr_set_wrap(bool on);
+bool bsr_wrap();
 
 }  // namespace pic

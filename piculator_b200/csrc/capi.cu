@@ -552,6 +552,7 @@ pic_status pic_set_tuning(int knob, int64_t value)
         case PIC_TUNE_MUL_SCHOOL_MAX: mul_set_thresholds(value, -1); break;
         case PIC_TUNE_MUL_FFT_MAX: mul_set_thresholds(-1, value); break;
         case PIC_TUNE_BATCH_GRAPHS: mul_batch_set_graphs(value != 0); break;
+        case PIC_TUNE_BSR_WRAP: bsr_set_wrap(value != 0); break;
         default: throw Error(PIC_ERR_INVALID, "unknown tuning knob");
         }
     });
@@ -579,6 +580,7 @@ int64_t pic_get_tuning(int knob)
     case PIC_TUNE_MUL_SCHOOL_MAX: return mul_school_max();
     case PIC_TUNE_MUL_FFT_MAX: return mul_fft_max();
     case PIC_TUNE_BATCH_GRAPHS: return 1;
+    case PIC_TUNE_BSR_WRAP: return bsr_wrap() ? 1 : 0;
     }
     return -1;
 }

@@ -180,13 +180,13 @@ __global__ void __launch_bounds__(kCvtThreads) crt3_k1(const uint64_t* __restric
 // Batched: product i has residues at Y + i * istride (+ q * pstride), zlen[i]
 // words out at z + i * zcap; cpp CTAs per product.
 __global__ void __launch_bounds__(kCvtThreads) crt3_batch_k1(const uint64_t* __restrict__ Y, size_t istride,
-                                                             size_t pstride, size_t N, Crt3Consts C,
+                                                             size_t pstride, size_t ncoef, Crt3Consts C,
                                                              uint32_t* __restrict__ z, uint32_t zcap,
                                                              const uint32_t* __restrict__ zlen, size_t cpp,
                                                              uint32_t* agg)
 {
     const size_t prod = blockIdx.x / cpp, lc = blockIdx.x % cpp;
-    crt3_block(Y + prod * istride, pstride, N, C, z + prod * (size_t)zcap, zlen[prod],
+    crt3_block(Y + prod * istride, pstride, ncoef, C, z + prod * (size_t)zcap, zlen[prod],
                (int64_t)lc * (int64_t)kCvtLPC, agg + blockIdx.x);
 }
 
@@ -387,16 +387,17 @@ void ntt3_inverse_to_words(uint64_t* y, int k, size_t ncoef, int depth, uint32_t
 }
 
 void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
-                         uint32_t zcap, const uint32_t* zlen, cudaStream_t s)
+                         uint32_t zcap, const uint32_t* zlen, cudaStream_t s, size_t ncoef)
 {
     if (count == 0) return;
+    if (ncoef == 0) ncoef = (size_t)1 << k;
     const Crt3Consts C = make_crt3(k, 1);
     const size_t cpp = (((size_t)zcap + 1) / 2 + kCvtLPC - 1) / kCvtLPC;
     const size_t nctas = count * cpp;
     DevBuf<uint32_t> agg(nctas, s);
     {
-        ProfScope ps(KC_CRT, (24.0 * ((size_t)1 << k) + 4.0 * zcap) * (double)count, s);
-        crt3_batch_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(y, istride, pstride, (size_t)1 << k, C, z, zcap, zlen,
+        ProfScope ps(KC_CRT, (24.0 * (double)ncoef + 4.0 * zcap) * (double)count, s);
+        crt3_batch_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(y, istride, pstride, ncoef, C, z, zcap, zlen,
                                                               cpp, agg.get());
         PIC_CHECK_LAUNCH();
         count_launch();

@@ -31,10 +31,12 @@ void ntt3_pointwise(uint64_t* a, const uint64_t* b, int k, cudaStream_t s);
 void ntt3_inverse_to_words(uint64_t* y, int k, size_t ncoef, int depth, uint32_t* z, size_t zw, cudaStream_t s);
 
 // Batched inverse output: product i's residues at y + i * istride + q * pstride
-// (length 2^k each, already inverse-transformed, one pointwise Montgomery
-// factor); zlen[i] words into z + i * zcap.
+// (transform length 2^k, already inverse-transformed, one pointwise Montgomery
+// factor); zlen[i] words into z + i * zcap.  ncoef (default 2^k) is the number
+// of coefficients read per product: a wrapped product stores its top
+// coefficients past the transform, at indices 2^k .. ncoef - 1.
 void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
-                         uint32_t zcap, const uint32_t* zlen, cudaStream_t s);
+                         uint32_t zcap, const uint32_t* zlen, cudaStream_t s, size_t ncoef = 0);
 
 // batch.cu: persistent schoolbook + binned three-prime NTT, replayed from a
 // CUDA graph when the sizes repeat.

@@ -17,15 +17,20 @@ def _same(dev, want) -> bool:
             and np.array_equal(got.words, want.words))
 
 
+# (schoolbook threshold, wrapped NTT merges): 8 sends nearly every level
+# through the batched NTT merges, with and without wrapped products.
 @pytest.mark.parametrize("a,b,p", CASES)
-@pytest.mark.parametrize("school_max", [192, 8])
-def test_bsr_vs_oracle(pic, oracle, a, b, p, school_max):
+@pytest.mark.parametrize("school_max,wrap", [(192, 1), (8, 1), (8, 0)])
+def test_bsr_vs_oracle(pic, oracle, a, b, p, school_max, wrap):
     saved = pic.get_tuning(pic.TUNE_BSR_SCHOOL_MAX)
+    saved_wrap = pic.get_tuning(pic.TUNE_BSR_WRAP)
     pic.set_tuning(pic.TUNE_BSR_SCHOOL_MAX, school_max)
+    pic.set_tuning(pic.TUNE_BSR_WRAP, wrap)
     try:
         P, Q, R = pic.bsr(a, b, p, pic.PI_CHOSEN)
     finally:
         pic.set_tuning(pic.TUNE_BSR_SCHOOL_MAX, saved)
+        pic.set_tuning(pic.TUNE_BSR_WRAP, saved_wrap)
     wP, wQ, wR = oracle.bsr(a, b, p)
     assert _same(Q, wQ), "Q"
     assert _same(R, wR), "R"
