@@ -524,7 +524,8 @@ __global__ void merge_pointwise_kernel(uint64_t* __restrict__ P, uint64_t* __res
 // the operands' top W pieces (indices >= t0 = Nm - s + 1): the product of
 // those pieces, d, gives c_(Nm+j) = d_(W-1+j), and its cyclic length
 // T >= 2W - 1 keeps those indices free of wrap.  For each of the W positions:
-//   y[j] <- y[j] - h (kept nonnegative by adding 2p), y[Nm + j] <- h,
+//   y[j] <- y[j] - h (kept nonnegative by adding 2p), y[Nm + j] <- h
+// (inverse outputs arrive in [0, 4p) and are first brought below 2p),
 // with h = d_(W-1+j) * Nm / T so that both halves carry the same scale Nm.
 // y items have stride ystride >= Nm + W; tail items have stride T.  `item`
 // selects which children hold products (all for P, the even ones for Q, R).
@@ -542,7 +543,10 @@ __global__ void wrap_fix_kernel(uint64_t* __restrict__ y, size_t ystride, const 
         const size_t child = q * nchild + it * item_mul;
         const uint64_t h = mont_mul(tail[child * T + W - 1 + j], cT, M);  // < p
         uint64_t* yi = y + child * ystride;
-        yi[j] = yi[j] + 2 * M.p - h;  // < 4p < 2^64: the CRT reduces any 64-bit input
+        const uint64_t p2 = 2 * M.p;
+        uint64_t v = yi[j];  // lazy inverse output, < 4p
+        v = v >= p2 ? v - p2 : v;
+        yi[j] = v + p2 - h;  // < 4p < 2^64: the CRT reduces any 64-bit input
         yi[Nm + j] = h;
     }
 }

@@ -126,13 +126,31 @@ const PrimeTables& prime_tables(uint64_t p)
     d.K = K;
     d.S = S;
     d.IB = IB;
-    d.lazy = p < (1ull << 62) ? 1 : 0;
+    // lazy butterflies need 4p < 2^64 and the c * 2^32 + 1 form (mul_p_lo)
+    d.lazy = (p < (1ull << 62) && (p & 0xffffffffull) == 1) ? 1 : 0;
     d.inner_fwd = upload(inf);
     d.inner_inv = upload(ini);
     d.olo_fwd = upload(lof);
     d.ohi_fwd = upload(hif);
     d.olo_inv = upload(loi);
     d.ohi_inv = upload(hii);
+    if (d.lazy) {
+        // the same outer roots as Shoup pairs (plain value, companion)
+        auto pairs = [&](const std::vector<uint64_t>& mont) {
+            std::vector<uint64_t> v(2 * mont.size());
+            const uint64_t rinv = host_powmod(to_mont(1, p), p - 2, p);  // R^-1 mod p
+            for (size_t i = 0; i < mont.size(); i++) {
+                const uint64_t x = host_mulmod(mont[i], rinv, p);
+                v[2 * i] = x;
+                v[2 * i + 1] = shoup_companion(x, p);
+            }
+            return upload(v);
+        };
+        d.slo_fwd = pairs(lof);
+        d.shi_fwd = pairs(hif);
+        d.slo_inv = pairs(loi);
+        d.shi_inv = pairs(hii);
+    }
     g_tabs[p] = t;
     return *t;
 }
@@ -208,10 +226,37 @@ static int col_width_log2(int lc)
 #define PIC_NTT_SWIZZLE 1
 #endif
 
+#ifndef PIC_NTT_QP1
+#define PIC_NTT_QP1 1
+#endif
+#ifndef PIC_NTT_DIT4
+#define PIC_NTT_DIT4 1
+#endif
+
 // ---------------------------------------------------------------------------
 // Butterflies.  Strict: operands and results in [0, p).  Lazy (Harvey 2014,
-// primes below 2^62 so 4p < 2^64): operands and results in [0, 2p); the Shoup
-// product is left in [0, 2p) without its final correction.
+// primes below 2^62 so 4p < 2^64): forward operands and results in [0, 2p);
+// inverse operands and results in [0, 4p) (PIC_NTT_DIT4: only the even input
+// is brought back below 2p, one correction per butterfly).  The Shoup product
+// is left in [0, 2p) without its final correction, for any 64-bit input.
+
+// q * p mod 2^64.  Lazy primes have the form c * 2^32 + 1, so
+// q p = q + ((q mod 2^32) c) 2^32 (mod 2^64): one 32-bit multiply-add.
+__device__ __forceinline__ uint64_t mul_p_lo(uint64_t q, uint64_t p)
+{
+#if PIC_NTT_QP1
+    const uint32_t c = (uint32_t)(p >> 32);
+    return q + ((uint64_t)((uint32_t)q * c) << 32);
+#else
+    return q * p;
+#endif
+}
+
+// x * w mod p in [0, 2p) (lazy primes), x < 2^64.
+__device__ __forceinline__ uint64_t shoup_lazy(uint64_t x, uint64_t w, uint64_t ws, uint64_t p)
+{
+    return x * w - mul_p_lo(mulhi64(x, ws), p);
+}
 
 template <bool LAZY>
 __device__ __forceinline__ void bfly_dif(uint64_t& a, uint64_t& b, uint64_t w, uint64_t ws, uint64_t p)
@@ -220,8 +265,7 @@ __device__ __forceinline__ void bfly_dif(uint64_t& a, uint64_t& b, uint64_t w, u
         const uint64_t p2 = 2 * p;
         uint64_t x = a + b;
         x = x >= p2 ? x - p2 : x;
-        const uint64_t t = a + p2 - b;
-        b = t * w - mulhi64(t, ws) * p;
+        b = shoup_lazy(a + p2 - b, w, ws, p);
         a = x;
     } else {
         const uint64_t x = a, y = b;
@@ -249,18 +293,41 @@ __device__ __forceinline__ void bfly_unit(uint64_t& a, uint64_t& b, uint64_t p)
     }
 }
 
+// Inverse-direction unit butterfly: lazy operands in [0, 4p).
+template <bool LAZY>
+__device__ __forceinline__ void bfly_unit_dit(uint64_t& a, uint64_t& b, uint64_t p)
+{
+#if PIC_NTT_DIT4
+    if (LAZY) {
+        const uint64_t p2 = 2 * p;
+        const uint64_t x = a >= p2 ? a - p2 : a;
+        const uint64_t y = b >= p2 ? b - p2 : b;
+        a = x + y;
+        b = x + p2 - y;
+        return;
+    }
+#endif
+    bfly_unit<LAZY>(a, b, p);
+}
+
 template <bool LAZY>
 __device__ __forceinline__ void bfly_dit(uint64_t& a, uint64_t& b, uint64_t w, uint64_t ws, uint64_t p)
 {
     if (LAZY) {
         const uint64_t p2 = 2 * p;
-        const uint64_t u = b * w - mulhi64(b, ws) * p;
+        const uint64_t u = shoup_lazy(b, w, ws, p);
+#if PIC_NTT_DIT4
+        const uint64_t x = a >= p2 ? a - p2 : a;
+        a = x + u;
+        b = x + p2 - u;
+#else
         uint64_t x = a + u;
         x = x >= p2 ? x - p2 : x;
         uint64_t y = a + p2 - u;
         y = y >= p2 ? y - p2 : y;
         a = x;
         b = y;
+#endif
     } else {
         const uint64_t x = a, y = shoup_mul(b, w, ws, p);
         a = add_mod(x, y, p);
@@ -317,7 +384,7 @@ __device__ __forceinline__ void group_levels(uint64_t (&x)[1 << B], int j, int l
             const int hm = 1 << (B - 1 - l);
             if (l == B - 1 && unit_last) {
 #pragma unroll
-                for (int m = 0; m < (1 << B); m += 2) bfly_unit<LAZY>(x[m], x[m + 1], p);
+                for (int m = 0; m < (1 << B); m += 2) bfly_unit_dit<LAZY>(x[m], x[m + 1], p);
                 continue;
             }
 #pragma unroll
@@ -485,14 +552,420 @@ __global__ void __launch_bounds__(256) ntt_cols_kernel(NttBatch B, int k, int lp
     }
 }
 
+// ---------------------------------------------------------------------------
+// Fast path for the lazy primes (c * 2^32 + 1 < 2^62, inner tables of order
+// 2^13): every geometry parameter of a pass is a compile-time constant, so the
+// group, stride and twiddle index arithmetic folds away, and the Shoup product
+// is written with explicit 32-bit multiply-adds and carries.
+
+#ifndef PIC_NTT_FAST
+#define PIC_NTT_FAST 1
+#endif
+
+struct LazyPrime {
+    uint64_t p, p2;
+    uint32_t c;  // p = c * 2^32 + 1
+};
+
+__device__ __forceinline__ LazyPrime lazy_prime(const PrimeDev& P)
+{
+    LazyPrime L;
+    L.p = P.p;
+    L.p2 = 2 * P.p;
+    L.c = (uint32_t)(P.p >> 32);
+    return L;
+}
+
+// x * w mod p in [0, 2p) for any x < 2^64 (Shoup, ws = floor(w 2^64 / p)).
+// q = floor(x ws / 2^64) from four 32 x 32 partial products; q p mod 2^64 =
+// q + ((q mod 2^32) c) 2^32.
+__device__ __forceinline__ uint64_t shoup_lazy32(uint64_t x, uint64_t w, uint64_t ws, uint32_t c)
+{
+    const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32);
+    const uint32_t s0 = (uint32_t)ws, s1 = (uint32_t)(ws >> 32);
+    const uint32_t w0 = (uint32_t)w, w1 = (uint32_t)(w >> 32);
+    uint32_t r0, r1;
+    asm("{\n\t.reg .u32 u0, u1, u2, q0, q1;\n\t"
+        "mul.hi.u32 u0, %2, %4;\n\t"
+        "mad.lo.cc.u32 u0, %2, %5, u0;\n\t"
+        "madc.hi.u32 u1, %2, %5, 0;\n\t"
+        "mad.lo.cc.u32 u0, %3, %4, u0;\n\t"
+        "madc.hi.cc.u32 u1, %3, %4, u1;\n\t"
+        "addc.u32 u2, 0, 0;\n\t"
+        "mad.lo.cc.u32 q0, %3, %5, u1;\n\t"
+        "madc.hi.u32 q1, %3, %5, u2;\n\t"
+        "mul.lo.u32 %0, %2, %6;\n\t"
+        "mul.hi.u32 %1, %2, %6;\n\t"
+        "mad.lo.u32 %1, %2, %7, %1;\n\t"
+        "mad.lo.u32 %1, %3, %6, %1;\n\t"
+        "mad.lo.u32 u1, q0, %8, q1;\n\t"
+        "sub.cc.u32 %0, %0, q0;\n\t"
+        "subc.u32 %1, %1, u1;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"(x0), "r"(x1), "r"(s0), "r"(s1), "r"(w0), "r"(w1), "r"(c));
+    return ((uint64_t)r1 << 32) | r0;
+}
+
+// Forward (DIF): operands and results in [0, 2p).
+__device__ __forceinline__ void fbfly_dif(uint64_t& a, uint64_t& b, const ulonglong2 t, const LazyPrime& L)
+{
+    uint64_t x = a + b;
+    x = x >= L.p2 ? x - L.p2 : x;
+    b = shoup_lazy32(a + L.p2 - b, t.x, t.y, L.c);
+    a = x;
+}
+
+__device__ __forceinline__ void fbfly_unit_dif(uint64_t& a, uint64_t& b, const LazyPrime& L)
+{
+    uint64_t x = a + b;
+    x = x >= L.p2 ? x - L.p2 : x;
+    uint64_t y = a + L.p2 - b;
+    y = y >= L.p2 ? y - L.p2 : y;
+    a = x;
+    b = y;
+}
+
+// Inverse (DIT): operands and results in [0, 4p).
+__device__ __forceinline__ void fbfly_dit(uint64_t& a, uint64_t& b, const ulonglong2 t, const LazyPrime& L)
+{
+    const uint64_t u = shoup_lazy32(b, t.x, t.y, L.c);
+    const uint64_t x = a >= L.p2 ? a - L.p2 : a;
+    a = x + u;
+    b = x + L.p2 - u;
+}
+
+__device__ __forceinline__ void fbfly_unit_dit(uint64_t& a, uint64_t& b, const LazyPrime& L)
+{
+    const uint64_t x = a >= L.p2 ? a - L.p2 : a;
+    const uint64_t y = b >= L.p2 ? b - L.p2 : b;
+    a = x + y;
+    b = x + L.p2 - y;
+}
+
+// The B levels of one group (elements base + j + m 2^LST, m < 2^B) with the
+// inner table of order 2^13: the twiddle of butterfly u at group level l is
+// root_(2^(B-l+LST))^(j + u 2^LST) = tw[(j + (u << LST)) << (13 - (B-l) - LST)].
+template <int B, bool INV, int LST>
+__device__ __forceinline__ void group_fast(uint64_t (&x)[1 << B], int j, const LazyPrime& L,
+                                           const ulonglong2* __restrict__ tw)
+{
+    static_assert(B + LST <= 13, "sub-block larger than the inner table");
+    if (!INV) {
+#pragma unroll
+        for (int l = 0; l < B; l++) {
+            const int hm = 1 << (B - 1 - l);
+            if (l == B - 1 && LST == 0) {
+#pragma unroll
+                for (int m = 0; m < (1 << B); m += 2) fbfly_unit_dif(x[m], x[m + 1], L);
+                continue;
+            }
+#pragma unroll
+            for (int m = 0; m < (1 << B); m++) {
+                if (m & hm) continue;
+                const int u = m & (hm - 1);
+                fbfly_dif(x[m], x[m + hm], __ldg(tw + ((j + (u << LST)) << (13 - (B - l) - LST))), L);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int l = B - 1; l >= 0; l--) {
+            const int hm = 1 << (B - 1 - l);
+            if (l == B - 1 && LST == 0) {
+#pragma unroll
+                for (int m = 0; m < (1 << B); m += 2) fbfly_unit_dit(x[m], x[m + 1], L);
+                continue;
+            }
+#pragma unroll
+            for (int m = 0; m < (1 << B); m++) {
+                if (m & hm) continue;
+                const int u = m & (hm - 1);
+                fbfly_dit(x[m], x[m + hm], __ldg(tw + ((j + (u << LST)) << (13 - (B - l) - LST))), L);
+            }
+        }
+    }
+}
+
+// Radix-8 rounds of a 2^LOGN transform (plus one radix-2 or radix-4 round when
+// 3 does not divide LOGN, at the smallest stride); forward rounds run from the
+// largest stride down, inverse rounds the other way.
+template <int LOGN>
+struct RoundPlan {
+    static constexpr int NF = LOGN / 3, REM = LOGN % 3, NR = NF + (REM ? 1 : 0);
+    template <int RR>
+    struct At {
+        static constexpr int B = RR < NF ? 3 : REM;
+        static constexpr int LB = LOGN - 3 * RR;  // log2 sub-block size
+        static constexpr int LST = LB - B;        // log2 stride inside a group
+    };
+};
+
+// Row layout: transform t of the CTA at s + (t << LR), element e at swz(e).
+// With several transforms per CTA (LRPC > 0, single-pass lengths), each
+// group takes the prime of its own transform: a CTA may straddle primes.
+template <bool INV, int LR, int LRPC, int NT, int R>
+__device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const NttBatch& Bt, size_t row0,
+                                                const LazyPrime& L0, const ulonglong2* __restrict__ tw0)
+{
+    using Plan = RoundPlan<LR>;
+    constexpr int RR = INV ? Plan::NR - 1 - R : R;
+    using A = typename Plan::template At<RR>;
+    constexpr int B = A::B, LB = A::LB, LST = A::LST;
+    constexpr int LG = LR - B;  // log2 groups per transform
+    constexpr int G = 1 << (LRPC + LG);
+    static_assert(G % NT == 0, "groups must split evenly over the threads");
+#pragma unroll
+    for (int q = 0; q < G / NT; q++) {
+        const int g = threadIdx.x + q * NT;
+        const int t = g >> LG, gi = g & ((1 << LG) - 1);
+        const int j = gi & ((1 << LST) - 1);
+        const int base = ((gi >> LST) << LB) + j;
+        uint64_t* ptr = s + (t << LR);
+        LazyPrime L = L0;
+        const ulonglong2* tw = tw0;
+        if (LRPC > 0 && row0 + t < (size_t)Bt.count) {  // rows past the batch keep the CTA's prime
+            const PrimeDev Pt = pick_prime(Bt, (int)(row0 + t));
+            L = lazy_prime(Pt);
+            tw = reinterpret_cast<const ulonglong2*>(INV ? Pt.inner_inv : Pt.inner_fwd);
+        }
+        uint64_t x[1 << B];
+#pragma unroll
+        for (int m = 0; m < (1 << B); m++) x[m] = ptr[swz(base + (m << LST))];
+        group_fast<B, INV, LST>(x, j, L, tw);
+#pragma unroll
+        for (int m = 0; m < (1 << B); m++) ptr[swz(base + (m << LST))] = x[m];
+    }
+    __syncthreads();
+    if constexpr (R + 1 < Plan::NR) rows_fast_round<INV, LR, LRPC, NT, R + 1>(s, Bt, row0, L0, tw0);
+}
+
+template <int LR, int LRPC>
+struct RowsFastShape {
+    static constexpr int TOT = 1 << (LR + LRPC);
+    static constexpr int NT = (TOT >> 3) > 512 ? 512 : (TOT >> 3);
+};
+
+// Contiguous row pass: 2^LRPC rows of 2^LR points per CTA.  LRPC > 0 only
+// for single-pass lengths (k = LR, one row per transform); the last CTA may
+// hold fewer than 2^LRPC transforms.
+template <bool INV, int LR, int LRPC>
+__global__ void __launch_bounds__(RowsFastShape<LR, LRPC>::NT, 1024 / RowsFastShape<LR, LRPC>::NT)
+    ntt_rows_fast_kernel(NttBatch B, int k)
+{
+    extern __shared__ uint64_t smem[];
+    constexpr int TOT = RowsFastShape<LR, LRPC>::TOT, NT = RowsFastShape<LR, LRPC>::NT;
+    constexpr int EMASK = (1 << LR) - 1;
+    const int lrow = k - LR;  // log2 rows per transform
+    const size_t rmask = ((size_t)1 << lrow) - 1;
+    const size_t row0 = (size_t)blockIdx.x << LRPC;
+    const size_t nrows = (size_t)B.count << lrow;
+    const PrimeDev P = pick_prime(B, (int)(row0 >> lrow));
+    const LazyPrime L = lazy_prime(P);
+#pragma unroll
+    for (int i = 0; i < TOT / NT; i++) {
+        const int idx = threadIdx.x + i * NT;
+        const size_t row = row0 + (idx >> LR);
+        uint64_t v = 0;
+        if (LRPC == 0 || row < nrows)
+            v = B.data[(row >> lrow) * B.stride + ((row & rmask) << LR) + (idx & EMASK)];
+        smem[(idx & ~EMASK) + swz(idx & EMASK)] = v;
+    }
+    __syncthreads();
+    rows_fast_round<INV, LR, LRPC, NT, 0>(smem, B, row0, L,
+                                          reinterpret_cast<const ulonglong2*>(INV ? P.inner_inv : P.inner_fwd));
+#pragma unroll
+    for (int i = 0; i < TOT / NT; i++) {
+        const int idx = threadIdx.x + i * NT;
+        const size_t row = row0 + (idx >> LR);
+        if (LRPC == 0 || row < nrows)
+            B.data[(row >> lrow) * B.stride + ((row & rmask) << LR) + (idx & EMASK)] =
+                smem[(idx & ~EMASK) + swz(idx & EMASK)];
+    }
+}
+
+// Column tile: 2^LC rows x 2^LW columns, element (m, w) at s[(m << LW) + w];
+// consecutive threads take consecutive columns.
+template <bool INV, int LC, int LW, int R>
+__device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const LazyPrime& L,
+                                                const ulonglong2* __restrict__ tw)
+{
+    using Plan = RoundPlan<LC>;
+    constexpr int RR = INV ? Plan::NR - 1 - R : R;
+    using A = typename Plan::template At<RR>;
+    constexpr int B = A::B, LB = A::LB, LST = A::LST;
+    constexpr int LG = LC - B;  // log2 groups per column
+    constexpr int G = 1 << (LW + LG);
+    constexpr int WMASK = (1 << LW) - 1;
+#pragma unroll
+    for (int g = threadIdx.x; g < G; g += 256) {
+        const int w = g & WMASK, gi = g >> LW;
+        const int j = gi & ((1 << LST) - 1);
+        const int base = ((gi >> LST) << LB) + j;
+        uint64_t x[1 << B];
+#pragma unroll
+        for (int m = 0; m < (1 << B); m++) x[m] = s[((base + (m << LST)) << LW) + w];
+        group_fast<B, INV, LST>(x, j, L, tw);
+#pragma unroll
+        for (int m = 0; m < (1 << B); m++) s[((base + (m << LST)) << LW) + w] = x[m];
+    }
+    __syncthreads();
+    if constexpr (R + 1 < Plan::NR) cols_fast_round<INV, LC, LW, R + 1>(s, L, tw);
+}
+
+// Strided column pass (same tiling as ntt_cols_kernel).  The inter-pass
+// twiddle root_(2^lblock)^((c0 + w) k1) is applied as two Shoup products
+// with the two-level outer tables: forward after the column DIF, inverse
+// before the column DIT.
+template <bool INV, int LC, int LW>
+__global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatch B, int k, int lpre)
+{
+    extern __shared__ uint64_t smem[];
+    constexpr int TOT = 1 << (LC + LW), WMASK = (1 << LW) - 1;
+    const int lM = k - lpre - LC;
+    const int ltiles = lM - LW;
+    const size_t cta = blockIdx.x;
+    const int tr = (int)(cta >> (ltiles + lpre));
+    const size_t rem = cta & (((size_t)1 << (ltiles + lpre)) - 1);
+    const size_t ob = rem >> ltiles;
+    const uint32_t c0 = (uint32_t)((rem & (((size_t)1 << ltiles) - 1)) << LW);
+    const PrimeDev P = pick_prime(B, tr);
+    const LazyPrime L = lazy_prime(P);
+    uint64_t* base = B.data + (size_t)tr * B.stride + (ob << (k - lpre)) + c0;
+    const int esh = P.K - (k - lpre);  // exponents of a root of order 2^(k - lpre), scaled to order 2^K
+    const int S = P.S;
+    const uint64_t smask = ((uint64_t)1 << S) - 1;
+    const ulonglong2* __restrict__ slo = reinterpret_cast<const ulonglong2*>(INV ? P.slo_inv : P.slo_fwd);
+    const ulonglong2* __restrict__ shi = reinterpret_cast<const ulonglong2*>(INV ? P.shi_inv : P.shi_fwd);
+    auto twiddle = [&](uint64_t v, int m, int w) {
+        const uint64_t k1 = __brev((unsigned)m) >> (32 - LC);
+        const uint64_t E = ((uint64_t)(c0 + w) * k1) << esh;
+        const ulonglong2 h = __ldg(shi + (E >> S)), l = __ldg(slo + (E & smask));
+        return shoup_lazy32(shoup_lazy32(v, h.x, h.y, L.c), l.x, l.y, L.c);
+    };
+#pragma unroll 2
+    for (int idx = threadIdx.x; idx < TOT; idx += 256) {
+        const int m = idx >> LW, w = idx & WMASK;
+        uint64_t v = base[((size_t)m << lM) + w];
+        if (INV) v = twiddle(v, m, w);
+        smem[idx] = v;
+    }
+    __syncthreads();
+    cols_fast_round<INV, LC, LW, 0>(smem, L, reinterpret_cast<const ulonglong2*>(INV ? P.inner_inv : P.inner_fwd));
+#pragma unroll 2
+    for (int idx = threadIdx.x; idx < TOT; idx += 256) {
+        const int m = idx >> LW, w = idx & WMASK;
+        uint64_t v = smem[idx];
+        if (!INV) v = twiddle(v, m, w);
+        base[((size_t)m << lM) + w] = v;
+    }
+}
+
 template <typename K>
 static void set_smem(K kern, size_t smem)
 {
     if (smem > 48 * 1024) PIC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 }
 
+// The fast kernels serve batches of lazy primes whose inner tables have order
+// 2^13, with the default radix-8 rounds.
+static bool fast_ok(const NttBatch& b, int k)
+{
+    if (!PIC_NTT_FAST || g_geom[k].rbits != 3) return false;
+    for (int q = 0; q * b.per_prime < b.count; q++)
+        if (!b.prime[q].lazy || b.prime[q].IB != 13 || (q > 0 && (b.prime[q].slo_fwd == nullptr) !=
+                                                                     (b.prime[0].slo_fwd == nullptr)))
+            return false;
+    return true;
+}
+
+constexpr int fast_lrpc(int lr) { return lr < 11 ? 11 - lr : 0; }
+
+template <bool INV, int LR>
+static void launch_rows_fast_t(const NttBatch& b, int k, cudaStream_t s)
+{
+    constexpr int LRPC = fast_lrpc(LR);
+    using Sh = RowsFastShape<LR, LRPC>;
+    const size_t rows = (size_t)b.count << (k - LR);
+    const size_t grid = (rows + ((size_t)1 << LRPC) - 1) >> LRPC;
+    const size_t smem = sizeof(uint64_t) * Sh::TOT;
+    set_smem(ntt_rows_fast_kernel<INV, LR, LRPC>, smem);
+    ntt_rows_fast_kernel<INV, LR, LRPC><<<(unsigned)grid, Sh::NT, smem, s>>>(b, k);
+}
+
+template <bool INV>
+static bool launch_rows_fast(const NttBatch& b, int k, int lr, cudaStream_t s)
+{
+    if (!(lr == k || lr >= 11)) return false;
+    switch (lr) {
+    case 1: launch_rows_fast_t<INV, 1>(b, k, s); break;
+    case 2: launch_rows_fast_t<INV, 2>(b, k, s); break;
+    case 3: launch_rows_fast_t<INV, 3>(b, k, s); break;
+    case 4: launch_rows_fast_t<INV, 4>(b, k, s); break;
+    case 5: launch_rows_fast_t<INV, 5>(b, k, s); break;
+    case 6: launch_rows_fast_t<INV, 6>(b, k, s); break;
+    case 7: launch_rows_fast_t<INV, 7>(b, k, s); break;
+    case 8: launch_rows_fast_t<INV, 8>(b, k, s); break;
+    case 9: launch_rows_fast_t<INV, 9>(b, k, s); break;
+    case 10: launch_rows_fast_t<INV, 10>(b, k, s); break;
+    case 11: launch_rows_fast_t<INV, 11>(b, k, s); break;
+    case 12: launch_rows_fast_t<INV, 12>(b, k, s); break;
+    case 13: launch_rows_fast_t<INV, 13>(b, k, s); break;
+    default: return false;
+    }
+    return true;
+}
+
+template <bool INV, int LC, int LW>
+static void launch_cols_fast_t(const NttBatch& b, int k, int lpre, size_t grid, cudaStream_t s)
+{
+    constexpr size_t smem = sizeof(uint64_t) << (LC + LW);
+    set_smem(ntt_cols_fast_kernel<INV, LC, LW>, smem);
+    ntt_cols_fast_kernel<INV, LC, LW><<<(unsigned)grid, 256, smem, s>>>(b, k, lpre);
+}
+
+template <bool INV, int LC>
+static bool launch_cols_fast_lc(const NttBatch& b, int k, int lpre, int lw, size_t grid, cudaStream_t s)
+{
+    switch (lw) {
+    case 2: if constexpr (LC + 2 <= 13) { launch_cols_fast_t<INV, LC, 2>(b, k, lpre, grid, s); return true; } break;
+    case 3: if constexpr (LC + 3 <= 13) { launch_cols_fast_t<INV, LC, 3>(b, k, lpre, grid, s); return true; } break;
+    case 4: if constexpr (LC + 4 <= 13) { launch_cols_fast_t<INV, LC, 4>(b, k, lpre, grid, s); return true; } break;
+    case 5: if constexpr (LC + 5 <= 13) { launch_cols_fast_t<INV, LC, 5>(b, k, lpre, grid, s); return true; } break;
+    case 6: if constexpr (LC + 6 <= 13) { launch_cols_fast_t<INV, LC, 6>(b, k, lpre, grid, s); return true; } break;
+    default: break;
+    }
+    return false;
+}
+
+template <bool INV>
+static bool launch_cols_fast(const NttBatch& b, int k, int lpre, int lc, int lw, size_t grid, cudaStream_t s)
+{
+    switch (lc) {
+    case 1: return launch_cols_fast_lc<INV, 1>(b, k, lpre, lw, grid, s);
+    case 2: return launch_cols_fast_lc<INV, 2>(b, k, lpre, lw, grid, s);
+    case 3: return launch_cols_fast_lc<INV, 3>(b, k, lpre, lw, grid, s);
+    case 4: return launch_cols_fast_lc<INV, 4>(b, k, lpre, lw, grid, s);
+    case 5: return launch_cols_fast_lc<INV, 5>(b, k, lpre, lw, grid, s);
+    case 6: return launch_cols_fast_lc<INV, 6>(b, k, lpre, lw, grid, s);
+    case 7: return launch_cols_fast_lc<INV, 7>(b, k, lpre, lw, grid, s);
+    case 8: return launch_cols_fast_lc<INV, 8>(b, k, lpre, lw, grid, s);
+    case 9: return launch_cols_fast_lc<INV, 9>(b, k, lpre, lw, grid, s);
+    case 10: return launch_cols_fast_lc<INV, 10>(b, k, lpre, lw, grid, s);
+    case 11: return launch_cols_fast_lc<INV, 11>(b, k, lpre, lw, grid, s);
+    default: return false;
+    }
+}
+
 static void launch_rows(bool inv, const NttBatch& b, int k, int lr, cudaStream_t s)
 {
+    if (fast_ok(b, k)) {
+        ProfScope ps(KC_NTT_ROWS, 16.0 * (double)b.count * (double)((size_t)1 << k), s);
+        if (inv ? launch_rows_fast<true>(b, k, lr, s) : launch_rows_fast<false>(b, k, lr, s)) {
+            PIC_CHECK_LAUNCH();
+            count_launch();
+            return;
+        }
+    }
     int lrpc = 0;
     if (lr == k) {
         // several whole transforms per CTA when short, never straddling primes
@@ -540,6 +1013,12 @@ static void launch_cols(bool inv, const NttBatch& b, int k, int lpre, int lc, cu
     const size_t grid = (size_t)b.count << (lM - lw + lpre);
     const size_t smem = sizeof(uint64_t) << (lc + lw);
     ProfScope ps(KC_NTT_COLS, 16.0 * (double)b.count * (double)((size_t)1 << k), s);
+    if (fast_ok(b, k) && b.prime[0].slo_fwd != nullptr &&
+        (inv ? launch_cols_fast<true>(b, k, lpre, lc, lw, grid, s) : launch_cols_fast<false>(b, k, lpre, lc, lw, grid, s))) {
+        PIC_CHECK_LAUNCH();
+        count_launch();
+        return;
+    }
     const bool lazy = b.prime[0].lazy != 0;
 #define PIC_COLS(I, Z, R)                                                                          \
     do {                                                                                         \

@@ -2,8 +2,9 @@
 // 64-bit primes (< 2^63) on sm_100a.
 //
 // Forward = decimation in frequency, natural order in, bit-reversed order out.
-// For primes below 2^62 outputs are only reduced to [0, 2p) (lazy butterflies);
-// the Montgomery consumers (pointwise products, CRT) accept that range.
+// For primes c * 2^32 + 1 below 2^62 (lazy butterflies) forward outputs are
+// only reduced to [0, 2p) and inverse outputs to [0, 4p); the Montgomery
+// consumers (pointwise products, CRT) accept any 64-bit operand.
 // Inverse = decimation in time, bit-reversed in, natural out, unscaled.
 // A convolution therefore never permutes: forward, pointwise, inverse.  The
 // natural-order NTT of the reference (NNT::NTT, NTT.cpp:191-223) is forward +
@@ -43,6 +44,12 @@ struct PrimeDev {
     const uint64_t* ohi_fwd;    // Montgomery form root_(2^K)^(i 2^S), i < 2^(K-S)
     const uint64_t* olo_inv;
     const uint64_t* ohi_inv;
+    // Lazy primes only (else null): the outer roots as Shoup pairs (w, w'),
+    // same indexing as olo / ohi.
+    const uint64_t* slo_fwd;
+    const uint64_t* shi_fwd;
+    const uint64_t* slo_inv;
+    const uint64_t* shi_inv;
 };
 
 // Host-owned tables for one prime (built once, cached for the process).
