@@ -464,6 +464,225 @@ __global__ void __launch_bounds__(256) merge_school_kernel(MergeArgs m)
 }
 
 // ---------------------------------------------------------------------------
+// Warp-per-parent schoolbook merge for short nodes (every child slot <= 64
+// words): the same arithmetic as merge_school_kernel with warp-wide scans and
+// __syncwarp instead of block barriers, several parents per CTA, and the six
+// child operands fetched with independent loads.
+
+constexpr int kWarpMergeMax = 64;  // largest child slot (words)
+constexpr int kWarpMergeWarps = 8;
+
+// Exclusive warp scan of one (g, p) per lane, lanes in position order.
+__device__ __forceinline__ uint32_t warp_gp_scan(uint32_t gp, uint32_t* total)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t v = gp;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) v = gp_combine(o, v);
+    }
+    uint32_t excl = __shfl_up_sync(0xffffffffu, v, 1);
+    if (lane == 0) excl = kGPIdentity;
+    *total = __shfl_sync(0xffffffffu, v, 31);
+    return excl;
+}
+
+// z[0..na+nb) = a * b in the warp's shared region; col holds 3 (na + nb)
+// words.  Returns the length without the leading zero word (0 if empty).
+__device__ uint32_t warp_mul(const uint32_t* a, uint32_t na, const uint32_t* b, uint32_t nb, uint32_t* z,
+                             uint32_t* col)
+{
+    const int lane = threadIdx.x & 31;
+    if (na == 0 || nb == 0) return 0;
+    const uint32_t zw = na + nb;
+    for (uint32_t c = lane; c < zw; c += 32) {
+        uint64_t lo = 0;
+        uint32_t hi = 0;
+        if (c + 1 < zw) {
+            const uint32_t i_lo = c + 1 > nb ? c + 1 - nb : 0;
+            const uint32_t i_hi = c < na - 1 ? c : na - 1;
+            for (uint32_t i = i_lo; i <= i_hi; i++) {
+                const uint64_t pr = (uint64_t)a[i] * b[c - i];
+                lo += pr;
+                hi += (lo < pr);
+            }
+        }
+        col[3 * c] = (uint32_t)lo;
+        col[3 * c + 1] = (uint32_t)(lo >> 32);
+        col[3 * c + 2] = hi;
+    }
+    __syncwarp();
+    const uint32_t per = (zw + 31) / 32;
+    const uint32_t w0 = lane * per, w1 = min(w0 + per, zw);
+    auto digit = [&](uint32_t w, uint32_t& g) -> uint32_t {
+        uint64_t sw = col[3 * w], sp = 0;
+        if (w >= 1) {
+            sw += col[3 * (w - 1) + 1];
+            sp += col[3 * (w - 1)];
+        }
+        if (w >= 2) {
+            sw += col[3 * (w - 2) + 2];
+            sp += col[3 * (w - 2) + 1];
+        }
+        if (w >= 3) sp += col[3 * (w - 3) + 2];
+        const uint64_t t = (sw & 0xffffffffu) + (sp >> 32);
+        g = (uint32_t)(t >> 32);
+        return (uint32_t)t;
+    };
+    uint32_t gp = kGPIdentity;
+    for (uint32_t w = w0; w < w1; w++) {
+        uint32_t g;
+        const uint32_t d = digit(w, g);
+        gp = gp_combine(gp, g | ((uint32_t)(d == 0xffffffffu) << 1));
+    }
+    uint32_t total;
+    uint32_t cin = warp_gp_scan(gp, &total) & 1u;
+    for (uint32_t w = w0; w < w1; w++) {
+        uint32_t g;
+        const uint32_t d = digit(w, g);
+        z[w] = d + cin;
+        cin = g | ((uint32_t)(d == 0xffffffffu) & cin);
+    }
+    __syncwarp();
+    return z[zw - 1] == 0 ? zw - 1 : zw;
+}
+
+// Signed sum of magnitudes into z (capacity max(na, nb) + 1); the reference's
+// sign dispatch (BigFloat.cpp:288-305) on exact operands.
+__device__ uint32_t warp_signed_add(bool sa, const uint32_t* a, uint32_t na, bool sb, const uint32_t* b, uint32_t nb,
+                                    uint32_t* z, bool* sz)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t n = max(na, nb);
+    auto A = [&](uint32_t i) -> uint32_t { return i < na ? a[i] : 0u; };
+    auto B = [&](uint32_t i) -> uint32_t { return i < nb ? b[i] : 0u; };
+    const bool sub = sa != sb;
+    bool swap = false;
+    if (sub) {
+        unsigned long long mine = 0;
+        for (uint32_t i = lane; i < n; i += 32)
+            if (A(i) != B(i)) mine = i + 1;
+        const uint32_t h = (uint32_t)warp_max_u64(mine);
+        if (h == 0) {
+            *sz = true;
+            return 0;
+        }
+        swap = A(h - 1) < B(h - 1);
+    }
+    const uint32_t per = (n + 31) / 32;
+    const uint32_t w0 = lane * per, w1 = min(w0 + per, n);
+    uint32_t gp = kGPIdentity;
+    for (uint32_t i = w0; i < w1; i++) {
+        const uint32_t x = swap ? B(i) : A(i), y = swap ? A(i) : B(i);
+        uint32_t d, g, p;
+        if (!sub) {
+            const uint64_t s = (uint64_t)x + y;
+            d = (uint32_t)s;
+            g = (uint32_t)(s >> 32);
+            p = d == 0xffffffffu;
+        } else {
+            d = x - y;
+            g = x < y;
+            p = d == 0u;
+        }
+        gp = gp_combine(gp, g | (p << 1));
+    }
+    uint32_t total;
+    uint32_t cin = warp_gp_scan(gp, &total) & 1u;
+    for (uint32_t i = w0; i < w1; i++) {
+        const uint32_t x = swap ? B(i) : A(i), y = swap ? A(i) : B(i);
+        if (!sub) {
+            const uint64_t s = (uint64_t)x + y;
+            const uint32_t d = (uint32_t)s;
+            z[i] = d + cin;
+            cin = (uint32_t)(s >> 32) | ((uint32_t)(d == 0xffffffffu) & cin);
+        } else {
+            const uint32_t d = x - y;
+            z[i] = d - cin;
+            cin = (uint32_t)(x < y) | ((uint32_t)(d == 0u) & cin);
+        }
+    }
+    __syncwarp();
+    if (!sub) {
+        const uint32_t c = total & 1u;
+        if (lane == 0) z[n] = c;
+        __syncwarp();
+        *sz = sa;
+        return n + c;
+    }
+    unsigned long long mine = 0;
+    for (uint32_t i = lane; i < n; i += 32)
+        if (z[i] != 0) mine = i + 1;
+    const uint32_t len = (uint32_t)warp_max_u64(mine);
+    *sz = len == 0 ? true : (swap ? sb : sa);
+    return len;
+}
+
+// Shared words per warp for child slots (cP, cQ, cR).
+__host__ __device__ inline uint32_t warp_merge_words(uint32_t cP, uint32_t cQ, uint32_t cR)
+{
+    return 2 * (cP + cQ + cR) + (cP + cQ) + (cP + cR) + 3 * (cP + cQ);
+}
+
+__global__ void __launch_bounds__(32 * kWarpMergeWarps) merge_warp_kernel(MergeArgs m)
+{
+    extern __shared__ uint32_t sm[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const size_t i = (size_t)blockIdx.x * kWarpMergeWarps + wid;
+    if (i >= m.count) return;  // whole warps leave together
+    uint32_t* base = sm + (size_t)wid * warp_merge_words(m.ccP, m.ccQ, m.ccR);
+    uint32_t* PL = base;
+    uint32_t* QL = PL + m.ccP;
+    uint32_t* RL = QL + m.ccQ;
+    uint32_t* PR = RL + m.ccR;
+    uint32_t* QR = PR + m.ccP;
+    uint32_t* RR = QR + m.ccQ;
+    uint32_t* t1 = RR + m.ccR;
+    uint32_t* t2 = t1 + m.ccP + m.ccQ;
+    uint32_t* col = t2 + m.ccP + m.ccR;
+    const size_t L = 2 * i, R = 2 * i + 1;
+    const uint32_t nPL = m.cPl[L], nQL = m.cQl[L], nRL = m.cRl[L];
+    const uint32_t nPR = m.cPl[R], nQR = m.cQl[R], nRR = m.cRl[R];
+    const bool sL = m.cS[L] != 0, sR = m.cS[R] != 0;
+    // all six operands' loads issued before any is stored
+    for (uint32_t k = lane; k < (uint32_t)kWarpMergeMax; k += 32) {
+        const uint32_t pl = k < nPL ? m.cPw[L * m.ccP + k] : 0u;
+        const uint32_t ql = k < nQL ? m.cQw[L * m.ccQ + k] : 0u;
+        const uint32_t rl = k < nRL ? m.cRw[L * m.ccR + k] : 0u;
+        const uint32_t pr = k < nPR ? m.cPw[R * m.ccP + k] : 0u;
+        const uint32_t qr = k < nQR ? m.cQw[R * m.ccQ + k] : 0u;
+        const uint32_t rr = k < nRR ? m.cRw[R * m.ccR + k] : 0u;
+        if (k < nPL) PL[k] = pl;
+        if (k < nQL) QL[k] = ql;
+        if (k < nRL) RL[k] = rl;
+        if (k < nPR) PR[k] = pr;
+        if (k < nQR) QR[k] = qr;
+        if (k < nRR) RR[k] = rr;
+    }
+    __syncwarp();
+    const uint32_t nQ = warp_mul(QL, nQL, QR, nQR, t1, col);
+    for (uint32_t k = lane; k < nQ; k += 32) m.pQw[i * m.pcQ + k] = t1[k];
+    __syncwarp();
+    const uint32_t nR = warp_mul(RL, nRL, RR, nRR, t1, col);
+    for (uint32_t k = lane; k < nR; k += 32) m.pRw[i * m.pcR + k] = t1[k];
+    __syncwarp();
+    // P = PL QR + PR RL (PI.h:110)
+    const uint32_t n1 = warp_mul(PL, nPL, QR, nQR, t1, col);
+    const uint32_t n2 = warp_mul(PR, nPR, RL, nRL, t2, col);
+    bool sP;
+    uint32_t* pz = col;  // max(n1, n2) + 1 <= 3 (ccP + ccQ)
+    const uint32_t nP = warp_signed_add(sL, t1, n1, sR, t2, n2, pz, &sP);
+    for (uint32_t k = lane; k < nP; k += 32) m.pPw[i * m.pcP + k] = pz[k];
+    if (lane == 0) {
+        m.pPl[i] = nP;
+        m.pQl[i] = nQ;
+        m.pRl[i] = nR;
+        m.pS[i] = sP ? 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Batched three-prime NTT merge.
 
 // Child slot -> residues: out[(q * n2 + c) * ostride + j] = piece first + j of
@@ -695,6 +914,8 @@ static inline int ceil_log2_sz(size_t n)
 static Mod64 prime_mod(int q) { return make_mod(kProductPrimes[q]); }
 
 static bool g_wrap = true;
+static bool g_warp_merge = true;
+static bool g_top_batched = true;
 
 // Parameters of one level's batched NTT merge.  Every operand has at most
 // smax = ceil(cmax / 2) 64-bit pieces, every product at most L = 2 smax - 1
@@ -740,30 +961,47 @@ static MergeShape merge_shape(uint32_t cmax)
     return m;
 }
 
-static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
+// Destinations of the four products of a batch of parents (np of them):
+// T1 = PL QR and T2 = PR RL at T1 + i c1 / T2 + i c2, Q = QL QR and R = RL RR
+// at Q + i cQ / R + i cR, lengths (leading zero word dropped) in l1, l2, lQ,
+// lR.  R == nullptr skips R.
+struct ProductsOut {
+    uint32_t* T1 = nullptr;
+    uint32_t c1 = 0;
+    uint32_t* l1 = nullptr;
+    uint32_t* T2 = nullptr;
+    uint32_t c2 = 0;
+    uint32_t* l2 = nullptr;
+    uint32_t* Q = nullptr;
+    uint32_t cQ = 0;
+    uint32_t* lQ = nullptr;
+    uint32_t* R = nullptr;
+    uint32_t cR = 0;
+    uint32_t* lR = nullptr;
+};
+
+// Bytes of transform storage per parent for a level's NTT merge.
+static size_t ntt_bytes_per_parent(const MergeShape& sh) { return 3 * 2 * 3 * (sh.stride + sh.T) * sizeof(uint64_t); }
+
+// The products of parents [p0, p0 + np) of the level above `ch`: each child
+// operand is transformed once (six forward transforms per parent, four
+// inverse), every product exact.
+static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape& sh, const ProductsOut& o,
+                         cudaStream_t s)
 {
     const uint32_t ccP = ch.P.cap, ccQ = ch.Q.cap, ccR = ch.R.cap;
     const uint32_t cmax = std::max(ccP, std::max(ccQ, ccR));
-    const MergeShape sh = merge_shape(cmax);
     const int k = sh.k;
     const size_t N = sh.N, ST = sh.stride, T = sh.T;
-    // bytes per parent: three child arrays (P, Q, R of both children) x 3 primes
-    // (main and tail), plus the two word buffers for P's partial products
-    const size_t per_parent =
-        3 * 2 * 3 * (ST + T) * sizeof(uint64_t) + 4 * (size_t)(2 * ccP + ccQ + ccR);
-    size_t chunk = mem_budget / per_parent;
-    if (chunk < 1) chunk = 1;
-    if (chunk > par.count) chunk = par.count;
     const uint64_t P0 = kProductPrimes[0], P1 = kProductPrimes[1], P2 = kProductPrimes[2];
     const Mod64 m0 = prime_mod(0), m1 = prime_mod(1), m2 = prime_mod(2);
-    const uint32_t c1 = ccP + ccQ, c2 = ccP + ccR;
+    const bool needR = o.R != nullptr;
     // tail scale Nm / T in Montgomery form (mont_mul(x, c) = x Nm / T)
     uint64_t cT[3] = {0, 0, 0};
     if (sh.wrap)
         for (int q = 0; q < 3; q++) cT[q] = to_mont((uint64_t)(N / T), kProductPrimes[q]);
     const size_t ncoef = sh.wrap ? N + sh.W : N;
-    for (size_t p0 = 0; p0 < par.count; p0 += chunk) {
-        const size_t np = std::min(chunk, par.count - p0);
+    {
         const size_t nc = 2 * np, c0 = 2 * p0;
         DevBuf<uint64_t> bP(3 * nc * ST, s), bQ(3 * nc * ST, s), bR(3 * nc * ST, s);
         DevBuf<uint64_t> tP(sh.wrap ? 3 * nc * T : 0, s), tQ(sh.wrap ? 3 * nc * T : 0, s),
@@ -828,8 +1066,10 @@ static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
             eb.per_prime = (int)np;
             eb.data = bQ.get();
             ntt_inverse_dit(eb, k, s);
-            eb.data = bR.get();
-            ntt_inverse_dit(eb, k, s);
+            if (needR) {
+                eb.data = bR.get();
+                ntt_inverse_dit(eb, k, s);
+            }
         }
         if (sh.wrap) {
             NttBatch ib = tb;
@@ -841,45 +1081,77 @@ static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
             eb.per_prime = (int)np;
             eb.data = tQ.get();
             ntt_inverse_dit(eb, sh.kt, s);
-            eb.data = tR.get();
-            ntt_inverse_dit(eb, sh.kt, s);
+            if (needR) {
+                eb.data = tR.get();
+                ntt_inverse_dit(eb, sh.kt, s);
+            }
             ProfScope ps(KC_NTT_POINTWISE, 3.0 * 4 * np * (double)sh.W * 24.0, s);
             const size_t W = sh.W;
             wrap_fix_kernel<<<grid_for(3 * nc * W, 256), 256, 0, s>>>(bP.get(), ST, tP.get(), T, nc, 1, nc, N, W, m0,
                                                                       m1, m2, cT[0], cT[1], cT[2]);
             wrap_fix_kernel<<<grid_for(3 * np * W, 256), 256, 0, s>>>(bQ.get(), ST, tQ.get(), T, np, 2, nc, N, W, m0,
                                                                       m1, m2, cT[0], cT[1], cT[2]);
-            wrap_fix_kernel<<<grid_for(3 * np * W, 256), 256, 0, s>>>(bR.get(), ST, tR.get(), T, np, 2, nc, N, W, m0,
-                                                                      m1, m2, cT[0], cT[1], cT[2]);
+            if (needR)
+                wrap_fix_kernel<<<grid_for(3 * np * W, 256), 256, 0, s>>>(bR.get(), ST, tR.get(), T, np, 2, nc, N, W,
+                                                                          m0, m1, m2, cT[0], cT[1], cT[2]);
             PIC_CHECK_LAUNCH();
-            count_launch(3);
+            count_launch(needR ? 3 : 2);
         }
-        // CRT + carry into words
-        DevBuf<uint32_t> T1(np * c1, s), T2(np * c2, s), l1(np, s), l2(np, s);
-        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.Q.len.get(), p0, np, 0, 1, l1.get());
-        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.R.len.get(), p0, np, 1, 0, l2.get());
-        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.Q.len.get(), ch.Q.len.get(), p0, np, 0, 1,
-                                                             par.Q.len.get() + p0);
-        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.R.len.get(), ch.R.len.get(), p0, np, 0, 1,
-                                                             par.R.len.get() + p0);
+        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.Q.len.get(), p0, np, 0, 1, o.l1);
+        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.R.len.get(), p0, np, 1, 0, o.l2);
+        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.Q.len.get(), ch.Q.len.get(), p0, np, 0, 1, o.lQ);
+        if (needR)
+            product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.R.len.get(), ch.R.len.get(), p0, np, 0, 1, o.lR);
         PIC_CHECK_LAUNCH();
-        count_launch(4);
+        count_launch(needR ? 4 : 3);
         // T1: residues at bP items 2i (stride 2 ST), T2 at items 2i+1
         const size_t pstride = nc * ST;  // [prime][child][ST]
-        ntt3_batch_to_words(bP.get(), 2 * ST, pstride, np, k, T1.get(), c1, l1.get(), s, ncoef);
-        ntt3_batch_to_words(bP.get() + ST, 2 * ST, pstride, np, k, T2.get(), c2, l2.get(), s, ncoef);
-        ntt3_batch_to_words(bQ.get(), 2 * ST, pstride, np, k, par.Q.w.get() + p0 * par.Q.cap, par.Q.cap,
-                            par.Q.len.get() + p0, s, ncoef);
-        ntt3_batch_to_words(bR.get(), 2 * ST, pstride, np, k, par.R.w.get() + p0 * par.R.cap, par.R.cap,
-                            par.R.len.get() + p0, s, ncoef);
-        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(T1.get(), c1, l1.get(), np);
-        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(T2.get(), c2, l2.get(), np);
-        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(par.Q.w.get() + p0 * par.Q.cap, par.Q.cap,
-                                                         par.Q.len.get() + p0, np);
-        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(par.R.w.get() + p0 * par.R.cap, par.R.cap,
-                                                         par.R.len.get() + p0, np);
+        ntt3_batch_to_words(bP.get(), 2 * ST, pstride, np, k, o.T1, o.c1, o.l1, s, ncoef);
+        ntt3_batch_to_words(bP.get() + ST, 2 * ST, pstride, np, k, o.T2, o.c2, o.l2, s, ncoef);
+        ntt3_batch_to_words(bQ.get(), 2 * ST, pstride, np, k, o.Q, o.cQ, o.lQ, s, ncoef);
+        if (needR) ntt3_batch_to_words(bR.get(), 2 * ST, pstride, np, k, o.R, o.cR, o.lR, s, ncoef);
+        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.T1, o.c1, o.l1, np);
+        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.T2, o.c2, o.l2, np);
+        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.Q, o.cQ, o.lQ, np);
+        if (needR) fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.R, o.cR, o.lR, np);
         PIC_CHECK_LAUNCH();
-        count_launch(4);
+        count_launch(needR ? 4 : 3);
+    }
+    (void)cmax;
+    (void)P0;
+    (void)P1;
+    (void)P2;
+}
+
+static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
+{
+    const uint32_t ccP = ch.P.cap, ccQ = ch.Q.cap, ccR = ch.R.cap;
+    const uint32_t cmax = std::max(ccP, std::max(ccQ, ccR));
+    const MergeShape sh = merge_shape(cmax);
+    // bytes per parent: the transforms plus the two word buffers for P's
+    // partial products
+    const size_t per_parent = ntt_bytes_per_parent(sh) + 4 * (size_t)(2 * ccP + ccQ + ccR);
+    size_t chunk = mem_budget / per_parent;
+    if (chunk < 1) chunk = 1;
+    if (chunk > par.count) chunk = par.count;
+    const uint32_t c1 = ccP + ccQ, c2 = ccP + ccR;
+    for (size_t p0 = 0; p0 < par.count; p0 += chunk) {
+        const size_t np = std::min(chunk, par.count - p0);
+        DevBuf<uint32_t> T1(np * c1, s), T2(np * c2, s), l1(np, s), l2(np, s);
+        ProductsOut o;
+        o.T1 = T1.get();
+        o.c1 = c1;
+        o.l1 = l1.get();
+        o.T2 = T2.get();
+        o.c2 = c2;
+        o.l2 = l2.get();
+        o.Q = par.Q.w.get() + p0 * par.Q.cap;
+        o.cQ = par.Q.cap;
+        o.lQ = par.Q.len.get() + p0;
+        o.R = par.R.w.get() + p0 * par.R.cap;
+        o.cR = par.R.cap;
+        o.lR = par.R.len.get() + p0;
+        ntt_products(ch, p0, np, sh, o, s);
         {
             ProfScope ps(KC_LINEAR, 12.0 * (double)np * (double)c1, s);
             signed_add_kernel<<<(unsigned)np, 256, 0, s>>>(T1.get(), l1.get(), c1, T2.get(), l2.get(), c2,
@@ -922,8 +1194,18 @@ static void merge_school(Level& ch, Level& par, cudaStream_t s)
     if (smem > 48 * 1024)
         PIC_CUDA(cudaFuncSetAttribute(merge_school_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const uint32_t cmax = std::max(m.ccP, std::max(m.ccQ, m.ccR));
-    const int threads = cmax <= 16 ? 32 : (cmax <= 64 ? 64 : (cmax <= 256 ? 128 : 256));
     ProfScope ps(KC_BSR, 4.0 * (double)par.count * 2.0 * (m.ccP + m.ccQ + m.ccR), s);
+    if (cmax <= (uint32_t)kWarpMergeMax && g_warp_merge) {
+        const size_t wsmem = sizeof(uint32_t) * warp_merge_words(m.ccP, m.ccQ, m.ccR) * kWarpMergeWarps;
+        if (wsmem > 48 * 1024)
+            PIC_CUDA(cudaFuncSetAttribute(merge_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
+        const size_t grid = (par.count + kWarpMergeWarps - 1) / kWarpMergeWarps;
+        merge_warp_kernel<<<(unsigned)grid, 32 * kWarpMergeWarps, wsmem, s>>>(m);
+        PIC_CHECK_LAUNCH();
+        count_launch();
+        return;
+    }
+    const int threads = cmax <= 16 ? 32 : (cmax <= 64 ? 64 : (cmax <= 256 ? 128 : 256));
     merge_school_kernel<<<(unsigned)par.count, threads, smem, s>>>(m);
     PIC_CHECK_LAUNCH();
     count_launch();
@@ -954,7 +1236,7 @@ struct TopSource {
 };
 
 static void bsr_top(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, size_t p, int depth,
-                    int stop_depth, TopSource& src)
+                    int stop_depth, TopSource& src, bool need_R = true)
 {
     if (depth == stop_depth) {
         P = src.P[src.next];
@@ -973,10 +1255,124 @@ static void bsr_top(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t 
     bsr_top(P1, Q1, R1, m, b, p, depth + 1, stop_depth, src);
     P = P0.mul(Q1, p).add(P1.mul(R0, p), p);
     Q = Q0.mul(Q1, p);
-    R = R0.mul(R1, p);
+    if (need_R) R = R0.mul(R1, p);
 }
 
-void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, size_t p)
+// One level of the merges above the batched range, the reference's merge with
+// precision p (PI.h:110-112): every operand is chopped to its top p + 2 words
+// as BigFloat::mul does (BigFloat.cpp:337-366), the four products are exact
+// products of the chopped operands computed together (each operand
+// transformed once, wrapped lengths), and P = T1.add(T2, p) with the
+// reference's add.  Children 2i, 2i + 1 -> parent i.  Returns false (and
+// computes nothing) if a Q or R child is negative, which the series never
+// produces.
+static bool top_level_merge(const std::vector<BigFloat>& cP, const std::vector<BigFloat>& cQ,
+                            const std::vector<BigFloat>& cR, size_t p, bool need_R, std::vector<BigFloat>& oP,
+                            std::vector<BigFloat>& oQ, std::vector<BigFloat>& oR, cudaStream_t s)
+{
+    const size_t nc = cP.size(), np = nc / 2;
+    struct View {
+        const uint32_t* T;
+        size_t L;
+        int64_t exp;
+        bool sign;
+    };
+    const size_t pw = p + 2;  // p + YCL_BIGFLOAT_EXTRA_PRECISION (BigFloat.h:6)
+    auto chop = [&](const BigFloat& x) {
+        View v{x.device_words(), x.get_precision(), x.get_exponent(), x.get_sign()};
+        if (p != 0 && v.L > pw) {
+            const size_t c = v.L - pw;
+            v.T += c;
+            v.L = pw;
+            v.exp += (int64_t)c;
+        }
+        return v;
+    };
+    std::vector<View> vP(nc), vQ(nc), vR(nc);
+    uint32_t capP = 1, capQ = 1, capR = 1;
+    for (size_t i = 0; i < nc; i++) {
+        vP[i] = chop(cP[i]);
+        vQ[i] = chop(cQ[i]);
+        vR[i] = chop(cR[i]);
+        if (!vQ[i].sign || !vR[i].sign) return false;
+        capP = std::max<uint32_t>(capP, (uint32_t)vP[i].L);
+        capQ = std::max<uint32_t>(capQ, (uint32_t)vQ[i].L);
+        capR = std::max<uint32_t>(capR, (uint32_t)vR[i].L);
+    }
+    // the children as a batched level
+    Level ch;
+    alloc_level(ch, nc, capP, capQ, capR, s);
+    std::vector<uint32_t> lP(nc), lQ(nc), lR(nc);
+    std::vector<uint8_t> sg(nc);
+    for (size_t i = 0; i < nc; i++) {
+        if (vP[i].L)
+            PIC_CUDA(cudaMemcpyAsync(ch.P.w.get() + i * capP, vP[i].T, 4 * vP[i].L, cudaMemcpyDeviceToDevice, s));
+        if (vQ[i].L)
+            PIC_CUDA(cudaMemcpyAsync(ch.Q.w.get() + i * capQ, vQ[i].T, 4 * vQ[i].L, cudaMemcpyDeviceToDevice, s));
+        if (vR[i].L)
+            PIC_CUDA(cudaMemcpyAsync(ch.R.w.get() + i * capR, vR[i].T, 4 * vR[i].L, cudaMemcpyDeviceToDevice, s));
+        lP[i] = (uint32_t)vP[i].L;
+        lQ[i] = (uint32_t)vQ[i].L;
+        lR[i] = (uint32_t)vR[i].L;
+        sg[i] = vP[i].sign ? 1 : 0;
+    }
+    PIC_CUDA(cudaMemcpyAsync(ch.P.len.get(), lP.data(), 4 * nc, cudaMemcpyHostToDevice, s));
+    PIC_CUDA(cudaMemcpyAsync(ch.Q.len.get(), lQ.data(), 4 * nc, cudaMemcpyHostToDevice, s));
+    PIC_CUDA(cudaMemcpyAsync(ch.R.len.get(), lR.data(), 4 * nc, cudaMemcpyHostToDevice, s));
+    PIC_CUDA(cudaMemcpyAsync(ch.sign.get(), sg.data(), nc, cudaMemcpyHostToDevice, s));
+    // the products, in parent chunks that fit a quarter of the free memory
+    const MergeShape sh = merge_shape(std::max(capP, std::max(capQ, capR)));
+    const uint32_t c1 = capP + capQ, c2 = capP + capR, cq = 2 * capQ, cr = 2 * capR;
+    auto sT1 = alloc_words(np * c1), sT2 = alloc_words(np * c2), sQ = alloc_words(np * cq);
+    std::shared_ptr<WordStore> sR = need_R ? alloc_words(np * cr) : nullptr;
+    DevBuf<uint32_t> lens(4 * np, s);
+    size_t free_b = 0, total_b = 0;
+    PIC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    size_t chunk = std::max<size_t>(free_b / 4, (size_t)1 << 30) / ntt_bytes_per_parent(sh);
+    if (chunk < 1) chunk = 1;
+    for (size_t p0 = 0; p0 < np; p0 += chunk) {
+        const size_t n = std::min(chunk, np - p0);
+        ProductsOut o;
+        o.T1 = sT1->base + p0 * c1;
+        o.c1 = c1;
+        o.l1 = lens.get() + p0;
+        o.T2 = sT2->base + p0 * c2;
+        o.c2 = c2;
+        o.l2 = lens.get() + np + p0;
+        o.Q = sQ->base + p0 * cq;
+        o.cQ = cq;
+        o.lQ = lens.get() + 2 * np + p0;
+        if (need_R) {
+            o.R = sR->base + p0 * cr;
+            o.cR = cr;
+            o.lR = lens.get() + 3 * np + p0;
+        }
+        ntt_products(ch, p0, n, sh, o, s);
+    }
+    std::vector<uint32_t> hl(4 * np, 0);
+    PIC_CUDA(cudaMemcpyAsync(hl.data(), lens.get(), 4 * (need_R ? 4 : 3) * np, cudaMemcpyDeviceToHost, s));
+    PIC_CUDA(cudaStreamSynchronize(s));
+    // BigFloat::mul's result: sign product, exponent sum, empty if an operand is
+    auto product = [&](const View& x, const View& y, const std::shared_ptr<WordStore>& st, const uint32_t* w,
+                       uint32_t L) {
+        if (x.L == 0 || y.L == 0) return BigFloat();
+        return BigFloat::from_device(x.sign == y.sign, x.exp + y.exp, st, w, L);
+    };
+    oP.resize(np);
+    oQ.resize(np);
+    oR.resize(np);
+    for (size_t i = 0; i < np; i++) {
+        const size_t L = 2 * i, R = 2 * i + 1;
+        const BigFloat t1 = product(vP[L], vQ[R], sT1, sT1->base + i * c1, hl[i]);
+        const BigFloat t2 = product(vP[R], vR[L], sT2, sT2->base + i * c2, hl[np + i]);
+        oP[i] = t1.add(t2, p);
+        oQ[i] = product(vQ[L], vQ[R], sQ, sQ->base + i * cq, hl[2 * np + i]);
+        oR[i] = need_R ? product(vR[L], vR[R], sR, sR->base + i * cr, hl[3 * np + i]) : BigFloat();
+    }
+    return true;
+}
+
+void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, size_t p, bool need_root_R)
 {
     cudaStream_t s = ctx().stream;
     const uint32_t T = b - a;
@@ -1080,7 +1476,29 @@ void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, s
         src.R.push_back(BigFloat::from_device(true, 0, sR, sR->base + i * cur.R.cap, lR[i]));
     }
     TraceSpan tspan(s);
-    bsr_top(P, Q, R, a, b, p, 0, Dtop, src);
+    // levels Dtop - 1 .. 0, each as one batched merge of all its parents;
+    // `stop` is the depth the node lists in src hold
+    int stop = Dtop;
+    for (int d = Dtop - 1; d >= 0 && g_top_batched; d--) {
+        std::vector<BigFloat> nP, nQ, nR;
+        TraceSpan lspan(s);
+        if (!top_level_merge(src.P, src.Q, src.R, p, d > 0 || need_root_R, nP, nQ, nR, s)) break;
+        if (tracing())
+            fprintf(stderr, "{\"trace\": \"bsr_top_level\", \"depth\": %d, \"parents\": %zu, \"ms\": %.3f}\n", d,
+                    nP.size(), lspan.end_ms());
+        src.P = std::move(nP);
+        src.Q = std::move(nQ);
+        src.R = std::move(nR);
+        stop = d;
+    }
+    if (stop == 0) {
+        P = src.P[0];
+        Q = src.Q[0];
+        R = src.R[0];
+    } else {
+        src.next = 0;
+        bsr_top(P, Q, R, a, b, p, 0, stop, src, need_root_R);
+    }
     if (tracing())
         fprintf(stderr, "{\"trace\": \"bsr_top\", \"nodes\": %zu, \"depth\": %d, \"ms\": %.3f}\n", cnt, Dtop,
                 tspan.end_ms());

@@ -6,8 +6,11 @@
 
 namespace pic {
 
-// Same P, Q, R as Pi_BSR(P, Q, R, a, b, p) word for word.
-void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, size_t p);
+// Same P, Q, R as Pi_BSR(P, Q, R, a, b, p) word for word.  need_root_R =
+// false skips the root's R = R0 R1, which Pi() never reads (PI.h:176-181);
+// R is then left empty.
+void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, size_t p,
+                bool need_root_R = true);
 void bsr_set_school_threshold(uint32_t words);
 uint32_t bsr_school_threshold();
 // Wrapped products in the NTT merges (main transform at the smaller power of

@@ -100,7 +100,7 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
     try {
         tm.mark();
         if (mode == PIC_PI_PLAIN) bsr_recursive(P, Q, R, 0, (uint32_t)terms, (size_t)p);
-        else bsr_chosen(P, Q, R, 0, (uint32_t)terms, (size_t)p);
+        else bsr_chosen(P, Q, R, 0, (uint32_t)terms, (size_t)p, /*need_root_R=*/false);
         if (tracing()) {
             PIC_CUDA(cudaStreamSynchronize(ctx().stream));
             fprintf(stderr, "{\"trace\": \"bsr_done\"}\n");
