@@ -337,7 +337,8 @@ class Transform:
         return DeviceBigFloat(out.value)
 
 
-TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS, TUNE_BSR_WRAP = range(5)
+(TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS, TUNE_BSR_WRAP,
+ TUNE_BSR_SMALL_MERGE) = range(6)
 
 
 def set_tuning(knob: int, value: int) -> None:

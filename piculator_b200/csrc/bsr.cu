@@ -116,44 +116,61 @@ __device__ __forceinline__ void sw_mul_u32(SW<N>& x, uint32_t m)
             carry >>= 32;
         }
     }
-    if (carry && x.n < N) x.w[x.n++] = (uint32_t)carry;
+    // the carry word lands at index x.n (static indexing keeps x in registers)
+    const int n = x.n;
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        if (i == n && carry) x.w[i] = (uint32_t)carry;
+    if (carry && n < N) x.n = n + 1;
 }
 
+// Canonical length: one past the highest nonzero word (static indexing keeps
+// the words in registers).
+template <int N>
+__device__ __forceinline__ int sw_top(const SW<N>& x)
+{
+    int n = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++)
+        if (x.w[k] != 0) n = k + 1;
+    return n;
+}
+
+// z = a * b over the full capacities (words past a.n / b.n are zero).
 template <int NA, int NB, int NZ>
 __device__ __forceinline__ void sw_mul(const SW<NA>& a, const SW<NB>& b, SW<NZ>& z)
 {
+    static_assert(NZ >= NA + NB, "product capacity");
 #pragma unroll
     for (int i = 0; i < NZ; i++) z.w[i] = 0;
 #pragma unroll
     for (int i = 0; i < NA; i++) {
-        if (i >= a.n) continue;
         uint64_t carry = 0;
 #pragma unroll
         for (int j = 0; j < NB; j++) {
-            if (j >= b.n) continue;
             carry += (uint64_t)a.w[i] * b.w[j] + z.w[i + j];
             z.w[i + j] = (uint32_t)carry;
             carry >>= 32;
         }
-        if (i + b.n < NZ) z.w[i + b.n] = (uint32_t)carry;
+        z.w[i + NB] = (uint32_t)carry;
     }
-    int n = (a.n && b.n) ? a.n + b.n : 0;
-    if (n > NZ) n = NZ;
-    while (n > 0 && z.w[n - 1] == 0) n--;
-    z.n = n;
+    z.n = sw_top(z);
 }
 
+// -1, 0, 1 as a <, ==, > b: the highest differing word decides.
 template <int N>
 __device__ __forceinline__ int sw_cmp(const SW<N>& a, const SW<N>& b)
 {
-    for (int i = N - 1; i >= 0; i--) {
-        if (a.w[i] != b.w[i]) return a.w[i] < b.w[i] ? -1 : 1;
-    }
-    return 0;
+    int c = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        if (a.w[i] != b.w[i]) c = a.w[i] < b.w[i] ? -1 : 1;
+    return c;
 }
 
 // Signed sum: (sa, a) + (sb, b) -> (sz, z), the reference's add with
-// sign dispatch (BigFloat.cpp:288-305) on exact integers.
+// sign dispatch (BigFloat.cpp:288-305) on exact integers.  N must leave room
+// for the carry word.
 template <int N>
 __device__ __forceinline__ void sw_signed_add(bool sa, const SW<N>& a, bool sb, const SW<N>& b, bool& sz, SW<N>& z)
 {
@@ -168,21 +185,18 @@ __device__ __forceinline__ void sw_signed_add(bool sa, const SW<N>& a, bool sb, 
         sz = sa;
     } else {
         const int c = sw_cmp(a, b);
-        const SW<N>& big = c >= 0 ? a : b;
-        const SW<N>& sml = c >= 0 ? b : a;
         uint32_t br = 0;
 #pragma unroll
         for (int i = 0; i < N; i++) {
-            const uint64_t d = (uint64_t)big.w[i] - sml.w[i] - br;
+            const uint32_t x = c >= 0 ? a.w[i] : b.w[i], y = c >= 0 ? b.w[i] : a.w[i];
+            const uint64_t d = (uint64_t)x - y - br;
             z.w[i] = (uint32_t)d;
             br = (uint32_t)(d >> 63);
         }
         sz = c > 0 ? sa : (c < 0 ? sb : true);
     }
-    int n = N;
-    while (n > 0 && z.w[n - 1] == 0) n--;
-    z.n = n;
-    if (n == 0) sz = true;
+    z.n = sw_top(z);
+    if (z.n == 0) sz = true;
 }
 
 // Leaf b (PI.h:67-88).
@@ -213,7 +227,9 @@ __device__ __forceinline__ void leaf(uint32_t b, LeafV& v)
 template <int N>
 __device__ __forceinline__ void store_sw(const SW<N>& x, uint32_t* slot, uint32_t cap, uint32_t* len)
 {
-    for (int i = 0; i < (int)cap && i < N; i++) slot[i] = x.w[i];
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        if (i < (int)cap) slot[i] = x.w[i];
     *len = (uint32_t)x.n;
 }
 
@@ -461,6 +477,88 @@ __global__ void __launch_bounds__(256) merge_school_kernel(MergeArgs m)
         m.pRl[i] = nR;
         m.pS[i] = sP ? 1 : 0;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Thread-per-parent merge for the shortest nodes: every operand and product
+// in registers (fixed capacities CP, CQ, CR >= the child slots), fully
+// unrolled word loops, the same results as merge_school_kernel.
+
+template <int N>
+__device__ __forceinline__ void sw_load(SW<N>& x, const uint32_t* __restrict__ w, uint32_t cap,
+                                        const uint32_t* __restrict__ len, size_t c)
+{
+    const int n = (int)len[c];
+    const uint32_t* src = w + c * (size_t)cap;
+#pragma unroll
+    for (int k = 0; k < N; k++) x.w[k] = k < n ? src[k] : 0u;
+    x.n = n;
+}
+
+template <int NA, int NB>
+__device__ __forceinline__ void sw_widen(const SW<NA>& a, SW<NB>& b)
+{
+#pragma unroll
+    for (int k = 0; k < NB; k++) b.w[k] = k < NA ? a.w[k] : 0u;
+    b.n = a.n;
+}
+
+template <int CP, int CQ, int CR>
+__global__ void __launch_bounds__(128) merge_thread_kernel(MergeArgs m)
+{
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= m.count) return;
+    const size_t L = 2 * i, R = 2 * i + 1;
+    {
+        SW<CQ> a, b;
+        sw_load(a, m.cQw, m.ccQ, m.cQl, L);
+        sw_load(b, m.cQw, m.ccQ, m.cQl, R);
+        SW<2 * CQ> z;
+        sw_mul(a, b, z);
+        store_sw(z, m.pQw + i * m.pcQ, m.pcQ, m.pQl + i);
+    }
+    {
+        SW<CR> a, b;
+        sw_load(a, m.cRw, m.ccR, m.cRl, L);
+        sw_load(b, m.cRw, m.ccR, m.cRl, R);
+        SW<2 * CR> z;
+        sw_mul(a, b, z);
+        store_sw(z, m.pRw + i * m.pcR, m.pcR, m.pRl + i);
+    }
+    // P = PL QR + PR RL (PI.h:110)
+    constexpr int NP = CP + CQ + 1;
+    SW<NP> t1, t2;
+    {
+        SW<CP> a;
+        SW<CQ> b;
+        sw_load(a, m.cPw, m.ccP, m.cPl, L);
+        sw_load(b, m.cQw, m.ccQ, m.cQl, R);
+        SW<CP + CQ> z;
+        sw_mul(a, b, z);
+        sw_widen(z, t1);
+    }
+    {
+        SW<CP> a;
+        SW<CR> b;
+        sw_load(a, m.cPw, m.ccP, m.cPl, R);
+        sw_load(b, m.cRw, m.ccR, m.cRl, L);
+        SW<CP + CR> z;
+        sw_mul(a, b, z);
+        sw_widen(z, t2);
+    }
+    bool sP;
+    SW<NP> P;
+    sw_signed_add(m.cS[L] != 0, t1, m.cS[R] != 0, t2, sP, P);
+    store_sw(P, m.pPw + i * m.pcP, m.pcP, m.pPl + i);
+    m.pS[i] = sP ? 1 : 0;
+}
+
+template <int CP, int CQ, int CR>
+static bool launch_merge_thread(const MergeArgs& m, cudaStream_t s)
+{
+    if (m.ccP > (uint32_t)CP || m.ccQ > (uint32_t)CQ || m.ccR > (uint32_t)CR) return false;
+    merge_thread_kernel<CP, CQ, CR><<<(unsigned)((m.count + 127) / 128), 128, 0, s>>>(m);
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -914,7 +1012,7 @@ static inline int ceil_log2_sz(size_t n)
 static Mod64 prime_mod(int q) { return make_mod(kProductPrimes[q]); }
 
 static bool g_wrap = true;
-static bool g_warp_merge = true;
+static int g_small_merge = 2;  // 0: CTA schoolbook, 1: + warp per parent, 2: + thread per parent
 static bool g_top_batched = true;
 
 // Parameters of one level's batched NTT merge.  Every operand has at most
@@ -1195,7 +1293,13 @@ static void merge_school(Level& ch, Level& par, cudaStream_t s)
         PIC_CUDA(cudaFuncSetAttribute(merge_school_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const uint32_t cmax = std::max(m.ccP, std::max(m.ccQ, m.ccR));
     ProfScope ps(KC_BSR, 4.0 * (double)par.count * 2.0 * (m.ccP + m.ccQ + m.ccR), s);
-    if (cmax <= (uint32_t)kWarpMergeMax && g_warp_merge) {
+    if (g_small_merge >= 2 && (launch_merge_thread<16, 16, 12>(m, s) || launch_merge_thread<20, 20, 14>(m, s) ||
+                               launch_merge_thread<28, 28, 20>(m, s))) {
+        PIC_CHECK_LAUNCH();
+        count_launch();
+        return;
+    }
+    if (cmax <= (uint32_t)kWarpMergeMax && g_small_merge >= 1) {
         const size_t wsmem = sizeof(uint32_t) * warp_merge_words(m.ccP, m.ccQ, m.ccR) * kWarpMergeWarps;
         if (wsmem > 48 * 1024)
             PIC_CUDA(cudaFuncSetAttribute(merge_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
@@ -1216,6 +1320,8 @@ static uint32_t g_school_max = 600;
 
 void bsr_set_school_threshold(uint32_t words) { g_school_max = words; }
 void bsr_set_wrap(bool on) { g_wrap = on; }
+void bsr_set_small_merge(int mode) { g_small_merge = mode; }
+int bsr_small_merge() { return g_small_merge; }
 bool bsr_wrap() { return g_wrap; }
 uint32_t bsr_school_threshold() { return g_school_max; }
 

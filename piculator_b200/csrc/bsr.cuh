@@ -17,5 +17,10 @@ uint32_t bsr_school_threshold();
 // two plus a short tail product); on by default.
 void bsr_set_wrap(bool on);
 bool bsr_wrap();
+// Kernels for the short schoolbook levels: 0 one CTA per parent, 1 also one
+// warp per parent (nodes <= 64 words), 2 also one thread per parent (nodes
+// <= 28 words, the default).
+void bsr_set_small_merge(int mode);
+int bsr_small_merge();
 
 }  // namespace pic

@@ -20,17 +20,19 @@ def _same(dev, want) -> bool:
 # (schoolbook threshold, wrapped NTT merges): 8 sends nearly every level
 # through the batched NTT merges, with and without wrapped products.
 @pytest.mark.parametrize("a,b,p", CASES)
-@pytest.mark.parametrize("school_max,wrap", [(192, 1), (8, 1), (8, 0)])
-def test_bsr_vs_oracle(pic, oracle, a, b, p, school_max, wrap):
-    saved = pic.get_tuning(pic.TUNE_BSR_SCHOOL_MAX)
-    saved_wrap = pic.get_tuning(pic.TUNE_BSR_WRAP)
-    pic.set_tuning(pic.TUNE_BSR_SCHOOL_MAX, school_max)
-    pic.set_tuning(pic.TUNE_BSR_WRAP, wrap)
+# Small-merge modes: 2 = thread, warp and CTA kernels (by node size), 0 = CTA
+# kernel for every schoolbook level.
+@pytest.mark.parametrize("school_max,wrap,small", [(192, 1, 2), (192, 1, 0), (8, 1, 2), (8, 0, 2)])
+def test_bsr_vs_oracle(pic, oracle, a, b, p, school_max, wrap, small):
+    knobs = {pic.TUNE_BSR_SCHOOL_MAX: school_max, pic.TUNE_BSR_WRAP: wrap, pic.TUNE_BSR_SMALL_MERGE: small}
+    saved = {k: pic.get_tuning(k) for k in knobs}
+    for k, v in knobs.items():
+        pic.set_tuning(k, v)
     try:
         P, Q, R = pic.bsr(a, b, p, pic.PI_CHOSEN)
     finally:
-        pic.set_tuning(pic.TUNE_BSR_SCHOOL_MAX, saved)
-        pic.set_tuning(pic.TUNE_BSR_WRAP, saved_wrap)
+        for k, v in saved.items():
+            pic.set_tuning(k, v)
     wP, wQ, wR = oracle.bsr(a, b, p)
     assert _same(Q, wQ), "Q"
     assert _same(R, wR), "R"
