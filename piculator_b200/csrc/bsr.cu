@@ -1001,6 +1001,182 @@ __global__ void __launch_bounds__(256) signed_add_kernel(const uint32_t* __restr
     }
 }
 
+// ---- the same signed sum spread over many CTAs per parent -------------------
+// For levels with few, long parents: one CTA per (parent, chunk of kWideWPC
+// words), the chunks' carries (or borrows) joined by a segmented scan.
+//   wide_cmp:    highest differing word of |T1|, |T2| per parent (atomicMax)
+//   wide_k1:     chunk digits with in-chunk carries, chunk (G, P) aggregate
+//   (carry_scan_segments: carry-in per chunk)
+//   wide_ripple: +1 / -1 rippled into chunks with a carry-in
+//   wide_final:  length (highest nonzero word, atomicMax), carry word, sign
+constexpr int kWideIPT = 8;
+constexpr uint32_t kWideWPC = 256 * kWideIPT;
+
+struct WideAdd {
+    const uint32_t *t1, *l1, *t2, *l2;
+    uint32_t c1, c2;
+    const uint8_t* cS;  // children's P signs
+    size_t c0;          // first parent (level index)
+    uint32_t *Pw, *Pl, cP;
+    uint8_t* Ps;
+    uint32_t* hd;    // per parent: highest differing word + 1
+    uint32_t* agg;   // per (parent, chunk): (G, P), then carry-in
+    uint32_t* aggc;  // per (parent, chunk): (G, P) kept for the final carry
+    uint32_t cpp;    // chunks per parent
+};
+
+struct WideOp {
+    bool sub, swap, zero;
+};
+
+__device__ __forceinline__ WideOp wide_op(const WideAdd& w, size_t i)
+{
+    WideOp o;
+    const bool sa = w.cS[2 * (w.c0 + i)] != 0, sb = w.cS[2 * (w.c0 + i) + 1] != 0;
+    o.sub = sa != sb;
+    o.swap = false;
+    o.zero = false;
+    if (o.sub) {
+        const uint32_t h = w.hd[i];
+        if (h == 0) {
+            o.zero = true;
+        } else {
+            const uint32_t na = w.l1[i], nb = w.l2[i];
+            const uint32_t x = h - 1 < na ? w.t1[i * (size_t)w.c1 + h - 1] : 0u;
+            const uint32_t y = h - 1 < nb ? w.t2[i * (size_t)w.c2 + h - 1] : 0u;
+            o.swap = x < y;
+        }
+    }
+    return o;
+}
+
+__global__ void __launch_bounds__(256) wide_cmp_kernel(WideAdd w)
+{
+    const size_t i = blockIdx.x / w.cpp, c = blockIdx.x % w.cpp;
+    const uint32_t na = w.l1[i], nb = w.l2[i], n = max(na, nb);
+    const uint32_t b0 = (uint32_t)c * kWideWPC;
+    if (b0 >= n) return;
+    const uint32_t* a = w.t1 + i * (size_t)w.c1;
+    const uint32_t* b = w.t2 + i * (size_t)w.c2;
+    unsigned long long mine = 0;
+    for (uint32_t k = b0 + threadIdx.x; k < b0 + kWideWPC && k < n; k += blockDim.x) {
+        const uint32_t x = k < na ? a[k] : 0u, y = k < nb ? b[k] : 0u;
+        if (x != y) mine = k + 1;
+    }
+    mine = warp_max_u64(mine);
+    if ((threadIdx.x & 31) == 0 && mine) atomicMax(w.hd + i, (uint32_t)mine);
+}
+
+__global__ void __launch_bounds__(256) wide_k1_kernel(WideAdd w)
+{
+    const size_t i = blockIdx.x / w.cpp, c = blockIdx.x % w.cpp;
+    const uint32_t na = w.l1[i], nb = w.l2[i], n = max(na, nb);
+    const WideOp o = wide_op(w, i);
+    const uint32_t* a = w.t1 + i * (size_t)w.c1;
+    const uint32_t* b = w.t2 + i * (size_t)w.c2;
+    uint32_t* z = w.Pw + (w.c0 + i) * (size_t)w.cP;
+    const uint32_t w0 = (uint32_t)c * kWideWPC + threadIdx.x * kWideIPT;
+    auto X = [&](uint32_t k) -> uint32_t {
+        const uint32_t u = k < na ? a[k] : 0u, v = k < nb ? b[k] : 0u;
+        return o.swap ? v : u;
+    };
+    auto Y = [&](uint32_t k) -> uint32_t {
+        const uint32_t u = k < na ? a[k] : 0u, v = k < nb ? b[k] : 0u;
+        return o.swap ? u : v;
+    };
+    uint32_t gp = kGPIdentity;
+    uint32_t xs[kWideIPT], ys[kWideIPT];
+#pragma unroll
+    for (int u = 0; u < kWideIPT; u++) {
+        const uint32_t k = w0 + u;
+        xs[u] = k < n ? X(k) : 0u;
+        ys[u] = k < n ? Y(k) : 0u;
+        uint32_t g = 0, p = 1;
+        if (k < n) {
+            if (!o.sub) {
+                const uint64_t sum = (uint64_t)xs[u] + ys[u];
+                g = (uint32_t)(sum >> 32);
+                p = (uint32_t)sum == 0xffffffffu;
+            } else {
+                g = xs[u] < ys[u];
+                p = xs[u] == ys[u];
+            }
+        }
+        gp = gp_combine(gp, g | (p << 1));
+    }
+    uint32_t total;
+    uint32_t cin = block_gp_scan(gp, &total) & 1u;
+#pragma unroll
+    for (int u = 0; u < kWideIPT; u++) {
+        const uint32_t k = w0 + u;
+        if (k >= n || o.zero) break;
+        if (!o.sub) {
+            const uint64_t sum = (uint64_t)xs[u] + ys[u];
+            const uint32_t d = (uint32_t)sum;
+            z[k] = d + cin;
+            cin = (uint32_t)(sum >> 32) | ((uint32_t)(d == 0xffffffffu) & cin);
+        } else {
+            const uint32_t d = xs[u] - ys[u];
+            z[k] = d - cin;
+            cin = (uint32_t)(xs[u] < ys[u]) | ((uint32_t)(d == 0u) & cin);
+        }
+    }
+    if (threadIdx.x == 0) {
+        w.agg[blockIdx.x] = total;
+        w.aggc[blockIdx.x] = total;
+    }
+}
+
+// Chunks with a carry-in: +1 (add) or -1 (subtract) rippled from the chunk's
+// first word to the first word that absorbs it.
+__global__ void __launch_bounds__(256) wide_ripple_kernel(WideAdd w)
+{
+    if (w.agg[blockIdx.x] == 0) return;
+    const size_t i = blockIdx.x / w.cpp, c = blockIdx.x % w.cpp;
+    const uint32_t n = max(w.l1[i], w.l2[i]);
+    const WideOp o = wide_op(w, i);
+    if (o.zero) return;
+    uint32_t* z = w.Pw + (w.c0 + i) * (size_t)w.cP;
+    const uint32_t b0 = (uint32_t)c * kWideWPC, e = min(b0 + kWideWPC, n);
+    const uint32_t stop = o.sub ? 0u : 0xffffffffu;  // words that pass the carry on
+    unsigned long long mine = ~0ull;
+    for (uint32_t k = b0 + threadIdx.x; k < e; k += blockDim.x)
+        if (z[k] != stop && k < mine) mine = k;
+    const uint32_t f = (uint32_t)min((unsigned long long)e, block_min_u64(mine));
+    for (uint32_t k = b0 + threadIdx.x; k < f; k += blockDim.x) z[k] = ~stop;
+    if (threadIdx.x == 0 && f < e) z[f] += o.sub ? 0xffffffffu : 1u;
+}
+
+// Length, carry word and sign.  Parent lengths start at zero.
+__global__ void __launch_bounds__(256) wide_final_kernel(WideAdd w)
+{
+    const size_t i = blockIdx.x / w.cpp, c = blockIdx.x % w.cpp;
+    const uint32_t n = max(w.l1[i], w.l2[i]);
+    const WideOp o = wide_op(w, i);
+    const bool sa = w.cS[2 * (w.c0 + i)] != 0, sb = w.cS[2 * (w.c0 + i) + 1] != 0;
+    uint32_t* z = w.Pw + (w.c0 + i) * (size_t)w.cP;
+    if (!o.sub) {
+        // the carry out of the last chunk: its (G, P) joined with its carry-in
+        const uint32_t last = n ? (n - 1) / kWideWPC : 0;
+        if (c == last && threadIdx.x == 0) {
+            const uint32_t gp = w.aggc[blockIdx.x], cin = w.agg[blockIdx.x];
+            const uint32_t carry = n ? ((gp & 1u) | ((gp >> 1) & cin)) : 0u;
+            if (carry) z[n] = 1;
+            w.Pl[w.c0 + i] = n + carry;
+            w.Ps[w.c0 + i] = sa ? 1 : 0;
+        }
+        return;
+    }
+    if (c == 0 && threadIdx.x == 0) w.Ps[w.c0 + i] = o.zero ? 1 : ((o.swap ? sb : sa) ? 1 : 0);
+    if (o.zero) return;
+    const uint32_t b0 = (uint32_t)c * kWideWPC, e = min(b0 + kWideWPC, n);
+    unsigned long long mine = 0;
+    for (uint32_t k = b0 + threadIdx.x; k < e; k += blockDim.x)
+        if (z[k] != 0) mine = k + 1;
+    mine = warp_max_u64(mine);
+    if ((threadIdx.x & 31) == 0 && mine) atomicMax(w.Pl + w.c0 + i, (uint32_t)mine);
+}
+
 static inline int ceil_log2_sz(size_t n)
 {
     int k = 0;
@@ -1014,6 +1190,7 @@ static Mod64 prime_mod(int q) { return make_mod(kProductPrimes[q]); }
 static bool g_wrap = true;
 static int g_small_merge = 2;  // 0: CTA schoolbook, 1: + warp per parent, 2: + thread per parent
 static bool g_top_batched = true;
+static bool g_wide_add = true;
 
 // Parameters of one level's batched NTT merge.  Every operand has at most
 // smax = ceil(cmax / 2) 64-bit pieces, every product at most L = 2 smax - 1
@@ -1250,8 +1427,25 @@ static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
         o.cR = par.R.cap;
         o.lR = par.R.len.get() + p0;
         ntt_products(ch, p0, np, sh, o, s);
-        {
-            ProfScope ps(KC_LINEAR, 12.0 * (double)np * (double)c1, s);
+        ProfScope ps(KC_LINEAR, 12.0 * (double)np * (double)c1, s);
+        const uint32_t cpp = (uint32_t)((std::max(c1, c2) + kWideWPC - 1) / kWideWPC);
+        if (g_wide_add && np < 2 * 148 && cpp > 1) {
+            // few long parents: spread each sum over many CTAs
+            DevBuf<uint32_t> hd(np, s), agg(np * cpp, s), aggc(np * cpp, s);
+            PIC_CUDA(cudaMemsetAsync(hd.get(), 0, 4 * np, s));
+            PIC_CUDA(cudaMemsetAsync(par.P.len.get() + p0, 0, 4 * np, s));
+            WideAdd w{T1.get(), l1.get(), T2.get(), l2.get(), c1, c2, ch.sign.get(), p0, par.P.w.get(),
+                      par.P.len.get(), par.P.cap, par.sign.get(), hd.get(), agg.get(), aggc.get(), cpp};
+            const unsigned grid = (unsigned)(np * cpp);
+            wide_cmp_kernel<<<grid, 256, 0, s>>>(w);
+            wide_k1_kernel<<<grid, 256, 0, s>>>(w);
+            PIC_CHECK_LAUNCH();
+            carry_scan_segments(agg.get(), np, cpp, s);
+            wide_ripple_kernel<<<grid, 256, 0, s>>>(w);
+            wide_final_kernel<<<grid, 256, 0, s>>>(w);
+            PIC_CHECK_LAUNCH();
+            count_launch(4);
+        } else {
             signed_add_kernel<<<(unsigned)np, 256, 0, s>>>(T1.get(), l1.get(), c1, T2.get(), l2.get(), c2,
                                                           ch.sign.get(), p0, par.P.w.get(), par.P.len.get(),
                                                           par.sign.get(), par.P.cap);

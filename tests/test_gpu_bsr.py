@@ -8,7 +8,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 CASES = [(0, 5, 100), (0, 4, 16), (0, 50, 10_000), (0, 706, 923), (17, 600, 5_000),
-         (0, 3000, 200), (0, 2000, 100_000), (1000, 1257, 50)]
+         (0, 3000, 200), (0, 2000, 100_000), (1000, 1257, 50), (0, 8000, 300_000)]
 
 
 def _same(dev, want) -> bool:
