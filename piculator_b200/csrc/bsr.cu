@@ -273,6 +273,51 @@ __global__ void bottom_kernel(const uint32_t* __restrict__ bnd, size_t count,
 //
 // Shared-memory helpers; every thread of the block must call them.
 
+// (s2:s1:s0) += a * b: one multiply-add into a 96-bit column sum.
+__device__ __forceinline__ void mac96(uint32_t& s0, uint32_t& s1, uint32_t& s2, uint32_t a, uint32_t b)
+{
+    asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+        "addc.u32 %2, %2, 0;"
+        : "+r"(s0), "+r"(s1), "+r"(s2)
+        : "r"(a), "r"(b));
+}
+
+// Column sums col[3c..3c+2] = sum_i a_i b_(c-i) (96 bits) for the four
+// columns c0 .. c0 + 3: a[i] is loaded once for all four, b slides through a
+// four-word register window.
+__device__ __forceinline__ void colsum4(const uint32_t* a, int na, const uint32_t* b, int nb, int c0, uint32_t zw,
+                                        uint32_t* col)
+{
+    uint32_t s0[4] = {0, 0, 0, 0}, s1[4] = {0, 0, 0, 0}, s2[4] = {0, 0, 0, 0};
+    const int ilo = max(0, c0 - nb + 1), ihi = min(c0 + 3, na - 1);
+    uint32_t W[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const int j = c0 + u - ilo;
+        W[u] = (j >= 0 && j < nb) ? b[j] : 0u;
+    }
+    for (int i = ilo; i <= ihi; i++) {
+        const uint32_t ai = a[i];
+#pragma unroll
+        for (int u = 0; u < 4; u++) mac96(s0[u], s1[u], s2[u], ai, W[u]);
+        W[3] = W[2];
+        W[2] = W[1];
+        W[1] = W[0];
+        const int j = c0 - i - 1;
+        W[0] = j >= 0 ? b[j] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const uint32_t c = (uint32_t)c0 + u;
+        if (c < zw) {
+            col[3 * c] = s0[u];
+            col[3 * c + 1] = s1[u];
+            col[3 * c + 2] = s2[u];
+        }
+    }
+}
+
 // z[0..na+nb) = a * b; col must hold 3 (na + nb) words.  Returns the length
 // without leading zeros (0 if either operand is empty).
 __device__ uint32_t cta_mul(const uint32_t* a, uint32_t na, const uint32_t* b, uint32_t nb, uint32_t* z,
@@ -283,22 +328,7 @@ __device__ uint32_t cta_mul(const uint32_t* a, uint32_t na, const uint32_t* b, u
         return 0;
     }
     const uint32_t zw = na + nb;
-    for (uint32_t c = threadIdx.x; c < zw; c += blockDim.x) {
-        uint64_t lo = 0;
-        uint32_t hi = 0;
-        if (c + 1 < zw) {
-            const uint32_t i_lo = c + 1 > nb ? c + 1 - nb : 0;
-            const uint32_t i_hi = c < na - 1 ? c : na - 1;
-            for (uint32_t i = i_lo; i <= i_hi; i++) {
-                const uint64_t pr = (uint64_t)a[i] * b[c - i];
-                lo += pr;
-                hi += (lo < pr);
-            }
-        }
-        col[3 * c] = (uint32_t)lo;
-        col[3 * c + 1] = (uint32_t)(lo >> 32);
-        col[3 * c + 2] = hi;
-    }
+    for (uint32_t g = threadIdx.x; 4 * g < zw; g += blockDim.x) colsum4(a, (int)na, b, (int)nb, (int)(4 * g), zw, col);
     __syncthreads();
     // each thread owns a contiguous run of output words
     const uint32_t per = (zw + blockDim.x - 1) / blockDim.x;
@@ -594,22 +624,7 @@ __device__ uint32_t warp_mul(const uint32_t* a, uint32_t na, const uint32_t* b, 
     const int lane = threadIdx.x & 31;
     if (na == 0 || nb == 0) return 0;
     const uint32_t zw = na + nb;
-    for (uint32_t c = lane; c < zw; c += 32) {
-        uint64_t lo = 0;
-        uint32_t hi = 0;
-        if (c + 1 < zw) {
-            const uint32_t i_lo = c + 1 > nb ? c + 1 - nb : 0;
-            const uint32_t i_hi = c < na - 1 ? c : na - 1;
-            for (uint32_t i = i_lo; i <= i_hi; i++) {
-                const uint64_t pr = (uint64_t)a[i] * b[c - i];
-                lo += pr;
-                hi += (lo < pr);
-            }
-        }
-        col[3 * c] = (uint32_t)lo;
-        col[3 * c + 1] = (uint32_t)(lo >> 32);
-        col[3 * c + 2] = hi;
-    }
+    for (uint32_t g = lane; 4 * g < zw; g += 32) colsum4(a, (int)na, b, (int)nb, (int)(4 * g), zw, col);
     __syncwarp();
     const uint32_t per = (zw + 31) / 32;
     const uint32_t w0 = lane * per, w1 = min(w0 + per, zw);
