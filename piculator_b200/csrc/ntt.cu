@@ -150,6 +150,21 @@ const PrimeTables& prime_tables(uint64_t p)
         d.shi_fwd = pairs(hif);
         d.slo_inv = pairs(loi);
         d.shi_inv = pairs(hii);
+        if (IB == kInnerBits) {
+            // per-level inner tables from the order-2^IB tables: the root of
+            // order 2^m is inner root^(2^(IB - m))
+            std::vector<uint64_t> lf((size_t)2 << IB), li((size_t)2 << IB);
+            for (int lm = 1; lm <= IB; lm++)
+                for (size_t e = 0; e < ((size_t)1 << (lm - 1)); e++) {
+                    const size_t dst = ((size_t)1 << (lm - 1)) - 1 + e, src = e << (IB - lm);
+                    lf[2 * dst] = inf[2 * src];
+                    lf[2 * dst + 1] = inf[2 * src + 1];
+                    li[2 * dst] = ini[2 * src];
+                    li[2 * dst + 1] = ini[2 * src + 1];
+                }
+            d.lvl_fwd = upload(lf);
+            d.lvl_inv = upload(li);
+        }
     }
     g_tabs[p] = t;
     return *t;
@@ -644,8 +659,9 @@ __device__ __forceinline__ void fbfly_unit_dit(uint64_t& a, uint64_t& b, const L
 }
 
 // The B levels of one group (elements base + j + m 2^LST, m < 2^B) with the
-// inner table of order 2^13: the twiddle of butterfly u at group level l is
-// root_(2^(B-l+LST))^(j + u 2^LST) = tw[(j + (u << LST)) << (13 - (B-l) - LST)].
+// per-level inner tables: the twiddle of butterfly u at group level l is
+// root_(2^(B-l+LST))^(j + u 2^LST), pair 2^(B-l+LST-1) - 1 + j + u 2^LST, so
+// lanes with consecutive j read consecutive pairs.
 template <int B, bool INV, int LST>
 __device__ __forceinline__ void group_fast(uint64_t (&x)[1 << B], int j, const LazyPrime& L,
                                            const ulonglong2* __restrict__ tw)
@@ -664,7 +680,7 @@ __device__ __forceinline__ void group_fast(uint64_t (&x)[1 << B], int j, const L
             for (int m = 0; m < (1 << B); m++) {
                 if (m & hm) continue;
                 const int u = m & (hm - 1);
-                fbfly_dif(x[m], x[m + hm], __ldg(tw + ((j + (u << LST)) << (13 - (B - l) - LST))), L);
+                fbfly_dif(x[m], x[m + hm], __ldg(tw + ((1 << (B - l + LST - 1)) - 1) + j + (u << LST)), L);
             }
         }
     } else {
@@ -680,7 +696,7 @@ __device__ __forceinline__ void group_fast(uint64_t (&x)[1 << B], int j, const L
             for (int m = 0; m < (1 << B); m++) {
                 if (m & hm) continue;
                 const int u = m & (hm - 1);
-                fbfly_dit(x[m], x[m + hm], __ldg(tw + ((j + (u << LST)) << (13 - (B - l) - LST))), L);
+                fbfly_dit(x[m], x[m + hm], __ldg(tw + ((1 << (B - l + LST - 1)) - 1) + j + (u << LST)), L);
             }
         }
     }
@@ -726,7 +742,7 @@ __device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const 
         if (LRPC > 0 && row0 + t < (size_t)Bt.count) {  // rows past the batch keep the CTA's prime
             const PrimeDev Pt = pick_prime(Bt, (int)(row0 + t));
             L = lazy_prime(Pt);
-            tw = reinterpret_cast<const ulonglong2*>(INV ? Pt.inner_inv : Pt.inner_fwd);
+            tw = reinterpret_cast<const ulonglong2*>(INV ? Pt.lvl_inv : Pt.lvl_fwd);
         }
         uint64_t x[1 << B];
 #pragma unroll
@@ -772,7 +788,7 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC>::NT, 1024 / RowsFastSh
     }
     __syncthreads();
     rows_fast_round<INV, LR, LRPC, NT, 0>(smem, B, row0, L,
-                                          reinterpret_cast<const ulonglong2*>(INV ? P.inner_inv : P.inner_fwd));
+                                          reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
 #pragma unroll
     for (int i = 0; i < TOT / NT; i++) {
         const int idx = threadIdx.x + i * NT;
@@ -850,7 +866,7 @@ __global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatc
         smem[idx] = v;
     }
     __syncthreads();
-    cols_fast_round<INV, LC, LW, 0>(smem, L, reinterpret_cast<const ulonglong2*>(INV ? P.inner_inv : P.inner_fwd));
+    cols_fast_round<INV, LC, LW, 0>(smem, L, reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
 #pragma unroll 2
     for (int idx = threadIdx.x; idx < TOT; idx += 256) {
         const int m = idx >> LW, w = idx & WMASK;
@@ -872,8 +888,8 @@ static bool fast_ok(const NttBatch& b, int k)
 {
     if (!PIC_NTT_FAST || g_geom[k].rbits != 3) return false;
     for (int q = 0; q * b.per_prime < b.count; q++)
-        if (!b.prime[q].lazy || b.prime[q].IB != 13 || (q > 0 && (b.prime[q].slo_fwd == nullptr) !=
-                                                                     (b.prime[0].slo_fwd == nullptr)))
+        if (!b.prime[q].lazy || b.prime[q].IB != 13 || b.prime[q].lvl_fwd == nullptr ||
+            (q > 0 && (b.prime[q].slo_fwd == nullptr) != (b.prime[0].slo_fwd == nullptr)))
             return false;
     return true;
 }

@@ -50,6 +50,11 @@ struct PrimeDev {
     const uint64_t* shi_fwd;
     const uint64_t* slo_inv;
     const uint64_t* shi_inv;
+    // Lazy primes only (else null): inner roots by level, Shoup pairs.  The
+    // roots of order 2^m (m = 1 .. 13), root^e for e < 2^(m-1), sit at pair
+    // index 2^(m-1) - 1 + e, so consecutive e are consecutive pairs.
+    const uint64_t* lvl_fwd;
+    const uint64_t* lvl_inv;
 };
 
 // Host-owned tables for one prime (built once, cached for the process).
