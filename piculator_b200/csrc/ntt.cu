@@ -3,6 +3,8 @@
 #include <string.h>
 
 #include <map>
+#include <tuple>
+#include <vector>
 #include <mutex>
 
 #include "common.cuh"
@@ -128,6 +130,11 @@ const PrimeTables& prime_tables(uint64_t p)
     d.IB = IB;
     // lazy butterflies need 4p < 2^64 and the c * 2^32 + 1 form (mul_p_lo)
     d.lazy = (p < (1ull << 62) && (p & 0xffffffffull) == 1) ? 1 : 0;
+    {
+        const unsigned __int128 mu = (~(unsigned __int128)0) / p;  // floor(2^128 / p): p does not divide 2^128
+        d.mu_hi = (uint64_t)(mu >> 64);
+        d.mu_lo = (uint64_t)mu;
+    }
     d.inner_fwd = upload(inf);
     d.inner_inv = upload(ini);
     d.olo_fwd = upload(lof);
@@ -828,12 +835,47 @@ __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const 
     if constexpr (R + 1 < Plan::NR) cols_fast_round<INV, LC, LW, R + 1>(s, L, tw);
 }
 
+// floor(x 2^64 / p) for x < p: q' = floor(x mu / 2^64) with mu = floor(2^128 /
+// p) is q or q - 1 (x < 2^62), and the remainder x 2^64 - q' p < 2p decides.
+__device__ __forceinline__ uint64_t shoup_companion_dev(uint64_t x, uint64_t p, uint64_t mu_hi, uint64_t mu_lo)
+{
+    const uint64_t q = x * mu_hi + __umul64hi(x, mu_lo);
+    const uint64_t r = (uint64_t)0 - q * p;
+    return r >= p ? q + 1 : q;
+}
+
+// Pass twiddle tables: for a column pass over blocks of 2^lblock points split
+// 2^LC x M, entry m M + c = root_(2^lblock)^(+-c brev_LC(m)) as a Shoup pair,
+// laid out like the data so the pass streams it with the same coalescing.
+struct PassTw {
+    const ulonglong2* t[kMaxPrimesPerBatch];
+};
+
+__global__ void pass_table_kernel(ulonglong2* __restrict__ out, PrimeDev P, int inv, int lblock, int lc)
+{
+    const size_t n = (size_t)1 << lblock;
+    const int lM = lblock - lc;
+    const int esh = P.K - lblock;
+    const LazyPrime L = lazy_prime(P);
+    const ulonglong2* slo = reinterpret_cast<const ulonglong2*>(inv ? P.slo_inv : P.slo_fwd);
+    const ulonglong2* shi = reinterpret_cast<const ulonglong2*>(inv ? P.shi_inv : P.shi_fwd);
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
+        const uint64_t m = g >> lM, c = g & (((size_t)1 << lM) - 1);
+        const uint64_t k1 = __brev((unsigned)m) >> (32 - lc);
+        const uint64_t E = (c * k1) << esh;
+        const ulonglong2 h = __ldg(shi + (E >> P.S)), l = __ldg(slo + (E & (((uint64_t)1 << P.S) - 1)));
+        uint64_t x = shoup_lazy32(h.x, l.x, l.y, L.c);
+        x = x >= L.p ? x - L.p : x;
+        out[g] = make_ulonglong2(x, shoup_companion_dev(x, L.p, P.mu_hi, P.mu_lo));
+    }
+}
+
 // Strided column pass (same tiling as ntt_cols_kernel).  The inter-pass
 // twiddle root_(2^lblock)^((c0 + w) k1) is applied as two Shoup products
 // with the two-level outer tables: forward after the column DIF, inverse
 // before the column DIT.
 template <bool INV, int LC, int LW>
-__global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatch B, int k, int lpre)
+__global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatch B, int k, int lpre, PassTw pt)
 {
     extern __shared__ uint64_t smem[];
     constexpr int TOT = 1 << (LC + LW), WMASK = (1 << LW) - 1;
@@ -852,13 +894,18 @@ __global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatc
     const uint64_t smask = ((uint64_t)1 << S) - 1;
     const ulonglong2* __restrict__ slo = reinterpret_cast<const ulonglong2*>(INV ? P.slo_inv : P.slo_fwd);
     const ulonglong2* __restrict__ shi = reinterpret_cast<const ulonglong2*>(INV ? P.shi_inv : P.shi_fwd);
+    const ulonglong2* __restrict__ T = tr < B.per_prime ? pt.t[0] : (tr < 2 * B.per_prime ? pt.t[1] : pt.t[2]);
     auto twiddle = [&](uint64_t v, int m, int w) {
+        if (T != nullptr) {  // the pass table: one Shoup product, streamed like the data
+            const ulonglong2 t = __ldg(T + ((size_t)m << lM) + c0 + w);
+            return shoup_lazy32(v, t.x, t.y, L.c);
+        }
         const uint64_t k1 = __brev((unsigned)m) >> (32 - LC);
         const uint64_t E = ((uint64_t)(c0 + w) * k1) << esh;
         const ulonglong2 h = __ldg(shi + (E >> S)), l = __ldg(slo + (E & smask));
         return shoup_lazy32(shoup_lazy32(v, h.x, h.y, L.c), l.x, l.y, L.c);
     };
-#pragma unroll 2
+#pragma unroll 8
     for (int idx = threadIdx.x; idx < TOT; idx += 256) {
         const int m = idx >> LW, w = idx & WMASK;
         uint64_t v = base[((size_t)m << lM) + w];
@@ -867,7 +914,7 @@ __global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatc
     }
     __syncthreads();
     cols_fast_round<INV, LC, LW, 0>(smem, L, reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
-#pragma unroll 2
+#pragma unroll 8
     for (int idx = threadIdx.x; idx < TOT; idx += 256) {
         const int m = idx >> LW, w = idx & WMASK;
         uint64_t v = smem[idx];
@@ -931,12 +978,51 @@ static bool launch_rows_fast(const NttBatch& b, int k, int lr, cudaStream_t s)
     return true;
 }
 
+// Pass twiddle tables for root orders up to 2^kPassTableMaxBits (at most
+// 6 x 16 x 2^24 bytes per order for the three product primes): built on the
+// device on first use per (prime, direction, order, column height), kept for
+// the process; never built while the stream is being captured (the pass then
+// forms its twiddles from the two-level tables).
+constexpr int kPassTableMaxBits = 24;
+static std::mutex g_pass_lock;
+static std::map<std::tuple<uint64_t, int, int, int>, ulonglong2*> g_pass_tables;
+
+static const ulonglong2* pass_table(const PrimeDev& P, bool inv, int lblock, int lc, cudaStream_t s)
+{
+    if (lblock > kPassTableMaxBits) return nullptr;
+    const auto key = std::make_tuple(P.p, inv ? 1 : 0, lblock, lc);
+    std::lock_guard<std::mutex> g(g_pass_lock);
+    auto it = g_pass_tables.find(key);
+    if (it != g_pass_tables.end()) return it->second;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PIC_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return nullptr;
+    ulonglong2* d = nullptr;
+    if (cudaMalloc(&d, sizeof(ulonglong2) << lblock) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;  // no room: the pass keeps the two-level tables
+    }
+    const size_t n = (size_t)1 << lblock;
+    pass_table_kernel<<<grid_for(n, 256), 256, 0, s>>>(d, P, inv ? 1 : 0, lblock, lc);
+    PIC_CHECK_LAUNCH();
+    count_launch();
+    g_pass_tables[key] = d;
+    return d;
+}
+
 template <bool INV, int LC, int LW>
 static void launch_cols_fast_t(const NttBatch& b, int k, int lpre, size_t grid, cudaStream_t s)
 {
     constexpr size_t smem = sizeof(uint64_t) << (LC + LW);
+    PassTw pt{};
+    bool all = true;
+    for (int q = 0; q * b.per_prime < b.count; q++) {
+        pt.t[q] = pass_table(b.prime[q], INV, k - lpre, LC, s);
+        all = all && pt.t[q] != nullptr;
+    }
+    if (!all) pt = PassTw{};  // one form for every prime of the launch
     set_smem(ntt_cols_fast_kernel<INV, LC, LW>, smem);
-    ntt_cols_fast_kernel<INV, LC, LW><<<(unsigned)grid, 256, smem, s>>>(b, k, lpre);
+    ntt_cols_fast_kernel<INV, LC, LW><<<(unsigned)grid, 256, smem, s>>>(b, k, lpre, pt);
 }
 
 template <bool INV, int LC>

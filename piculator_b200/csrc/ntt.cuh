@@ -55,6 +55,8 @@ struct PrimeDev {
     // index 2^(m-1) - 1 + e, so consecutive e are consecutive pairs.
     const uint64_t* lvl_fwd;
     const uint64_t* lvl_inv;
+    // floor(2^128 / p) = mu_hi 2^64 + mu_lo: Shoup companions on the device
+    uint64_t mu_hi, mu_lo;
 };
 
 // Host-owned tables for one prime (built once, cached for the process).
