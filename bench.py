@@ -367,7 +367,9 @@ def ours(args):
     if rank == 0:
         mean_phase = {k: statistics.mean(p[k] for p in phases)
                       for k in ("seconds_bsr", "seconds_div", "seconds_invsqrt", "seconds_final_mul")}
-        mean_phase["step_seconds"] = [round(p["seconds_total"], 4) for p in phases]
+        mean_phase["step_seconds"] = [[round(p[k], 4) for k in ("seconds_total", "seconds_bsr", "seconds_div",
+                                                                 "seconds_invsqrt", "seconds_final_mul")]
+                                      for p in phases]
         line = {
             "metric": METRIC, "value": dev_s, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_s * 1000.0, "higher_is_better": False,

@@ -829,24 +829,37 @@ __global__ void slot_split_kernel(uint64_t* __restrict__ out, const uint32_t* __
 // For every parent i and prime q (arrays laid out [q][child][stride], the
 // transforms of length 2^k at the start of each item):
 //   T1 = PL QR -> P[2i], T2 = PR RL -> P[2i+1], Q = QL QR -> Q[2i], R = RL RR -> R[2i]
-__global__ void merge_pointwise_kernel(uint64_t* __restrict__ P, uint64_t* __restrict__ Q, uint64_t* __restrict__ R,
-                                       size_t npar, int k, size_t stride, Mod64 m0, Mod64 m1, Mod64 m2)
+__global__ void __launch_bounds__(256) merge_pointwise_kernel(uint64_t* __restrict__ P, uint64_t* __restrict__ Q,
+                                                              uint64_t* __restrict__ R, uint32_t npar, int k,
+                                                              size_t stride, uint32_t jbpr, Mod64 m0, Mod64 m1,
+                                                              Mod64 m2)
 {
-    const size_t N = (size_t)1 << k;
-    const size_t total = 3 * npar * N;
-    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
-        const size_t q = g / (npar * N);
-        const size_t r = g - q * npar * N;
-        const size_t i = r >> k, j = r & (N - 1);
-        const Mod64& M = q == 0 ? m0 : (q == 1 ? m1 : m2);
-        const size_t base = q * 2 * npar;
-        const size_t L = (base + 2 * i) * stride + j, Rr = (base + 2 * i + 1) * stride + j;
-        const uint64_t pl = P[L], pr = P[Rr], ql = Q[L], qr = Q[Rr], rl = R[L], rr = R[Rr];
-        P[L] = mont_mul(pl, qr, M);
-        P[Rr] = mont_mul(pr, rl, M);
-        Q[L] = mont_mul(ql, qr, M);
-        R[L] = mont_mul(rl, rr, M);
-    }
+    // block -> (prime q, parent i, run of 512 points); two points per thread
+    const uint32_t row = blockIdx.x / jbpr, jb = blockIdx.x - row * jbpr;
+    const uint32_t q = row / npar, i = row - q * npar;
+    const size_t j = ((size_t)jb * blockDim.x + threadIdx.x) * 2;
+    if (j >= ((size_t)1 << k)) return;
+    const Mod64& M = q == 0 ? m0 : (q == 1 ? m1 : m2);
+    const size_t base = (size_t)q * 2 * npar;
+    const size_t L = (base + 2 * (size_t)i) * stride + j, Rr = L + stride;
+    const ulonglong2 pl = *reinterpret_cast<const ulonglong2*>(P + L), pr = *reinterpret_cast<const ulonglong2*>(P + Rr);
+    const ulonglong2 ql = *reinterpret_cast<const ulonglong2*>(Q + L), qr = *reinterpret_cast<const ulonglong2*>(Q + Rr);
+    const ulonglong2 rl = *reinterpret_cast<const ulonglong2*>(R + L), rr = *reinterpret_cast<const ulonglong2*>(R + Rr);
+    *reinterpret_cast<ulonglong2*>(P + L) = make_ulonglong2(mont_mul(pl.x, qr.x, M), mont_mul(pl.y, qr.y, M));
+    *reinterpret_cast<ulonglong2*>(P + Rr) = make_ulonglong2(mont_mul(pr.x, rl.x, M), mont_mul(pr.y, rl.y, M));
+    *reinterpret_cast<ulonglong2*>(Q + L) = make_ulonglong2(mont_mul(ql.x, qr.x, M), mont_mul(ql.y, qr.y, M));
+    *reinterpret_cast<ulonglong2*>(R + L) = make_ulonglong2(mont_mul(rl.x, rr.x, M), mont_mul(rl.y, rr.y, M));
+}
+
+// Launch over 3 primes x npar parents x 2^k points (stride even, 2^k >= 2).
+static void launch_merge_pointwise(uint64_t* P, uint64_t* Q, uint64_t* R, size_t npar, int k, size_t stride,
+                                   const Mod64& m0, const Mod64& m1, const Mod64& m2, cudaStream_t s)
+{
+    PIC_REQUIRE(k >= 1 && stride % 2 == 0 && npar <= 0x7fffffffu / 3, PIC_ERR_INVALID, "pointwise merge shape");
+    const uint32_t jbpr = (uint32_t)((((size_t)1 << k) + 511) / 512);
+    const size_t blocks = 3 * npar * (size_t)jbpr;
+    PIC_REQUIRE(blocks <= 0x7fffffffu, PIC_ERR_INVALID, "pointwise merge grid too large");
+    merge_pointwise_kernel<<<(unsigned)blocks, 256, 0, s>>>(P, Q, R, (uint32_t)npar, k, stride, jbpr, m0, m1, m2);
 }
 
 // Wrapped products.  A product of two operands of at most s pieces has
@@ -1337,11 +1350,8 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
             }
         {
             ProfScope ps(KC_NTT_POINTWISE, 3.0 * 3 * np * (double)(N + T) * 80.0 / 8.0, s);
-            merge_pointwise_kernel<<<grid_for(3 * np * N, 256), 256, 0, s>>>(bP.get(), bQ.get(), bR.get(), np, k, ST,
-                                                                           m0, m1, m2);
-            if (sh.wrap)
-                merge_pointwise_kernel<<<grid_for(3 * np * T, 256), 256, 0, s>>>(tP.get(), tQ.get(), tR.get(), np,
-                                                                               sh.kt, T, m0, m1, m2);
+            launch_merge_pointwise(bP.get(), bQ.get(), bR.get(), np, k, ST, m0, m1, m2, s);
+            if (sh.wrap) launch_merge_pointwise(tP.get(), tQ.get(), tR.get(), np, sh.kt, T, m0, m1, m2, s);
             PIC_CHECK_LAUNCH();
             count_launch(sh.wrap ? 2 : 1);
         }
@@ -1641,9 +1651,7 @@ static bool top_level_merge(const std::vector<BigFloat>& cP, const std::vector<B
     auto sT1 = alloc_words(np * c1), sT2 = alloc_words(np * c2), sQ = alloc_words(np * cq);
     std::shared_ptr<WordStore> sR = need_R ? alloc_words(np * cr) : nullptr;
     DevBuf<uint32_t> lens(4 * np, s);
-    size_t free_b = 0, total_b = 0;
-    PIC_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    size_t chunk = std::max<size_t>(free_b / 4, (size_t)1 << 30) / ntt_bytes_per_parent(sh);
+    size_t chunk = std::max<size_t>(device_available_bytes() / 4, (size_t)1 << 30) / ntt_bytes_per_parent(sh);
     if (chunk < 1) chunk = 1;
     for (size_t p0 = 0; p0 < np; p0 += chunk) {
         const size_t n = std::min(chunk, np - p0);
@@ -1743,8 +1751,7 @@ void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, s
         count_launch();
     }
     // merge up to Dtop
-    size_t free_b = 0, total_b = 0;
-    PIC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t free_b = device_available_bytes();
     for (int d = Db - 1; d >= Dtop; d--) {
         const size_t cnt = (size_t)1 << d;
         const double n = ceil((double)T / (double)cnt);

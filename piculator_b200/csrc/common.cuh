@@ -60,6 +60,8 @@ inline void count_launch(uint64_t n = 1) { ctx().launches.fetch_add(n, std::memo
 // threshold raised at init so freed blocks stay cached for reuse).
 void* dev_alloc(size_t bytes, cudaStream_t s);
 void dev_free(void* p, size_t bytes, cudaStream_t s);
+// Free device memory plus what the allocation pool holds unused.
+size_t device_available_bytes();
 
 template <typename T>
 struct DevBuf {

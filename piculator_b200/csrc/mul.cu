@@ -58,27 +58,36 @@ constexpr size_t kCvtLPC = (size_t)kCvtThreads * kCvtLPT;
 constexpr size_t kCvtWPC = 2 * kCvtLPC;
 
 struct Crt3Consts {
-    uint64_t p[3], pinv[3];
-    uint64_t scale[3];     // R^2 N^-1 mod p_q: undoes the pointwise R^-1 and the unscaled inverse
-    uint64_t inv01_m;      // Montgomery form of p0^-1 mod p1
-    uint64_t p0_mod_p2_m;  // Montgomery form of p0 mod p2
-    uint64_t inv012_m;     // Montgomery form of (p0 p1)^-1 mod p2
+    uint64_t p[3];
+    uint32_t c[3];      // p = c 2^32 + 1
+    ulonglong2 scale[3];  // N^-1 R^depth mod p_q (Shoup pair): undoes the pointwise R^-1 and the unscaled inverse
+    ulonglong2 inv01;     // p0^-1 mod p1
+    ulonglong2 p0m2;      // p0 mod p2
+    ulonglong2 inv012;    // (p0 p1)^-1 mod p2
     uint64_t p0p1_lo, p0p1_hi;
 };
 
+// x * w mod p in [0, p) for a Shoup pair w (product primes c 2^32 + 1).
+__device__ __forceinline__ uint64_t crt_mul(uint64_t x, const ulonglong2& w, uint64_t p, uint32_t c)
+{
+    const uint64_t r = shoup_lazy32(x, w.x, w.y, c);
+    return r >= p ? r - p : r;
+}
+
 // Garner's CRT: x = r0 + p0 (v1 + p1 v2), 0 <= x < p0 p1 p2, as three limbs.
+// Inputs may be any 64-bit residue representatives (lazy transforms).
 __device__ __forceinline__ void crt3(const Crt3Consts& C, uint64_t y0, uint64_t y1, uint64_t y2, uint64_t& l0,
                                      uint64_t& l1, uint64_t& l2)
 {
-    const uint64_t r0 = mont_mul(y0, C.scale[0], C.p[0], C.pinv[0]);
-    const uint64_t r1 = mont_mul(y1, C.scale[1], C.p[1], C.pinv[1]);
-    const uint64_t r2 = mont_mul(y2, C.scale[2], C.p[2], C.pinv[2]);
+    const uint64_t r0 = crt_mul(y0, C.scale[0], C.p[0], C.c[0]);
+    const uint64_t r1 = crt_mul(y1, C.scale[1], C.p[1], C.c[1]);
+    const uint64_t r2 = crt_mul(y2, C.scale[2], C.p[2], C.c[2]);
     const uint64_t r0m1 = r0 >= C.p[1] ? r0 - C.p[1] : r0;
-    const uint64_t v1 = mont_mul(sub_mod(r1, r0m1, C.p[1]), C.inv01_m, C.p[1], C.pinv[1]);
+    const uint64_t v1 = crt_mul(sub_mod(r1, r0m1, C.p[1]), C.inv01, C.p[1], C.c[1]);
     const uint64_t r0m2 = r0 >= C.p[2] ? r0 - C.p[2] : r0;
     uint64_t t = sub_mod(r2, r0m2, C.p[2]);
-    t = sub_mod(t, mont_mul(v1, C.p0_mod_p2_m, C.p[2], C.pinv[2]), C.p[2]);
-    const uint64_t v2 = mont_mul(t, C.inv012_m, C.p[2], C.pinv[2]);
+    t = sub_mod(t, crt_mul(v1, C.p0m2, C.p[2], C.c[2]), C.p[2]);
+    const uint64_t v2 = crt_mul(t, C.inv012, C.p[2], C.c[2]);
     // p0 * v1 + r0
     uint64_t a0 = C.p[0] * v1, a1 = mulhi64(C.p[0], v1);
     a0 += r0;
@@ -317,26 +326,27 @@ double fft_coef_to_words(const double2* T, size_t ncoef, double scale, int bits,
     return e;
 }
 
-// Scale folded into the CRT: R^(depth+1) N^-1 undoes `depth` pointwise
-// Montgomery products (each contributes R^-1) and the unscaled inverse (N).
+// Scale folded into the CRT: multiplying by R^depth N^-1 undoes `depth`
+// pointwise Montgomery products (each contributes R^-1) and the unscaled
+// inverse (N).  Every constant is a Shoup pair (value, companion).
 static Crt3Consts make_crt3(int k, int depth)
 {
     Crt3Consts C;
     const uint64_t N = (uint64_t)1 << k;
+    auto pair = [](uint64_t w, uint64_t p) { return make_ulonglong2(w, shoup_companion(w, p)); };
     for (int q = 0; q < 3; q++) {
         const uint64_t p = kProductPrimes[q];
-        const Mod64 m = make_mod(p);
         C.p[q] = p;
-        C.pinv[q] = m.pinv_neg;
+        C.c[q] = (uint32_t)(p >> 32);
         uint64_t sc = host_powmod(N % p, p - 2, p);
         for (int d = 0; d < depth; d++) sc = to_mont(sc, p);
-        C.scale[q] = to_mont(sc, p);  // mont_mul(y, scale) = y * R^(depth+1) N^-1
+        C.scale[q] = pair(sc, p);  // y * N^-1 R^depth
     }
     const uint64_t p0 = C.p[0], p1 = C.p[1], p2 = C.p[2];
-    C.inv01_m = to_mont(host_powmod(p0 % p1, p1 - 2, p1), p1);
-    C.p0_mod_p2_m = to_mont(p0 % p2, p2);
+    C.inv01 = pair(host_powmod(p0 % p1, p1 - 2, p1), p1);
+    C.p0m2 = pair(p0 % p2, p2);
     const uint64_t p01m2 = host_mulmod(p0 % p2, p1 % p2, p2);
-    C.inv012_m = to_mont(host_powmod(p01m2, p2 - 2, p2), p2);
+    C.inv012 = pair(host_powmod(p01m2, p2 - 2, p2), p2);
     const unsigned __int128 p01 = (unsigned __int128)p0 * p1;
     C.p0p1_lo = (uint64_t)p01;
     C.p0p1_hi = (uint64_t)(p01 >> 64);

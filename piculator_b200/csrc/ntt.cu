@@ -598,37 +598,6 @@ __device__ __forceinline__ LazyPrime lazy_prime(const PrimeDev& P)
     return L;
 }
 
-// x * w mod p in [0, 2p) for any x < 2^64 (Shoup, ws = floor(w 2^64 / p)).
-// q = floor(x ws / 2^64) from four 32 x 32 partial products; q p mod 2^64 =
-// q + ((q mod 2^32) c) 2^32.
-__device__ __forceinline__ uint64_t shoup_lazy32(uint64_t x, uint64_t w, uint64_t ws, uint32_t c)
-{
-    const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32);
-    const uint32_t s0 = (uint32_t)ws, s1 = (uint32_t)(ws >> 32);
-    const uint32_t w0 = (uint32_t)w, w1 = (uint32_t)(w >> 32);
-    uint32_t r0, r1;
-    asm("{\n\t.reg .u32 u0, u1, u2, q0, q1;\n\t"
-        "mul.hi.u32 u0, %2, %4;\n\t"
-        "mad.lo.cc.u32 u0, %2, %5, u0;\n\t"
-        "madc.hi.u32 u1, %2, %5, 0;\n\t"
-        "mad.lo.cc.u32 u0, %3, %4, u0;\n\t"
-        "madc.hi.cc.u32 u1, %3, %4, u1;\n\t"
-        "addc.u32 u2, 0, 0;\n\t"
-        "mad.lo.cc.u32 q0, %3, %5, u1;\n\t"
-        "madc.hi.u32 q1, %3, %5, u2;\n\t"
-        "mul.lo.u32 %0, %2, %6;\n\t"
-        "mul.hi.u32 %1, %2, %6;\n\t"
-        "mad.lo.u32 %1, %2, %7, %1;\n\t"
-        "mad.lo.u32 %1, %3, %6, %1;\n\t"
-        "mad.lo.u32 u1, q0, %8, q1;\n\t"
-        "sub.cc.u32 %0, %0, q0;\n\t"
-        "subc.u32 %1, %1, u1;\n\t"
-        "}"
-        : "=r"(r0), "=r"(r1)
-        : "r"(x0), "r"(x1), "r"(s0), "r"(s1), "r"(w0), "r"(w1), "r"(c));
-    return ((uint64_t)r1 << 32) | r0;
-}
-
 // Forward (DIF): operands and results in [0, 2p).
 __device__ __forceinline__ void fbfly_dif(uint64_t& a, uint64_t& b, const ulonglong2 t, const LazyPrime& L)
 {

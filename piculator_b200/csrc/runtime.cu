@@ -94,6 +94,19 @@ void* dev_alloc(size_t bytes, cudaStream_t s)
     return p;
 }
 
+size_t device_available_bytes()
+{
+    size_t free_b = 0, total_b = 0;
+    PIC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    // memory the stream-ordered pool holds but no live buffer uses is available too
+    cudaMemPool_t pool;
+    PIC_CUDA(cudaDeviceGetDefaultMemPool(&pool, g_ctx.device));
+    uint64_t reserved = 0;
+    PIC_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    const uint64_t used = g_ctx.bytes_in_use.load();
+    return free_b + (reserved > used ? (size_t)(reserved - used) : 0);
+}
+
 void dev_free(void* p, size_t bytes, cudaStream_t s)
 {
     if (!p) return;
