@@ -9,7 +9,9 @@ so the fixtures can be regenerated bit for bit:
 
     python tests/golden/make_golden.py [--big]
 
---big adds the 10M- and 100M-digit pi runs (minutes of CPU).
+--big adds the 10M- and 100M-digit pi runs (minutes of CPU); --huge also the
+1e9-digit run (about two hours on 8 cores; its entry keeps the thread count
+and time of the run that produced it).
 """
 from __future__ import annotations
 
@@ -47,9 +49,10 @@ def run_pi(digits: int, threads: int) -> tuple[bytes, dict]:
     return data, timing
 
 
-def gen_pi(big: bool) -> dict:
+def gen_pi(big: bool, huge: bool = False) -> dict:
     out = {}
-    sizes = [10_000, 100_000, 1_000_000] + ([10_000_000, 100_000_000] if big else [])
+    sizes = [10_000, 100_000, 1_000_000] + ([10_000_000, 100_000_000] if big or huge else [])
+    sizes += [1_000_000_000] if huge else []
     for d in sizes:
         data, t = run_pi(d, os.cpu_count() or 1)
         out[str(d)] = {"md5": md5(data), "bytes": len(data), "head": data[:80].decode(),
@@ -158,17 +161,18 @@ def gen_bigfloat(ref: Reference) -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--big", action="store_true")
+    ap.add_argument("--huge", action="store_true")
     args = ap.parse_args()
     ref = Reference()
     fixtures = {
-        "pi": gen_pi(args.big),
+        "pi": gen_pi(args.big, args.huge),
         "products": gen_products(ref),
         "ntt": gen_ntt(ref),
         "bigfloat": gen_bigfloat(ref),
         "generator": "tests/golden/make_golden.py (reference compiled from its own sources)",
     }
     path = os.path.join(HERE, "reference_golden.json")
-    if os.path.exists(path) and not args.big:
+    if os.path.exists(path):
         old = json.load(open(path))
         for d, v in old.get("pi", {}).items():
             fixtures["pi"].setdefault(d, v)

@@ -23,9 +23,16 @@ def test_pi_matches_reference(pic, golden, digits, form):
 
 
 @pytest.mark.slow
-def test_pi_10m_matches_reference(pic, golden):
-    text, st = pic.pi_hex(10_000_000, pic.PI_CHOSEN)
-    assert hashlib.md5(text).hexdigest() == golden["pi"]["10000000"]["md5"]
+@pytest.mark.parametrize("digits", [10_000_000, 100_000_000, 1_000_000_000])
+def test_pi_large_matches_reference(pic, golden, digits):
+    """Up to the full 1e9-digit run: every hex digit equal to the reference's
+    pi.txt (the 1e9 fixture is the reference program's own 8-thread run)."""
+    text, st = pic.pi_hex(digits, pic.PI_CHOSEN)
+    g = golden["pi"][str(digits)]
+    assert len(text) == g["bytes"]
+    assert text[:80].decode() == g["head"]
+    assert text[-80:].decode() == g["tail"]
+    assert hashlib.md5(text).hexdigest() == g["md5"]
 
 
 def test_pi_oracle_agrees_small(pic, oracle):
