@@ -190,6 +190,37 @@ def reference_arm(args):
     print(json.dumps(line))
 
 
+def int_roof(P, torch, L, stream):
+    """Row-pass butterflies per second on a 2^23-word three-prime product
+    (3 row passes per product, each over 3 x 2^23 points and row_bits levels)
+    against the register-only butterfly ceiling."""
+    k, n = 23, 1 << 23
+    row_bits = P.get_ntt_geometry(k)[0]
+    a = torch.randint(-2**31, 2**31 - 1, (n,), dtype=torch.int32, device="cuda")
+    b = torch.randint(-2**31, 2**31 - 1, (n,), dtype=torch.int32, device="cuda")
+    z = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+    for _ in range(2):
+        P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, "ntt3")
+    torch.cuda.synchronize()
+    P.check(L.pic_profile_begin())
+    reps = 5
+    for _ in range(reps):
+        P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, "ntt3")
+    stats = (P.KernelStat * 32)()
+    cnt = C.c_int()
+    P.check(L.pic_profile_end(stats, 32, C.byref(cnt)))
+    rows = [s for s in stats[: cnt.value] if s.name.decode() == "ntt_rows"]
+    if not rows or rows[0].seconds <= 0:
+        return None
+    bfly = rows[0].launches * 3 * (n // 2) * row_bits
+    achieved = bfly / rows[0].seconds / 1e9
+    ceiling = P.butterfly_rate()
+    return {"kernel": "ntt_rows", "workload": "three-prime product of two 2^23-word operands",
+            "row_bits": row_bits, "achieved": achieved, "ceiling": ceiling, "unit": "G butterflies/s",
+            "frac": achieved / ceiling,
+            "ceiling_basis": "lazy Shoup DIF butterflies with operands in registers, no memory traffic"}
+
+
 def batched_products(P, torch, L, stream, count: int = 8192, top: int = 8192, seed: int = 7):
     """8192 independent products per call, operand sizes log-uniform in
     1..8192 limbs (splitmix64 seed 7), uniform random limbs: one pic_mul_batch
@@ -325,12 +356,29 @@ def ours(args):
     top = max(kstats, key=lambda k: k["seconds"])
     achieved = top["bytes"] / top["seconds"] / 1e9 if top["seconds"] > 0 else 0.0
     total_k = sum(k["seconds"] for k in kstats) or 1.0
+    # DRAM bytes per algorithmic byte of the NTT passes, from one ncu capture of
+    # the 2^23-word three-prime product (dram__bytes_read.sum +
+    # dram__bytes_write.sum over 16 B per point): the row pass moves 14.9 B per
+    # point, the column pass 30.8 B (data plus its twiddle table); both are per
+    # point, so they scale to a launch of any size.
+    dram_per_alg = {"ntt_rows": 14.9 / 16.0, "ntt_cols": 30.8 / 16.0}
+    avg_bytes = top["bytes"] / max(top["launches"], 1)
+    traffic = avg_bytes * dram_per_alg[top["name"]] if top["name"] in dram_per_alg else None
     roofline = {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "launches": top["launches"],
+                "traffic": traffic, "traffic_basis": "ncu DRAM bytes per point of the 2^23-word product, scaled "
+                                                     "to the kernel's average launch",
+                "launches": top["launches"],
                 "avg_launch_ms": 1e3 * top["seconds"] / max(top["launches"], 1),
                 "share_of_kernel_time": top["seconds"] / total_k,
                 "measured": "CUDA events around every launch of the kernel, over K extra profiled steps"}
+
+    # The integer roofline of the same passes: butterflies per second of the
+    # row pass on the 2^23-word three-prime product against the register-only
+    # butterfly rate of this GPU (pic_measure_butterfly_rate).
+    int_roofline = None
+    if rank == 0:
+        int_roofline = int_roof(P, torch, L, stream)
 
     plain = None
     if not args.no_plain and rank == 0:
@@ -382,6 +430,7 @@ def ours(args):
                     "d2h_bytes_per_step": int(outlen.value), "text_head": text_head},
             "gpu_launches": int(launches),
             "roofline": roofline,
+            "int_roofline": int_roofline,
             "cpu_baseline": cpu,
             "clocks": clk,
             "plain_vs_chosen": plain,

@@ -67,6 +67,11 @@ typedef struct {
 pic_status pic_profile_begin(void);
 pic_status pic_profile_end(pic_kernel_stat* out, int cap, int* n);
 
+/* The integer roofline of the NTT passes on this GPU: lazy 64-bit Shoup
+ * butterflies per second (in G) with operands in registers and no memory
+ * traffic.  No reference counterpart (a measurement aid). */
+pic_status pic_measure_butterfly_rate(double* gbfly_per_s);
+
 /* Test hook: make the next n device allocations fail with PIC_ERR_NO_MEMORY
  * (host-side fault injection; no GPU fault is involved). */
 void pic_debug_fail_allocations(int n);

@@ -80,6 +80,7 @@ _SIGS = {
     "pic_default_stream": ([], C.c_void_p),
     "pic_profile_begin": ([], C.c_int),
     "pic_profile_end": ([C.POINTER(KernelStat), C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "pic_measure_butterfly_rate": ([C.POINTER(C.c_double)], C.c_int),
     "pic_pi_compute": ([C.c_uint64, C.c_int, C.POINTER(C.c_void_p), C.POINTER(PiStats)], C.c_int),
     "pic_ntt_ensure_table": ([C.c_int], C.c_int),
     "pic_ntt_forward": ([_U64P, C.c_int, _P], C.c_int),
@@ -339,6 +340,14 @@ class Transform:
 
 (TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS, TUNE_BSR_WRAP,
  TUNE_BSR_SMALL_MERGE) = range(6)
+
+
+def butterfly_rate() -> float:
+    """G lazy Shoup butterflies per second with everything in registers: the
+    integer ceiling the NTT passes are measured against."""
+    v = C.c_double(0.0)
+    check(lib().pic_measure_butterfly_rate(C.byref(v)))
+    return v.value
 
 
 def set_tuning(knob: int, value: int) -> None:

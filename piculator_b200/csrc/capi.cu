@@ -132,6 +132,15 @@ pic_status pic_profile_end(pic_kernel_stat* out, int cap, int* n)
     });
 }
 
+pic_status pic_measure_butterfly_rate(double* gbfly_per_s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(gbfly_per_s);
+        *gbfly_per_s = butterfly_ceiling(ctx().stream);
+    });
+}
+
 // ---- NTT.h ---------------------------------------------------------------------
 static PrimeDev ref_prime_dev(int k)
 {

@@ -99,6 +99,9 @@ void ntt_pointwise_plain(uint64_t* T, const uint64_t* A, int k, const PrimeDev& 
 // T[i] = T[i] * n^-1 mod p.
 void ntt_scale_ninv(uint64_t* T, int k, const PrimeDev& P, cudaStream_t s);
 
+// G lazy Shoup butterflies per second with operands in registers (ceiling.cu).
+double butterfly_ceiling(cudaStream_t s);
+
 // Pass split used for length 2^k (for reporting / tests).
 std::vector<int> ntt_pass_bits(int k);
 // Tunable geometry per length (row-pass bits 8..13, column tile log2 width
