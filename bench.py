@@ -194,6 +194,8 @@ def int_roof(P, torch, L, stream):
     """Row-pass butterflies per second on a 2^23-word three-prime product
     (3 row passes per product, each over 3 x 2^23 points and row_bits levels)
     against the register-only butterfly ceiling."""
+    import ctypes as C
+
     k, n = 23, 1 << 23
     row_bits = P.get_ntt_geometry(k)[0]
     a = torch.randint(-2**31, 2**31 - 1, (n,), dtype=torch.int32, device="cuda")
