@@ -798,34 +798,6 @@ __global__ void __launch_bounds__(32 * kWarpMergeWarps) merge_warp_kernel(MergeA
 // ---------------------------------------------------------------------------
 // Batched three-prime NTT merge.
 
-// Child slot -> residues: out[(q * n2 + c) * ostride + j] = piece first + j of
-// child c0 + c, for j < 2^k (pieces past the child's length are zero).
-__global__ void slot_split_kernel(uint64_t* __restrict__ out, const uint32_t* __restrict__ w,
-                                  const uint32_t* __restrict__ len, uint32_t cap, size_t c0, size_t n2, int k,
-                                  size_t ostride, size_t first, uint64_t p0, uint64_t p1, uint64_t p2)
-{
-    const size_t N = (size_t)1 << k;
-    const size_t total = n2 * N;
-    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
-        const size_t c = g >> k, j = g & (N - 1);
-        const uint32_t n = len[c0 + c];
-        const uint32_t* x = w + (c0 + c) * (size_t)cap;
-        const size_t wi = 2 * (first + j);
-        uint64_t v = 0;
-        if (wi < n) {
-            v = x[wi];
-            if (wi + 1 < n) v |= (uint64_t)x[wi + 1] << 32;
-        }
-        uint64_t r0 = v, r1 = v, r2 = v;
-        while (r0 >= p0) r0 -= p0;
-        while (r1 >= p1) r1 -= p1;
-        while (r2 >= p2) r2 -= p2;
-        out[(0 * n2 + c) * ostride + j] = r0;
-        out[(1 * n2 + c) * ostride + j] = r1;
-        out[(2 * n2 + c) * ostride + j] = r2;
-    }
-}
-
 // For every parent i and prime q (arrays laid out [q][child][stride], the
 // transforms of length 2^k at the start of each item):
 //   T1 = PL QR -> P[2i], T2 = PR RL -> P[2i+1], Q = QL QR -> Q[2i], R = RL RR -> R[2i]
@@ -862,39 +834,6 @@ static void launch_merge_pointwise(uint64_t* P, uint64_t* Q, uint64_t* R, size_t
     merge_pointwise_kernel<<<(unsigned)blocks, 256, 0, s>>>(P, Q, R, (uint32_t)npar, k, stride, jbpr, m0, m1, m2);
 }
 
-// Wrapped products.  A product of two operands of at most s pieces has
-// L = 2s - 1 coefficients c_0..c_(L-1).  When L exceeds the main transform
-// length Nm (but s <= Nm), the cyclic product of length Nm holds
-// c_j + c_(Nm+j) for j < W = L - Nm.  The W top coefficients depend only on
-// the operands' top W pieces (indices >= t0 = Nm - s + 1): the product of
-// those pieces, d, gives c_(Nm+j) = d_(W-1+j), and its cyclic length
-// T >= 2W - 1 keeps those indices free of wrap.  For each of the W positions:
-//   y[j] <- y[j] - h (kept nonnegative by adding 2p), y[Nm + j] <- h
-// (inverse outputs arrive in [0, 4p) and are first brought below 2p),
-// with h = d_(W-1+j) * Nm / T so that both halves carry the same scale Nm.
-// y items have stride ystride >= Nm + W; tail items have stride T.  `item`
-// selects which children hold products (all for P, the even ones for Q, R).
-__global__ void wrap_fix_kernel(uint64_t* __restrict__ y, size_t ystride, const uint64_t* __restrict__ tail,
-                                size_t T, size_t nitems, size_t item_mul, size_t nchild, size_t Nm, size_t W,
-                                Mod64 m0, Mod64 m1, Mod64 m2, uint64_t c0, uint64_t c1, uint64_t c2)
-{
-    const size_t total = 3 * nitems * W;
-    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
-        const size_t q = g / (nitems * W);
-        const size_t r = g - q * nitems * W;
-        const size_t it = r / W, j = r - it * W;
-        const Mod64& M = q == 0 ? m0 : (q == 1 ? m1 : m2);
-        const uint64_t cT = q == 0 ? c0 : (q == 1 ? c1 : c2);
-        const size_t child = q * nchild + it * item_mul;
-        const uint64_t h = mont_mul(tail[child * T + W - 1 + j], cT, M);  // < p
-        uint64_t* yi = y + child * ystride;
-        const uint64_t p2 = 2 * M.p;
-        uint64_t v = yi[j];  // lazy inverse output, < 4p
-        v = v >= p2 ? v - p2 : v;
-        yi[j] = v + p2 - h;  // < 4p < 2^64: the CRT reduces any 64-bit input
-        yi[Nm + j] = h;
-    }
-}
 
 // Product lengths: z = a b with na, nb from the children; 0 if either is 0.
 __global__ void product_len_kernel(const uint32_t* la, const uint32_t* lb, size_t c0, size_t npar, int a_off,
@@ -1296,7 +1235,6 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
     const uint32_t cmax = std::max(ccP, std::max(ccQ, ccR));
     const int k = sh.k;
     const size_t N = sh.N, ST = sh.stride, T = sh.T;
-    const uint64_t P0 = kProductPrimes[0], P1 = kProductPrimes[1], P2 = kProductPrimes[2];
     const Mod64 m0 = prime_mod(0), m1 = prime_mod(1), m2 = prime_mod(2);
     const bool needR = o.R != nullptr;
     // tail scale Nm / T in Montgomery form (mont_mul(x, c) = x Nm / T)
@@ -1309,29 +1247,6 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         DevBuf<uint64_t> bP(3 * nc * ST, s), bQ(3 * nc * ST, s), bR(3 * nc * ST, s);
         DevBuf<uint64_t> tP(sh.wrap ? 3 * nc * T : 0, s), tQ(sh.wrap ? 3 * nc * T : 0, s),
             tR(sh.wrap ? 3 * nc * T : 0, s);
-        {
-            const size_t tot = nc * N;
-            ProfScope ps(KC_SPLIT, 3.0 * (4.0 * (double)nc * cmax + 24.0 * (double)tot), s);
-            slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bP.get(), ch.P.w.get(), ch.P.len.get(), ccP, c0, nc,
-                                                                 k, ST, 0, P0, P1, P2);
-            slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bQ.get(), ch.Q.w.get(), ch.Q.len.get(), ccQ, c0, nc,
-                                                                 k, ST, 0, P0, P1, P2);
-            slot_split_kernel<<<grid_for(tot, 256), 256, 0, s>>>(bR.get(), ch.R.w.get(), ch.R.len.get(), ccR, c0, nc,
-                                                                 k, ST, 0, P0, P1, P2);
-            PIC_CHECK_LAUNCH();
-            count_launch(3);
-            if (sh.wrap) {
-                const size_t tt = nc * T;
-                slot_split_kernel<<<grid_for(tt, 256), 256, 0, s>>>(tP.get(), ch.P.w.get(), ch.P.len.get(), ccP, c0,
-                                                                    nc, sh.kt, T, sh.t0, P0, P1, P2);
-                slot_split_kernel<<<grid_for(tt, 256), 256, 0, s>>>(tQ.get(), ch.Q.w.get(), ch.Q.len.get(), ccQ, c0,
-                                                                    nc, sh.kt, T, sh.t0, P0, P1, P2);
-                slot_split_kernel<<<grid_for(tt, 256), 256, 0, s>>>(tR.get(), ch.R.w.get(), ch.R.len.get(), ccR, c0,
-                                                                    nc, sh.kt, T, sh.t0, P0, P1, P2);
-                PIC_CHECK_LAUNCH();
-                count_launch(3);
-            }
-        }
         NttBatch fb;
         fb.stride = ST;
         fb.count = (int)(3 * nc);
@@ -1339,15 +1254,30 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         for (int q = 0; q < 3; q++) fb.prime[q] = prime_tables(kProductPrimes[q]).dev;
         NttBatch tb = fb;
         tb.stride = T;
-        for (uint64_t* d : {bP.get(), bQ.get(), bR.get()}) {
-            fb.data = d;
+        // the children's words are split into residues by each transform's
+        // first pass (SplitSrc): main transforms from piece 0, tails from t0
+        const Slots* arrays[3] = {&ch.P, &ch.Q, &ch.R};
+        uint64_t* mains[3] = {bP.get(), bQ.get(), bR.get()};
+        uint64_t* tails[3] = {tP.get(), tQ.get(), tR.get()};
+        for (int a = 0; a < 3; a++) {
+            SplitSrc src;
+            src.words = arrays[a]->w.get();
+            src.len = arrays[a]->len.get();
+            src.cap = arrays[a]->cap;
+            src.c0 = c0;
+            src.first = 0;
+            fb.data = mains[a];
+            fb.src = src;
             ntt_forward_dif(fb, k, s);
-        }
-        if (sh.wrap)
-            for (uint64_t* d : {tP.get(), tQ.get(), tR.get()}) {
-                tb.data = d;
+            if (sh.wrap) {
+                src.first = sh.t0;
+                tb.data = tails[a];
+                tb.src = src;
                 ntt_forward_dif(tb, sh.kt, s);
             }
+        }
+        fb.src = SplitSrc{};
+        tb.src = SplitSrc{};
         {
             ProfScope ps(KC_NTT_POINTWISE, 3.0 * 3 * np * (double)(N + T) * 80.0 / 8.0, s);
             launch_merge_pointwise(bP.get(), bQ.get(), bR.get(), np, k, ST, m0, m1, m2, s);
@@ -1387,13 +1317,10 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
             }
             ProfScope ps(KC_NTT_POINTWISE, 3.0 * 4 * np * (double)sh.W * 24.0, s);
             const size_t W = sh.W;
-            wrap_fix_kernel<<<grid_for(3 * nc * W, 256), 256, 0, s>>>(bP.get(), ST, tP.get(), T, nc, 1, nc, N, W, m0,
-                                                                      m1, m2, cT[0], cT[1], cT[2]);
-            wrap_fix_kernel<<<grid_for(3 * np * W, 256), 256, 0, s>>>(bQ.get(), ST, tQ.get(), T, np, 2, nc, N, W, m0,
-                                                                      m1, m2, cT[0], cT[1], cT[2]);
+            launch_wrap_fix(bP.get(), ST, tP.get(), T, nc, 1, nc, N, W, cT, s);
+            launch_wrap_fix(bQ.get(), ST, tQ.get(), T, np, 2, nc, N, W, cT, s);
             if (needR)
-                wrap_fix_kernel<<<grid_for(3 * np * W, 256), 256, 0, s>>>(bR.get(), ST, tR.get(), T, np, 2, nc, N, W,
-                                                                          m0, m1, m2, cT[0], cT[1], cT[2]);
+                launch_wrap_fix(bR.get(), ST, tR.get(), T, np, 2, nc, N, W, cT, s);
             PIC_CHECK_LAUNCH();
             count_launch(needR ? 3 : 2);
         }
@@ -1418,9 +1345,6 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         count_launch(needR ? 4 : 3);
     }
     (void)cmax;
-    (void)P0;
-    (void)P1;
-    (void)P2;
 }
 
 static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)

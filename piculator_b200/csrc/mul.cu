@@ -40,6 +40,28 @@ __global__ void split3_kernel(uint64_t* __restrict__ out, const uint32_t* __rest
     }
 }
 
+// Pieces first .. first + 2^k - 1 of a (zero past its end) -> residues at
+// out + q * stride.
+__global__ void split3_off_kernel(uint64_t* __restrict__ out, size_t stride, const uint32_t* __restrict__ a,
+                                  size_t na, size_t first, size_t N, uint64_t p0, uint64_t p1, uint64_t p2)
+{
+    for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < N; j += (size_t)gridDim.x * blockDim.x) {
+        const size_t wi = 2 * (first + j);
+        uint64_t v = 0;
+        if (wi < na) {
+            v = a[wi];
+            if (wi + 1 < na) v |= (uint64_t)a[wi + 1] << 32;
+        }
+        uint64_t r0 = v, r1 = v, r2 = v;
+        while (r0 >= p0) r0 -= p0;
+        while (r1 >= p1) r1 -= p1;
+        while (r2 >= p2) r2 -= p2;
+        out[j] = r0;
+        out[stride + j] = r1;
+        out[2 * stride + j] = r2;
+    }
+}
+
 // Reference layout, int_to_ntt NTT.cpp:330-341: two 16-bit points per word.
 __global__ void split16_kernel(uint64_t* __restrict__ T, size_t N, const uint32_t* __restrict__ A, size_t AL)
 {
@@ -440,7 +462,119 @@ void crt3_to_words_scratch(const uint64_t* y, int k, size_t ncoef, uint32_t* z, 
     carry_ripple(z, zw, kCvtWPC, agg, nctas, kCarryAdd, s);
 }
 
+// Wrapped products.  A product of operands of sa and sb pieces has
+// L = sa + sb - 1 coefficients c_0..c_(L-1).  When L exceeds the main
+// transform length Nm (but sa, sb <= Nm), the cyclic product of length Nm
+// holds c_j + c_(Nm+j) for j < W = L - Nm.  The W top coefficients depend only
+// on the top W pieces of each operand (a from index Nm - sb + 1, b from
+// Nm - sa + 1): the product of those pieces, d, gives c_(Nm+j) = d_(W-1+j),
+// and its cyclic length T >= 2W - 1 keeps those indices free of wrap.  For
+// each of the W positions:
+//   y[j] <- y[j] - h (kept nonnegative by adding 2p), y[Nm + j] <- h
+// (inverse outputs arrive in [0, 4p) and are first brought below 2p),
+// with h = d_(W-1+j) * Nm / T so that both halves carry the same scale Nm.
+// y items have stride ystride >= Nm + W; tail items have stride T.  `item`
+// selects which children hold products (all for P, the even ones for Q, R).
+__global__ void wrap_fix_kernel(uint64_t* __restrict__ y, size_t ystride, const uint64_t* __restrict__ tail,
+                                size_t T, size_t nitems, size_t item_mul, size_t nchild, size_t Nm, size_t W,
+                                Mod64 m0, Mod64 m1, Mod64 m2, uint64_t c0, uint64_t c1, uint64_t c2)
+{
+    const size_t total = 3 * nitems * W;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
+        const size_t q = g / (nitems * W);
+        const size_t r = g - q * nitems * W;
+        const size_t it = r / W, j = r - it * W;
+        const Mod64& M = q == 0 ? m0 : (q == 1 ? m1 : m2);
+        const uint64_t cT = q == 0 ? c0 : (q == 1 ? c1 : c2);
+        const size_t child = q * nchild + it * item_mul;
+        const uint64_t h = mont_mul(tail[child * T + W - 1 + j], cT, M);  // < p
+        uint64_t* yi = y + child * ystride;
+        const uint64_t p2 = 2 * M.p;
+        uint64_t v = yi[j];  // lazy inverse output, < 4p
+        v = v >= p2 ? v - p2 : v;
+        yi[j] = v + p2 - h;  // < 4p < 2^64: the CRT reduces any 64-bit input
+        yi[Nm + j] = h;
+    }
+}
+
+void launch_wrap_fix(uint64_t* y, size_t ystride, const uint64_t* tail, size_t T, size_t nitems, size_t item_mul,
+                     size_t nchild, size_t Nm, size_t W, const uint64_t cT[3], cudaStream_t s)
+{
+    const Mod64 m0 = make_mod(kProductPrimes[0]), m1 = make_mod(kProductPrimes[1]), m2 = make_mod(kProductPrimes[2]);
+    wrap_fix_kernel<<<grid_for(3 * nitems * W, 256), 256, 0, s>>>(y, ystride, tail, T, nitems, item_mul, nchild, Nm,
+                                                                W, m0, m1, m2, cT[0], cT[1], cT[2]);
+    PIC_CHECK_LAUNCH();
+}
+
 // ---- products ----------------------------------------------------------------
+static bool g_mul_wrap = true;
+void mul_set_wrap(bool on) { g_mul_wrap = on; }
+bool mul_wrap() { return g_mul_wrap; }
+
+static NttBatch ntt3_batch_stride(uint64_t* data, size_t stride)
+{
+    NttBatch bat;
+    bat.data = data;
+    bat.stride = stride;
+    bat.count = 3;
+    bat.per_prime = 1;
+    for (int q = 0; q < 3; q++) bat.prime[q] = prime_tables(kProductPrimes[q]).dev;
+    return bat;
+}
+
+// The wrapped form of mul_ntt3 (see wrap_fix_kernel): main transforms of
+// length Nm = 2^km, tails of length 2^kt over the top W pieces.
+static void mul_ntt3_wrapped(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int km,
+                             int kt, cudaStream_t s)
+{
+    const size_t zw = na + nb;
+    const size_t pa = (na + 1) / 2, pb = (nb + 1) / 2;
+    const size_t L = pa + pb - 1;
+    const size_t Nm = (size_t)1 << km, T = (size_t)1 << kt, W = L - Nm;
+    const size_t ST = Nm + ((W + 15) & ~(size_t)15);
+    const bool square = (a == b && na == nb);
+    const uint64_t P0 = kProductPrimes[0], P1 = kProductPrimes[1], P2 = kProductPrimes[2];
+    DevBuf<uint64_t> A(3 * ST, s), B(square ? 0 : 3 * ST, s), tA(3 * T, s), tB(square ? 0 : 3 * T, s);
+    {
+        ProfScope ps(KC_SPLIT, 4.0 * (double)(na + nb) + 24.0 * (double)(2 * (Nm + T)), s);
+        split3_off_kernel<<<grid_for(Nm, 256), 256, 0, s>>>(A.get(), ST, a, na, 0, Nm, P0, P1, P2);
+        split3_off_kernel<<<grid_for(T, 256), 256, 0, s>>>(tA.get(), T, a, na, Nm - pb + 1, T, P0, P1, P2);
+        if (!square) {
+            split3_off_kernel<<<grid_for(Nm, 256), 256, 0, s>>>(B.get(), ST, b, nb, 0, Nm, P0, P1, P2);
+            split3_off_kernel<<<grid_for(T, 256), 256, 0, s>>>(tB.get(), T, b, nb, Nm - pa + 1, T, P0, P1, P2);
+        }
+        PIC_CHECK_LAUNCH();
+        count_launch(square ? 2 : 4);
+    }
+    const NttBatch mA = ntt3_batch_stride(A.get(), ST), mB = ntt3_batch_stride(B.get(), ST);
+    const NttBatch xA = ntt3_batch_stride(tA.get(), T), xB = ntt3_batch_stride(tB.get(), T);
+    ntt_forward_dif(mA, km, s);
+    ntt_forward_dif(xA, kt, s);
+    if (!square) {
+        ntt_forward_dif(mB, km, s);
+        ntt_forward_dif(xB, kt, s);
+    }
+    ntt_pointwise_mont(mA, square ? A.get() : B.get(), km, s);
+    ntt_pointwise_mont(xA, square ? tA.get() : tB.get(), kt, s);
+    ntt_inverse_dit(mA, km, s);
+    ntt_inverse_dit(xA, kt, s);
+    uint64_t cT[3];
+    for (int q = 0; q < 3; q++) cT[q] = to_mont((uint64_t)(Nm / T), kProductPrimes[q]);
+    {
+        ProfScope ps(KC_NTT_POINTWISE, 3.0 * (double)W * 24.0, s);
+        launch_wrap_fix(A.get(), ST, tA.get(), T, 1, 1, 1, Nm, W, cT, s);
+        count_launch();
+    }
+    const Crt3Consts C = make_crt3(km, 1);
+    const size_t nctas = crt3_scratch_ctas(zw);
+    DevBuf<uint32_t> agg(nctas, s);
+    ProfScope ps(KC_CRT, 24.0 * (double)L + 4.0 * (double)zw, s);
+    crt3_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(A.get(), ST, L, C, z, zw, agg.get());
+    PIC_CHECK_LAUNCH();
+    count_launch();
+    finish_scan(z, zw, agg.get(), nctas, s);
+}
+
 void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s)
 {
     const size_t zw = na + nb;
@@ -450,6 +584,19 @@ void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size
     if (k < 1) k = 1;
     PIC_REQUIRE(k <= 30, PIC_ERR_LENGTH, "product too long for the three-prime NTT (2^30 points)");
     const size_t N = (size_t)1 << k;
+    if (g_mul_wrap && k >= 4) {
+        // wrapped when the product just exceeds a power of two and the tail is short
+        const size_t Nm = N / 2;
+        if (std::max(pa, pb) <= Nm && ncoef > Nm) {
+            const size_t W = ncoef - Nm;
+            int kt = ceil_log2(2 * W - 1);
+            if (kt < 2) kt = 2;
+            if (((size_t)1 << kt) <= Nm / 2) {
+                mul_ntt3_wrapped(z, a, na, b, nb, k - 1, kt, s);
+                return;
+            }
+        }
+    }
     const bool square = (a == b && na == nb);
     DevBuf<uint64_t> A(3 * N, s);
     DevBuf<uint64_t> B(square ? 0 : 3 * N, s);

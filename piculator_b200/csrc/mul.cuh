@@ -35,6 +35,17 @@ void ntt3_inverse_to_words(uint64_t* y, int k, size_t ncoef, int depth, uint32_t
 // factor); zlen[i] words into z + i * zcap.  ncoef (default 2^k) is the number
 // of coefficients read per product: a wrapped product stores its top
 // coefficients past the transform, at indices 2^k .. ncoef - 1.
+// Wrapped form of the three-prime product in mul_ntt3 (on by default).
+void mul_set_wrap(bool on);
+bool mul_wrap();
+
+// Wrapped products (see wrap_fix_kernel in mul.cu): nitems products, item
+// it of prime q at y + (q nchild + it item_mul) ystride (main, length Nm) and
+// tail + (q nchild + it item_mul) T (tail product, length T); cT = Nm / T in
+// Montgomery form per prime.
+void launch_wrap_fix(uint64_t* y, size_t ystride, const uint64_t* tail, size_t T, size_t nitems, size_t item_mul,
+                     size_t nchild, size_t Nm, size_t W, const uint64_t cT[3], cudaStream_t s);
+
 void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
                          uint32_t zcap, const uint32_t* zlen, cudaStream_t s, size_t ncoef = 0);
 

@@ -598,6 +598,34 @@ __device__ __forceinline__ LazyPrime lazy_prime(const PrimeDev& P)
     return L;
 }
 
+// Piece j of batch item tr from the item's child slot (SplitSrc), reduced to
+// [0, 2p) (a 64-bit piece is below 6p for the lazy primes).
+struct SrcRow {
+    const uint32_t* x;
+    uint32_t n;
+};
+
+__device__ __forceinline__ SrcRow src_row(const NttBatch& B, int tr)
+{
+    const size_t c = B.src.c0 + (size_t)(tr % B.per_prime);
+    SrcRow r;
+    r.x = B.src.words + c * (size_t)B.src.cap;
+    r.n = B.src.len[c];
+    return r;
+}
+
+__device__ __forceinline__ uint64_t src_piece(const NttBatch& B, const SrcRow& r, size_t j, uint64_t p2)
+{
+    const size_t wi = 2 * (B.src.first + j);
+    uint64_t v = 0;
+    if (wi < r.n) {
+        v = __ldg(r.x + wi);
+        if (wi + 1 < r.n) v |= (uint64_t)__ldg(r.x + wi + 1) << 32;
+    }
+    v = v >= p2 ? v - p2 : v;
+    return v >= p2 ? v - p2 : v;
+}
+
 // Forward (DIF): operands and results in [0, 2p).
 __device__ __forceinline__ void fbfly_dif(uint64_t& a, uint64_t& b, const ulonglong2 t, const LazyPrime& L)
 {
@@ -753,14 +781,31 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC>::NT, 1024 / RowsFastSh
     const size_t nrows = (size_t)B.count << lrow;
     const PrimeDev P = pick_prime(B, (int)(row0 >> lrow));
     const LazyPrime L = lazy_prime(P);
+    if (!INV && B.src.words != nullptr) {
+        // first forward pass of a single-pass length (row == transform): the
+        // input comes from the child slots
 #pragma unroll
-    for (int i = 0; i < TOT / NT; i++) {
-        const int idx = threadIdx.x + i * NT;
-        const size_t row = row0 + (idx >> LR);
-        uint64_t v = 0;
-        if (LRPC == 0 || row < nrows)
-            v = B.data[(row >> lrow) * B.stride + ((row & rmask) << LR) + (idx & EMASK)];
-        smem[(idx & ~EMASK) + swz(idx & EMASK)] = v;
+        for (int i = 0; i < TOT / NT; i++) {
+            const int idx = threadIdx.x + i * NT;
+            const size_t row = row0 + (idx >> LR);
+            uint64_t v = 0;
+            if (LRPC == 0 || row < nrows) {
+                const int tr = (int)row;
+                const uint64_t p2 = 2 * pick_prime(B, tr).p;
+                v = src_piece(B, src_row(B, tr), idx & EMASK, p2);
+            }
+            smem[(idx & ~EMASK) + swz(idx & EMASK)] = v;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < TOT / NT; i++) {
+            const int idx = threadIdx.x + i * NT;
+            const size_t row = row0 + (idx >> LR);
+            uint64_t v = 0;
+            if (LRPC == 0 || row < nrows)
+                v = B.data[(row >> lrow) * B.stride + ((row & rmask) << LR) + (idx & EMASK)];
+            smem[(idx & ~EMASK) + swz(idx & EMASK)] = v;
+        }
     }
     __syncthreads();
     rows_fast_round<INV, LR, LRPC, NT, 0>(smem, B, row0, L,
@@ -874,12 +919,23 @@ __global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatc
         const ulonglong2 h = __ldg(shi + (E >> S)), l = __ldg(slo + (E & smask));
         return shoup_lazy32(shoup_lazy32(v, h.x, h.y, L.c), l.x, l.y, L.c);
     };
+    if (!INV && B.src.words != nullptr) {
+        // first forward column pass (lpre == 0): the input comes from the
+        // child slot, point m M + c0 + w
+        const SrcRow sr = src_row(B, tr);
 #pragma unroll 8
-    for (int idx = threadIdx.x; idx < TOT; idx += 256) {
-        const int m = idx >> LW, w = idx & WMASK;
-        uint64_t v = base[((size_t)m << lM) + w];
-        if (INV) v = twiddle(v, m, w);
-        smem[idx] = v;
+        for (int idx = threadIdx.x; idx < TOT; idx += 256) {
+            const int m = idx >> LW, w = idx & WMASK;
+            smem[idx] = src_piece(B, sr, ((size_t)m << lM) + c0 + w, L.p2);
+        }
+    } else {
+#pragma unroll 8
+        for (int idx = threadIdx.x; idx < TOT; idx += 256) {
+            const int m = idx >> LW, w = idx & WMASK;
+            uint64_t v = base[((size_t)m << lM) + w];
+            if (INV) v = twiddle(v, m, w);
+            smem[idx] = v;
+        }
     }
     __syncthreads();
     cols_fast_round<INV, LC, LW, 0>(smem, L, reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
@@ -890,6 +946,30 @@ __global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatc
         if (!INV) v = twiddle(v, m, w);
         base[((size_t)m << lM) + w] = v;
     }
+}
+
+// The SplitSrc input written into `data` (for passes that read `data`).
+__global__ void src_split_kernel(NttBatch B, int k)
+{
+    const size_t N = (size_t)1 << k;
+    const size_t total = (size_t)B.count * N;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
+        const int tr = (int)(g >> k);
+        const size_t j = g & (N - 1);
+        const PrimeDev P = pick_prime(B, tr);
+        uint64_t v = src_piece(B, src_row(B, tr), j, 2 * P.p);
+        while (v >= P.p) v -= P.p;  // strict primes take [0, p)
+        B.data[(size_t)tr * B.stride + j] = v;
+    }
+}
+
+static void materialize_src(const NttBatch& b, int k, cudaStream_t s)
+{
+    const size_t total = (size_t)b.count << k;
+    ProfScope ps(KC_SPLIT, (4.0 + 8.0) * (double)total, s);
+    src_split_kernel<<<grid_for(total, 256), 256, 0, s>>>(b, k);
+    PIC_CHECK_LAUNCH();
+    count_launch();
 }
 
 template <typename K>
@@ -1037,6 +1117,7 @@ static void launch_rows(bool inv, const NttBatch& b, int k, int lr, cudaStream_t
             return;
         }
     }
+    if (!inv && b.src.words != nullptr) materialize_src(b, k, s);  // the general kernels read `data`
     int lrpc = 0;
     if (lr == k) {
         // several whole transforms per CTA when short, never straddling primes
@@ -1090,6 +1171,7 @@ static void launch_cols(bool inv, const NttBatch& b, int k, int lpre, int lc, cu
         count_launch();
         return;
     }
+    if (!inv && b.src.words != nullptr) materialize_src(b, k, s);  // the general kernels read `data`
     const bool lazy = b.prime[0].lazy != 0;
 #define PIC_COLS(I, Z, R)                                                                          \
     do {                                                                                         \
@@ -1127,16 +1209,20 @@ void ntt_forward_dif(const NttBatch& b, int k, cudaStream_t s)
 {
     check_batch(b, k);
     std::vector<int> bits = ntt_pass_bits(k);
+    NttBatch rest = b;
+    rest.src = SplitSrc{};  // only the first pass reads the child slots
     int lpre = 0;
     for (size_t i = 0; i + 1 < bits.size(); i++) {
-        launch_cols(false, b, k, lpre, bits[i], s);
+        launch_cols(false, i == 0 ? b : rest, k, lpre, bits[i], s);
         lpre += bits[i];
     }
-    launch_rows(false, b, k, bits.back(), s);
+    launch_rows(false, bits.size() == 1 ? b : rest, k, bits.back(), s);
 }
 
-void ntt_inverse_dit(const NttBatch& b, int k, cudaStream_t s)
+void ntt_inverse_dit(const NttBatch& b_in, int k, cudaStream_t s)
 {
+    NttBatch b = b_in;
+    b.src = SplitSrc{};
     check_batch(b, k);
     std::vector<int> bits = ntt_pass_bits(k);
     launch_rows(true, b, k, bits.back(), s);

@@ -78,12 +78,26 @@ extern const uint64_t kProductPrimes[3];
 
 // A batch of transforms of length 2^k laid out at data + i * stride
 // (i < count); transform i uses prime[i / per_prime].
+// A forward transform's input read straight from binary-splitting child
+// slots instead of `data`: item i (prime i / per_prime, child
+// c0 + i % per_prime) takes 64-bit pieces first + j of the child's words
+// (cap words per slot, len[child] of them used, zero above), reduced mod the
+// item's prime.  Only the first pass reads it; every pass writes `data`.
+struct SplitSrc {
+    const uint32_t* words = nullptr;  // null: the input is already in `data`
+    const uint32_t* len = nullptr;
+    uint32_t cap = 0;
+    size_t c0 = 0;
+    size_t first = 0;
+};
+
 struct NttBatch {
     uint64_t* data;
     size_t stride;
     int count;
     int per_prime;
     PrimeDev prime[kMaxPrimesPerBatch];
+    SplitSrc src;
 };
 
 void ntt_forward_dif(const NttBatch& b, int k, cudaStream_t s);

@@ -93,6 +93,35 @@ def test_all_ones_max_carry_chain(pic):
             assert z[n] == 0xFFFFFFFE and np.all(z[n + 1:] == 0xFFFFFFFF)
 
 
+# Sizes whose coefficient count just exceeds a power of two: the three-prime
+# product takes the wrapped form (main transform at the smaller power plus a
+# tail product), for equal, unequal and odd operand lengths.
+@pytest.mark.parametrize("na,nb", [(2200, 2200), (2201, 2199), (3000, 1300), (60000, 10000), (92000, 46000)])
+def test_wrapped_products(pic, na, nb):
+    a = random_words(na + 5, na)
+    b = random_words(nb + 9, nb)
+    want = _int(a) * _int(b)
+    saved = pic.get_tuning(pic.TUNE_MUL_WRAP)
+    try:
+        for wrap in (1, 0):
+            pic.set_tuning(pic.TUNE_MUL_WRAP, wrap)
+            z = pic.mul_host(a, b, "ntt3")
+            assert _int(z) == want, f"wrap={wrap}"
+    finally:
+        pic.set_tuning(pic.TUNE_MUL_WRAP, saved)
+
+
+def test_wrapped_square_same_pointer(pic, torch_cuda):
+    torch = torch_cuda
+    n = 2200
+    a = random_words(91, n)
+    ta = torch.from_numpy(a.view(np.int32)).cuda()
+    z = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+    pic.mul_dev(z.data_ptr(), ta.data_ptr(), n, ta.data_ptr(), n, "ntt3", torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert _int(z.cpu().numpy().view(np.uint32)) == _int(a) ** 2
+
+
 def test_squaring_same_pointer(pic, torch_cuda, oracle):
     torch = torch_cuda
     a = random_words(77, 3000)
