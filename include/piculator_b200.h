@@ -237,7 +237,8 @@ enum {
     PIC_TUNE_BATCH_GRAPHS = 3,   /* 1: pic_mul_batch replays captured CUDA graphs (default) */
     PIC_TUNE_BSR_WRAP = 4,       /* 1: binary-splitting NTT merges use wrapped products (default) */
     PIC_TUNE_BSR_SMALL_MERGE = 5, /* short schoolbook levels: 0 CTA, 1 + warp, 2 + thread per parent (default) */
-    PIC_TUNE_MUL_WRAP = 6         /* 1: three-prime products use the wrapped form when it is shorter (default) */
+    PIC_TUNE_MUL_WRAP = 6,        /* 1: three-prime products use the wrapped form when it is shorter (default) */
+    PIC_TUNE_BSR_COMBINE = 7      /* 1: binary-splitting NTT merges form P in the transform domain (default) */
 };
 pic_status pic_set_tuning(int knob, int64_t value);
 int64_t pic_get_tuning(int knob);

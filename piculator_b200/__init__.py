@@ -339,7 +339,7 @@ class Transform:
 
 
 (TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS, TUNE_BSR_WRAP,
- TUNE_BSR_SMALL_MERGE, TUNE_MUL_WRAP) = range(7)
+ TUNE_BSR_SMALL_MERGE, TUNE_MUL_WRAP, TUNE_BSR_COMBINE) = range(8)
 
 
 def butterfly_rate() -> float:

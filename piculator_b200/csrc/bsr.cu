@@ -801,10 +801,12 @@ __global__ void __launch_bounds__(32 * kWarpMergeWarps) merge_warp_kernel(MergeA
 // For every parent i and prime q (arrays laid out [q][child][stride], the
 // transforms of length 2^k at the start of each item):
 //   T1 = PL QR -> P[2i], T2 = PR RL -> P[2i+1], Q = QL QR -> Q[2i], R = RL RR -> R[2i]
+// or, with the children's P signs `sgn` (parent i at sgn[2i], sgn[2i + 1]),
+//   T1 +- T2 -> P[2i] (plus when the signs agree), nothing in P[2i+1].
 __global__ void __launch_bounds__(256) merge_pointwise_kernel(uint64_t* __restrict__ P, uint64_t* __restrict__ Q,
                                                               uint64_t* __restrict__ R, uint32_t npar, int k,
                                                               size_t stride, uint32_t jbpr, Mod64 m0, Mod64 m1,
-                                                              Mod64 m2)
+                                                              Mod64 m2, const uint8_t* __restrict__ sgn)
 {
     // block -> (prime q, parent i, run of 512 points); two points per thread
     const uint32_t row = blockIdx.x / jbpr, jb = blockIdx.x - row * jbpr;
@@ -817,21 +819,33 @@ __global__ void __launch_bounds__(256) merge_pointwise_kernel(uint64_t* __restri
     const ulonglong2 pl = *reinterpret_cast<const ulonglong2*>(P + L), pr = *reinterpret_cast<const ulonglong2*>(P + Rr);
     const ulonglong2 ql = *reinterpret_cast<const ulonglong2*>(Q + L), qr = *reinterpret_cast<const ulonglong2*>(Q + Rr);
     const ulonglong2 rl = *reinterpret_cast<const ulonglong2*>(R + L), rr = *reinterpret_cast<const ulonglong2*>(R + Rr);
-    *reinterpret_cast<ulonglong2*>(P + L) = make_ulonglong2(mont_mul(pl.x, qr.x, M), mont_mul(pl.y, qr.y, M));
-    *reinterpret_cast<ulonglong2*>(P + Rr) = make_ulonglong2(mont_mul(pr.x, rl.x, M), mont_mul(pr.y, rl.y, M));
+    if (sgn != nullptr) {
+        // P[2i] = T1 + T2 if the children's P have one sign, T1 - T2 otherwise
+        const bool same = (sgn[2 * i] != 0) == (sgn[2 * i + 1] != 0);
+        const uint64_t ax = mont_mul(pl.x, qr.x, M), ay = mont_mul(pl.y, qr.y, M);
+        const uint64_t bx = mont_mul(pr.x, rl.x, M), by = mont_mul(pr.y, rl.y, M);
+        *reinterpret_cast<ulonglong2*>(P + L) =
+            same ? make_ulonglong2(add_mod(ax, bx, M.p), add_mod(ay, by, M.p))
+                 : make_ulonglong2(sub_mod(ax, bx, M.p), sub_mod(ay, by, M.p));
+    } else {
+        *reinterpret_cast<ulonglong2*>(P + L) = make_ulonglong2(mont_mul(pl.x, qr.x, M), mont_mul(pl.y, qr.y, M));
+        *reinterpret_cast<ulonglong2*>(P + Rr) = make_ulonglong2(mont_mul(pr.x, rl.x, M), mont_mul(pr.y, rl.y, M));
+    }
     *reinterpret_cast<ulonglong2*>(Q + L) = make_ulonglong2(mont_mul(ql.x, qr.x, M), mont_mul(ql.y, qr.y, M));
     *reinterpret_cast<ulonglong2*>(R + L) = make_ulonglong2(mont_mul(rl.x, rr.x, M), mont_mul(rl.y, rr.y, M));
 }
 
 // Launch over 3 primes x npar parents x 2^k points (stride even, 2^k >= 2).
 static void launch_merge_pointwise(uint64_t* P, uint64_t* Q, uint64_t* R, size_t npar, int k, size_t stride,
-                                   const Mod64& m0, const Mod64& m1, const Mod64& m2, cudaStream_t s)
+                                   const Mod64& m0, const Mod64& m1, const Mod64& m2, const uint8_t* sgn,
+                                   cudaStream_t s)
 {
     PIC_REQUIRE(k >= 1 && stride % 2 == 0 && npar <= 0x7fffffffu / 3, PIC_ERR_INVALID, "pointwise merge shape");
     const uint32_t jbpr = (uint32_t)((((size_t)1 << k) + 511) / 512);
     const size_t blocks = 3 * npar * (size_t)jbpr;
     PIC_REQUIRE(blocks <= 0x7fffffffu, PIC_ERR_INVALID, "pointwise merge grid too large");
-    merge_pointwise_kernel<<<(unsigned)blocks, 256, 0, s>>>(P, Q, R, (uint32_t)npar, k, stride, jbpr, m0, m1, m2);
+    merge_pointwise_kernel<<<(unsigned)blocks, 256, 0, s>>>(P, Q, R, (uint32_t)npar, k, stride, jbpr, m0, m1, m2,
+                                                            sgn);
 }
 
 
@@ -863,11 +877,12 @@ __global__ void __launch_bounds__(256) signed_add_kernel(const uint32_t* __restr
 {
     const size_t i = blockIdx.x;
     const uint32_t na = l1[i], nb = l2[i];
-    const bool sa = cS[2 * (c0 + i)] != 0, sb = cS[2 * (c0 + i) + 1] != 0;
+    const bool sa = cS[2 * i] != 0, sb = cS[2 * i + 1] != 0;
     const uint32_t* a = t1 + i * (size_t)c1;
     const uint32_t* b = t2 + i * (size_t)c2;
     uint32_t* z = Pw + (c0 + i) * (size_t)cP;
     const uint32_t n = max(na, nb);
+    const uint32_t nz = min(n, cP);  // words past the slot are zero in the result
     auto A = [&](uint32_t k) -> uint32_t { return k < na ? a[k] : 0u; };
     auto B = [&](uint32_t k) -> uint32_t { return k < nb ? b[k] : 0u; };
     const bool sub = sa != sb;
@@ -926,7 +941,7 @@ __global__ void __launch_bounds__(256) signed_add_kernel(const uint32_t* __restr
 #pragma unroll
         for (int u = 0; u < IPT; u++) {
             const uint32_t k = w0 + u;
-            if (k >= n) break;
+            if (k >= nz) break;
             const uint32_t x = swap ? B(k) : A(k), y = swap ? A(k) : B(k);
             if (!sub) {
                 const uint64_t s = (uint64_t)x + y;
@@ -946,7 +961,7 @@ __global__ void __launch_bounds__(256) signed_add_kernel(const uint32_t* __restr
     if (!sub) {
         if (threadIdx.x == 0) {
             const uint32_t c = s_carry;
-            if (c) z[n] = 1;
+            if (c && n < cP) z[n] = 1;
             Pl[c0 + i] = n + (c ? 1 : 0);
             Ps[c0 + i] = sa ? 1 : 0;
         }
@@ -955,7 +970,7 @@ __global__ void __launch_bounds__(256) signed_add_kernel(const uint32_t* __restr
     // strip leading zeros after a subtraction, scanning down from the top
     __syncthreads();
     uint32_t l = 0;
-    for (uint32_t top = n; top > 0 && l == 0;) {
+    for (uint32_t top = nz; top > 0 && l == 0;) {
         const uint32_t lo = top > blockDim.x ? top - blockDim.x : 0;
         const uint32_t k = lo + threadIdx.x;
         unsigned long long mine = (k < top && z[k] != 0) ? k + 1 : 0;
@@ -982,7 +997,7 @@ constexpr uint32_t kWideWPC = 256 * kWideIPT;
 struct WideAdd {
     const uint32_t *t1, *l1, *t2, *l2;
     uint32_t c1, c2;
-    const uint8_t* cS;  // children's P signs
+    const uint8_t* cS;  // signs of the two addends of parent i at cS[2i], cS[2i + 1]
     size_t c0;          // first parent (level index)
     uint32_t *Pw, *Pl, cP;
     uint8_t* Ps;
@@ -999,7 +1014,7 @@ struct WideOp {
 __device__ __forceinline__ WideOp wide_op(const WideAdd& w, size_t i)
 {
     WideOp o;
-    const bool sa = w.cS[2 * (w.c0 + i)] != 0, sb = w.cS[2 * (w.c0 + i) + 1] != 0;
+    const bool sa = w.cS[2 * i] != 0, sb = w.cS[2 * i + 1] != 0;
     o.sub = sa != sb;
     o.swap = false;
     o.zero = false;
@@ -1076,7 +1091,7 @@ __global__ void __launch_bounds__(256) wide_k1_kernel(WideAdd w)
 #pragma unroll
     for (int u = 0; u < kWideIPT; u++) {
         const uint32_t k = w0 + u;
-        if (k >= n || o.zero) break;
+        if (k >= n || k >= w.cP || o.zero) break;  // words past the slot are zero in the result
         if (!o.sub) {
             const uint64_t sum = (uint64_t)xs[u] + ys[u];
             const uint32_t d = (uint32_t)sum;
@@ -1104,7 +1119,8 @@ __global__ void __launch_bounds__(256) wide_ripple_kernel(WideAdd w)
     const WideOp o = wide_op(w, i);
     if (o.zero) return;
     uint32_t* z = w.Pw + (w.c0 + i) * (size_t)w.cP;
-    const uint32_t b0 = (uint32_t)c * kWideWPC, e = min(b0 + kWideWPC, n);
+    const uint32_t b0 = (uint32_t)c * kWideWPC, e = min(min(b0 + kWideWPC, n), w.cP);
+    if (b0 >= e) return;
     const uint32_t stop = o.sub ? 0u : 0xffffffffu;  // words that pass the carry on
     unsigned long long mine = ~0ull;
     for (uint32_t k = b0 + threadIdx.x; k < e; k += blockDim.x)
@@ -1120,7 +1136,7 @@ __global__ void __launch_bounds__(256) wide_final_kernel(WideAdd w)
     const size_t i = blockIdx.x / w.cpp, c = blockIdx.x % w.cpp;
     const uint32_t n = max(w.l1[i], w.l2[i]);
     const WideOp o = wide_op(w, i);
-    const bool sa = w.cS[2 * (w.c0 + i)] != 0, sb = w.cS[2 * (w.c0 + i) + 1] != 0;
+    const bool sa = w.cS[2 * i] != 0, sb = w.cS[2 * i + 1] != 0;
     uint32_t* z = w.Pw + (w.c0 + i) * (size_t)w.cP;
     if (!o.sub) {
         // the carry out of the last chunk: its (G, P) joined with its carry-in
@@ -1128,7 +1144,7 @@ __global__ void __launch_bounds__(256) wide_final_kernel(WideAdd w)
         if (c == last && threadIdx.x == 0) {
             const uint32_t gp = w.aggc[blockIdx.x], cin = w.agg[blockIdx.x];
             const uint32_t carry = n ? ((gp & 1u) | ((gp >> 1) & cin)) : 0u;
-            if (carry) z[n] = 1;
+            if (carry && n < w.cP) z[n] = 1;
             w.Pl[w.c0 + i] = n + carry;
             w.Ps[w.c0 + i] = sa ? 1 : 0;
         }
@@ -1136,7 +1152,7 @@ __global__ void __launch_bounds__(256) wide_final_kernel(WideAdd w)
     }
     if (c == 0 && threadIdx.x == 0) w.Ps[w.c0 + i] = o.zero ? 1 : ((o.swap ? sb : sa) ? 1 : 0);
     if (o.zero) return;
-    const uint32_t b0 = (uint32_t)c * kWideWPC, e = min(b0 + kWideWPC, n);
+    const uint32_t b0 = (uint32_t)c * kWideWPC, e = min(min(b0 + kWideWPC, n), w.cP);
     unsigned long long mine = 0;
     for (uint32_t k = b0 + threadIdx.x; k < e; k += blockDim.x)
         if (z[k] != 0) mine = k + 1;
@@ -1220,7 +1236,21 @@ struct ProductsOut {
     uint32_t* R = nullptr;
     uint32_t cR = 0;
     uint32_t* lR = nullptr;
+    // Combined mode (csign != null, the children's P signs, parent i at
+    // csign[2i]): T1 receives V + K, V = T1 +- T2 (minus when the signs
+    // differ), K = sum_(j < ncoef) 2^(159 + 64 j), with ncoef from
+    // products_ncoef; c1 >= 2 ncoef + 6, l1 is set to 2 ncoef + 6; T2 unused.
+    const uint8_t* csign = nullptr;
 };
+
+// Coefficients the batched products of a level convert (main transform plus
+// wrapped top coefficients).
+static size_t products_ncoef(const MergeShape& sh) { return sh.wrap ? sh.N + sh.W : sh.N; }
+
+__global__ void fill_u32_kernel(uint32_t* p, size_t n, uint32_t v)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
 
 // Bytes of transform storage per parent for a level's NTT merge.
 static size_t ntt_bytes_per_parent(const MergeShape& sh) { return 3 * 2 * 3 * (sh.stride + sh.T) * sizeof(uint64_t); }
@@ -1241,7 +1271,7 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
     uint64_t cT[3] = {0, 0, 0};
     if (sh.wrap)
         for (int q = 0; q < 3; q++) cT[q] = to_mont((uint64_t)(N / T), kProductPrimes[q]);
-    const size_t ncoef = sh.wrap ? N + sh.W : N;
+    const size_t ncoef = products_ncoef(sh);
     {
         const size_t nc = 2 * np, c0 = 2 * p0;
         DevBuf<uint64_t> bP(3 * nc * ST, s), bQ(3 * nc * ST, s), bR(3 * nc * ST, s);
@@ -1280,20 +1310,27 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         tb.src = SplitSrc{};
         {
             ProfScope ps(KC_NTT_POINTWISE, 3.0 * 3 * np * (double)(N + T) * 80.0 / 8.0, s);
-            launch_merge_pointwise(bP.get(), bQ.get(), bR.get(), np, k, ST, m0, m1, m2, s);
-            if (sh.wrap) launch_merge_pointwise(tP.get(), tQ.get(), tR.get(), np, sh.kt, T, m0, m1, m2, s);
+            launch_merge_pointwise(bP.get(), bQ.get(), bR.get(), np, k, ST, m0, m1, m2, o.csign, s);
+            if (sh.wrap) launch_merge_pointwise(tP.get(), tQ.get(), tR.get(), np, sh.kt, T, m0, m1, m2, o.csign, s);
             PIC_CHECK_LAUNCH();
             count_launch(sh.wrap ? 2 : 1);
         }
-        // inverses: P holds T1, T2 for every parent (all items); Q, R the even items
+        // inverses: P holds T1, T2 for every parent (all items), or only the
+        // combined item 2i; Q, R the even items
+        const bool comb = o.csign != nullptr;
         {
-            NttBatch ib = fb;
-            ib.data = bP.get();
-            ntt_inverse_dit(ib, k, s);
             NttBatch eb = fb;
             eb.stride = 2 * ST;
             eb.count = (int)(3 * np);
             eb.per_prime = (int)np;
+            if (comb) {
+                eb.data = bP.get();
+                ntt_inverse_dit(eb, k, s);
+            } else {
+                NttBatch ib = fb;
+                ib.data = bP.get();
+                ntt_inverse_dit(ib, k, s);
+            }
             eb.data = bQ.get();
             ntt_inverse_dit(eb, k, s);
             if (needR) {
@@ -1302,13 +1339,18 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
             }
         }
         if (sh.wrap) {
-            NttBatch ib = tb;
-            ib.data = tP.get();
-            ntt_inverse_dit(ib, sh.kt, s);
             NttBatch eb = tb;
             eb.stride = 2 * T;
             eb.count = (int)(3 * np);
             eb.per_prime = (int)np;
+            if (comb) {
+                eb.data = tP.get();
+                ntt_inverse_dit(eb, sh.kt, s);
+            } else {
+                NttBatch ib = tb;
+                ib.data = tP.get();
+                ntt_inverse_dit(ib, sh.kt, s);
+            }
             eb.data = tQ.get();
             ntt_inverse_dit(eb, sh.kt, s);
             if (needR) {
@@ -1317,15 +1359,20 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
             }
             ProfScope ps(KC_NTT_POINTWISE, 3.0 * 4 * np * (double)sh.W * 24.0, s);
             const size_t W = sh.W;
-            launch_wrap_fix(bP.get(), ST, tP.get(), T, nc, 1, nc, N, W, cT, s);
+            if (comb) launch_wrap_fix(bP.get(), ST, tP.get(), T, np, 2, nc, N, W, cT, s);
+            else launch_wrap_fix(bP.get(), ST, tP.get(), T, nc, 1, nc, N, W, cT, s);
             launch_wrap_fix(bQ.get(), ST, tQ.get(), T, np, 2, nc, N, W, cT, s);
             if (needR)
                 launch_wrap_fix(bR.get(), ST, tR.get(), T, np, 2, nc, N, W, cT, s);
             PIC_CHECK_LAUNCH();
             count_launch(needR ? 3 : 2);
         }
-        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.Q.len.get(), p0, np, 0, 1, o.l1);
-        product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.R.len.get(), p0, np, 1, 0, o.l2);
+        if (comb) {
+            fill_u32_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.l1, np, (uint32_t)(2 * ncoef + 6));
+        } else {
+            product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.Q.len.get(), p0, np, 0, 1, o.l1);
+            product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.R.len.get(), p0, np, 1, 0, o.l2);
+        }
         product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.Q.len.get(), ch.Q.len.get(), p0, np, 0, 1, o.lQ);
         if (needR)
             product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.R.len.get(), ch.R.len.get(), p0, np, 0, 1, o.lR);
@@ -1333,12 +1380,18 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         count_launch(needR ? 4 : 3);
         // T1: residues at bP items 2i (stride 2 ST), T2 at items 2i+1
         const size_t pstride = nc * ST;  // [prime][child][ST]
-        ntt3_batch_to_words(bP.get(), 2 * ST, pstride, np, k, o.T1, o.c1, o.l1, s, ncoef);
-        ntt3_batch_to_words(bP.get() + ST, 2 * ST, pstride, np, k, o.T2, o.c2, o.l2, s, ncoef);
+        if (comb) {
+            ntt3_batch_to_words(bP.get(), 2 * ST, pstride, np, k, o.T1, o.c1, o.l1, s, ncoef, /*offset=*/true);
+        } else {
+            ntt3_batch_to_words(bP.get(), 2 * ST, pstride, np, k, o.T1, o.c1, o.l1, s, ncoef);
+            ntt3_batch_to_words(bP.get() + ST, 2 * ST, pstride, np, k, o.T2, o.c2, o.l2, s, ncoef);
+        }
         ntt3_batch_to_words(bQ.get(), 2 * ST, pstride, np, k, o.Q, o.cQ, o.lQ, s, ncoef);
         if (needR) ntt3_batch_to_words(bR.get(), 2 * ST, pstride, np, k, o.R, o.cR, o.lR, s, ncoef);
-        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.T1, o.c1, o.l1, np);
-        fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.T2, o.c2, o.l2, np);
+        if (!comb) {
+            fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.T1, o.c1, o.l1, np);
+            fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.T2, o.c2, o.l2, np);
+        }
         fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.Q, o.cQ, o.lQ, np);
         if (needR) fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.R, o.cR, o.lR, np);
         PIC_CHECK_LAUNCH();
@@ -1347,21 +1400,80 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
     (void)cmax;
 }
 
+// K = sum_(j < ncoef) 2^(159 + 64 j): bit 31 of words 4 + 2 j.
+__global__ void offset_words_kernel(uint32_t* K, size_t nwords)
+{
+    for (size_t w = blockIdx.x * (size_t)blockDim.x + threadIdx.x; w < nwords; w += (size_t)gridDim.x * blockDim.x)
+        K[w] = (w >= 4 && (w & 1) == 0) ? 0x80000000u : 0u;
+}
+
+// Addend signs of P = sL (V + K) + (not sL) K: parent i at out[2i], out[2i + 1].
+__global__ void sign_pair_kernel(const uint8_t* __restrict__ cs, size_t np, uint8_t* __restrict__ out)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
+        const uint8_t a = cs[2 * i] != 0 ? 1 : 0;
+        out[2 * i] = a;
+        out[2 * i + 1] = 1 - a;
+    }
+}
+
+// P = sa A + sb B for each parent of the chunk (signs at cS[2i], cS[2i + 1]),
+// into the parent slots; many CTAs per parent when parents are few and long.
+static void signed_sum(const uint32_t* A, const uint32_t* lA, uint32_t cA, const uint32_t* B, const uint32_t* lB,
+                       uint32_t cB, uint32_t nmax, const uint8_t* cS, size_t p0, size_t np, Level& par, cudaStream_t s)
+{
+    ProfScope ps(KC_LINEAR, 12.0 * (double)np * (double)nmax, s);
+    const uint32_t cpp = (uint32_t)((nmax + kWideWPC - 1) / kWideWPC);
+    if (g_wide_add && np < 2 * 148 && cpp > 1) {
+        DevBuf<uint32_t> hd(np, s), agg(np * cpp, s), aggc(np * cpp, s);
+        PIC_CUDA(cudaMemsetAsync(hd.get(), 0, 4 * np, s));
+        PIC_CUDA(cudaMemsetAsync(par.P.len.get() + p0, 0, 4 * np, s));
+        WideAdd w{A, lA, B, lB, cA, cB, cS, p0, par.P.w.get(), par.P.len.get(), par.P.cap, par.sign.get(), hd.get(),
+                  agg.get(), aggc.get(), cpp};
+        const unsigned grid = (unsigned)(np * cpp);
+        wide_cmp_kernel<<<grid, 256, 0, s>>>(w);
+        wide_k1_kernel<<<grid, 256, 0, s>>>(w);
+        PIC_CHECK_LAUNCH();
+        carry_scan_segments(agg.get(), np, cpp, s);
+        wide_ripple_kernel<<<grid, 256, 0, s>>>(w);
+        wide_final_kernel<<<grid, 256, 0, s>>>(w);
+        PIC_CHECK_LAUNCH();
+        count_launch(4);
+    } else {
+        signed_add_kernel<<<(unsigned)np, 256, 0, s>>>(A, lA, cA, B, lB, cB, cS, p0, par.P.w.get(), par.P.len.get(),
+                                                      par.sign.get(), par.P.cap);
+        PIC_CHECK_LAUNCH();
+        count_launch();
+    }
+}
+
+static bool g_combine = true;  // P formed in the transform domain (one inverse, one CRT)
+
 static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
 {
     const uint32_t ccP = ch.P.cap, ccQ = ch.Q.cap, ccR = ch.R.cap;
     const uint32_t cmax = std::max(ccP, std::max(ccQ, ccR));
     const MergeShape sh = merge_shape(cmax);
-    // bytes per parent: the transforms plus the two word buffers for P's
-    // partial products
-    const size_t per_parent = ntt_bytes_per_parent(sh) + 4 * (size_t)(2 * ccP + ccQ + ccR);
+    const size_t ncoef = products_ncoef(sh);
+    // combined form: P = sL (T1 +- T2) converted once as V + K (the CRT adds
+    // 2^159 to every coefficient so the signed ones stay exact), then
+    // P = sL (V + K) - sL K with the exact signed sum
+    const uint32_t cV = (uint32_t)(2 * ncoef + 8), cK = (uint32_t)(2 * ncoef + 3);
+    const uint32_t c1 = g_combine ? cV : ccP + ccQ, c2 = g_combine ? 0 : ccP + ccR;
+    // bytes per parent: the transforms plus the word buffers for P
+    const size_t per_parent = ntt_bytes_per_parent(sh) + 4 * (size_t)(c1 + c2 + ccQ + ccR);
     size_t chunk = mem_budget / per_parent;
     if (chunk < 1) chunk = 1;
     if (chunk > par.count) chunk = par.count;
-    const uint32_t c1 = ccP + ccQ, c2 = ccP + ccR;
+    DevBuf<uint32_t> K(g_combine ? cK : 0, s);
+    if (g_combine) {
+        offset_words_kernel<<<grid_for(cK, 256), 256, 0, s>>>(K.get(), cK);
+        PIC_CHECK_LAUNCH();
+        count_launch();
+    }
     for (size_t p0 = 0; p0 < par.count; p0 += chunk) {
         const size_t np = std::min(chunk, par.count - p0);
-        DevBuf<uint32_t> T1(np * c1, s), T2(np * c2, s), l1(np, s), l2(np, s);
+        DevBuf<uint32_t> T1(np * c1, s), T2(g_combine ? 0 : np * c2, s), l1(np, s), l2(np, s);
         ProductsOut o;
         o.T1 = T1.get();
         o.c1 = c1;
@@ -1375,31 +1487,18 @@ static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
         o.R = par.R.w.get() + p0 * par.R.cap;
         o.cR = par.R.cap;
         o.lR = par.R.len.get() + p0;
+        if (g_combine) o.csign = ch.sign.get() + 2 * p0;
         ntt_products(ch, p0, np, sh, o, s);
-        ProfScope ps(KC_LINEAR, 12.0 * (double)np * (double)c1, s);
-        const uint32_t cpp = (uint32_t)((std::max(c1, c2) + kWideWPC - 1) / kWideWPC);
-        if (g_wide_add && np < 2 * 148 && cpp > 1) {
-            // few long parents: spread each sum over many CTAs
-            DevBuf<uint32_t> hd(np, s), agg(np * cpp, s), aggc(np * cpp, s);
-            PIC_CUDA(cudaMemsetAsync(hd.get(), 0, 4 * np, s));
-            PIC_CUDA(cudaMemsetAsync(par.P.len.get() + p0, 0, 4 * np, s));
-            WideAdd w{T1.get(), l1.get(), T2.get(), l2.get(), c1, c2, ch.sign.get(), p0, par.P.w.get(),
-                      par.P.len.get(), par.P.cap, par.sign.get(), hd.get(), agg.get(), aggc.get(), cpp};
-            const unsigned grid = (unsigned)(np * cpp);
-            wide_cmp_kernel<<<grid, 256, 0, s>>>(w);
-            wide_k1_kernel<<<grid, 256, 0, s>>>(w);
+        if (g_combine) {
+            DevBuf<uint8_t> sg(2 * np, s);
+            sign_pair_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.sign.get() + 2 * p0, np, sg.get());
+            fill_u32_kernel<<<grid_for(np, 256), 256, 0, s>>>(l2.get(), np, cK);
             PIC_CHECK_LAUNCH();
-            carry_scan_segments(agg.get(), np, cpp, s);
-            wide_ripple_kernel<<<grid, 256, 0, s>>>(w);
-            wide_final_kernel<<<grid, 256, 0, s>>>(w);
-            PIC_CHECK_LAUNCH();
-            count_launch(4);
+            count_launch(2);
+            signed_sum(T1.get(), l1.get(), c1, K.get(), l2.get(), 0, cV, sg.get(), p0, np, par, s);
         } else {
-            signed_add_kernel<<<(unsigned)np, 256, 0, s>>>(T1.get(), l1.get(), c1, T2.get(), l2.get(), c2,
-                                                          ch.sign.get(), p0, par.P.w.get(), par.P.len.get(),
-                                                          par.sign.get(), par.P.cap);
-            PIC_CHECK_LAUNCH();
-            count_launch();
+            signed_sum(T1.get(), l1.get(), c1, T2.get(), l2.get(), c2, std::max(c1, c2), ch.sign.get() + 2 * p0, p0,
+                       np, par, s);
         }
     }
 }
@@ -1463,6 +1562,8 @@ static uint32_t g_school_max = 600;
 
 void bsr_set_school_threshold(uint32_t words) { g_school_max = words; }
 void bsr_set_wrap(bool on) { g_wrap = on; }
+void bsr_set_combine(bool on) { g_combine = on; }
+bool bsr_combine() { return g_combine; }
 void bsr_set_small_merge(int mode) { g_small_merge = mode; }
 int bsr_small_merge() { return g_small_merge; }
 bool bsr_wrap() { return g_wrap; }

@@ -21,6 +21,10 @@ bool bsr_wrap();
 // warp per parent (nodes <= 64 words), 2 also one thread per parent (nodes
 // <= 28 words, the default).
 void bsr_set_small_merge(int mode);
+// P of the batched NTT merges formed in the transform domain (one inverse
+// transform and one conversion instead of two; on by default).
+void bsr_set_combine(bool on);
+bool bsr_combine();
 int bsr_small_merge();
 
 }  // namespace pic

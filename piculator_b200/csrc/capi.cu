@@ -563,6 +563,7 @@ pic_status pic_set_tuning(int knob, int64_t value)
         case PIC_TUNE_BATCH_GRAPHS: mul_batch_set_graphs(value != 0); break;
         case PIC_TUNE_BSR_WRAP: bsr_set_wrap(value != 0); break;
         case PIC_TUNE_MUL_WRAP: mul_set_wrap(value != 0); break;
+        case PIC_TUNE_BSR_COMBINE: bsr_set_combine(value != 0); break;
         case PIC_TUNE_BSR_SMALL_MERGE:
             PIC_REQUIRE(value <= 2, PIC_ERR_INVALID, "small-merge mode is 0, 1 or 2");
             bsr_set_small_merge((int)value);
@@ -597,6 +598,7 @@ int64_t pic_get_tuning(int knob)
     case PIC_TUNE_BSR_WRAP: return bsr_wrap() ? 1 : 0;
     case PIC_TUNE_BSR_SMALL_MERGE: return bsr_small_merge();
     case PIC_TUNE_MUL_WRAP: return mul_wrap() ? 1 : 0;
+    case PIC_TUNE_BSR_COMBINE: return bsr_combine() ? 1 : 0;
     }
     return -1;
 }

@@ -87,6 +87,7 @@ struct Crt3Consts {
     ulonglong2 p0m2;      // p0 mod p2
     ulonglong2 inv012;    // (p0 p1)^-1 mod p2
     uint64_t p0p1_lo, p0p1_hi;
+    uint64_t off[3];      // 2^159 mod p_q when every coefficient gets the offset 2^159, else 0
 };
 
 // x * w mod p in [0, p) for a Shoup pair w (product primes c 2^32 + 1).
@@ -97,13 +98,18 @@ __device__ __forceinline__ uint64_t crt_mul(uint64_t x, const ulonglong2& w, uin
 }
 
 // Garner's CRT: x = r0 + p0 (v1 + p1 v2), 0 <= x < p0 p1 p2, as three limbs.
-// Inputs may be any 64-bit residue representatives (lazy transforms).
+// Inputs may be any 64-bit residue representatives (lazy transforms).  With
+// the offset set, x is the coefficient plus 2^159 (signed coefficients of
+// magnitude below 2^159 come out nonnegative and exact).
 __device__ __forceinline__ void crt3(const Crt3Consts& C, uint64_t y0, uint64_t y1, uint64_t y2, uint64_t& l0,
                                      uint64_t& l1, uint64_t& l2)
 {
-    const uint64_t r0 = crt_mul(y0, C.scale[0], C.p[0], C.c[0]);
-    const uint64_t r1 = crt_mul(y1, C.scale[1], C.p[1], C.c[1]);
-    const uint64_t r2 = crt_mul(y2, C.scale[2], C.p[2], C.c[2]);
+    const uint64_t r0s = crt_mul(y0, C.scale[0], C.p[0], C.c[0]);
+    const uint64_t r1s = crt_mul(y1, C.scale[1], C.p[1], C.c[1]);
+    const uint64_t r2o = crt_mul(y2, C.scale[2], C.p[2], C.c[2]);
+    const uint64_t r0 = add_mod(r0s, C.off[0], C.p[0]);
+    const uint64_t r1 = add_mod(r1s, C.off[1], C.p[1]);
+    const uint64_t r2 = add_mod(r2o, C.off[2], C.p[2]);
     const uint64_t r0m1 = r0 >= C.p[1] ? r0 - C.p[1] : r0;
     const uint64_t v1 = crt_mul(sub_mod(r1, r0m1, C.p[1]), C.inv01, C.p[1], C.c[1]);
     const uint64_t r0m2 = r0 >= C.p[2] ? r0 - C.p[2] : r0;
@@ -372,6 +378,7 @@ static Crt3Consts make_crt3(int k, int depth)
     const unsigned __int128 p01 = (unsigned __int128)p0 * p1;
     C.p0p1_lo = (uint64_t)p01;
     C.p0p1_hi = (uint64_t)(p01 >> 64);
+    for (int q = 0; q < 3; q++) C.off[q] = 0;
     return C;
 }
 
@@ -419,11 +426,13 @@ void ntt3_inverse_to_words(uint64_t* y, int k, size_t ncoef, int depth, uint32_t
 }
 
 void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
-                         uint32_t zcap, const uint32_t* zlen, cudaStream_t s, size_t ncoef)
+                         uint32_t zcap, const uint32_t* zlen, cudaStream_t s, size_t ncoef, bool offset)
 {
     if (count == 0) return;
     if (ncoef == 0) ncoef = (size_t)1 << k;
-    const Crt3Consts C = make_crt3(k, 1);
+    Crt3Consts C = make_crt3(k, 1);
+    if (offset)
+        for (int q = 0; q < 3; q++) C.off[q] = host_powmod(2, 159, C.p[q]);
     const size_t cpp = (((size_t)zcap + 1) / 2 + kCvtLPC - 1) / kCvtLPC;
     const size_t nctas = count * cpp;
     DevBuf<uint32_t> agg(nctas, s);

@@ -46,8 +46,11 @@ bool mul_wrap();
 void launch_wrap_fix(uint64_t* y, size_t ystride, const uint64_t* tail, size_t T, size_t nitems, size_t item_mul,
                      size_t nchild, size_t Nm, size_t W, const uint64_t cT[3], cudaStream_t s);
 
+// With `offset`, every coefficient j < ncoef is converted as c_j + 2^159 (for
+// signed coefficients |c_j| < 2^159): the words are the value plus the fixed
+// integer sum_j 2^(159 + 64 j).
 void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
-                         uint32_t zcap, const uint32_t* zlen, cudaStream_t s, size_t ncoef = 0);
+                         uint32_t zcap, const uint32_t* zlen, cudaStream_t s, size_t ncoef = 0, bool offset = false);
 
 // batch.cu: persistent schoolbook + binned three-prime NTT, replayed from a
 // CUDA graph when the sizes repeat.

@@ -22,9 +22,12 @@ def _same(dev, want) -> bool:
 @pytest.mark.parametrize("a,b,p", CASES)
 # Small-merge modes: 2 = thread, warp and CTA kernels (by node size), 0 = CTA
 # kernel for every schoolbook level.
-@pytest.mark.parametrize("school_max,wrap,small", [(192, 1, 2), (192, 1, 0), (8, 1, 2), (8, 0, 2)])
-def test_bsr_vs_oracle(pic, oracle, a, b, p, school_max, wrap, small):
-    knobs = {pic.TUNE_BSR_SCHOOL_MAX: school_max, pic.TUNE_BSR_WRAP: wrap, pic.TUNE_BSR_SMALL_MERGE: small}
+# Combine: P formed in the transform domain (1) or from two separate products (0).
+@pytest.mark.parametrize("school_max,wrap,small,combine", [(192, 1, 2, 1), (192, 1, 0, 1), (8, 1, 2, 1),
+                                                           (8, 0, 2, 1), (8, 1, 2, 0)])
+def test_bsr_vs_oracle(pic, oracle, a, b, p, school_max, wrap, small, combine):
+    knobs = {pic.TUNE_BSR_SCHOOL_MAX: school_max, pic.TUNE_BSR_WRAP: wrap, pic.TUNE_BSR_SMALL_MERGE: small,
+             pic.TUNE_BSR_COMBINE: combine}
     saved = {k: pic.get_tuning(k) for k in knobs}
     for k, v in knobs.items():
         pic.set_tuning(k, v)
