@@ -814,6 +814,7 @@ __global__ void __launch_bounds__(256) merge_pointwise_kernel(uint64_t* __restri
     const size_t j = ((size_t)jb * blockDim.x + threadIdx.x) * 2;
     if (j >= ((size_t)1 << k)) return;
     const Mod64& M = q == 0 ? m0 : (q == 1 ? m1 : m2);
+    const uint32_t c = (uint32_t)(M.p >> 32);  // product primes c 2^32 + 1
     const size_t base = (size_t)q * 2 * npar;
     const size_t L = (base + 2 * (size_t)i) * stride + j, Rr = L + stride;
     const ulonglong2 pl = *reinterpret_cast<const ulonglong2*>(P + L), pr = *reinterpret_cast<const ulonglong2*>(P + Rr);
@@ -822,17 +823,17 @@ __global__ void __launch_bounds__(256) merge_pointwise_kernel(uint64_t* __restri
     if (sgn != nullptr) {
         // P[2i] = T1 + T2 if the children's P have one sign, T1 - T2 otherwise
         const bool same = (sgn[2 * i] != 0) == (sgn[2 * i + 1] != 0);
-        const uint64_t ax = mont_mul(pl.x, qr.x, M), ay = mont_mul(pl.y, qr.y, M);
-        const uint64_t bx = mont_mul(pr.x, rl.x, M), by = mont_mul(pr.y, rl.y, M);
+        const uint64_t ax = mont_mul_c(pl.x, qr.x, M.p, c), ay = mont_mul_c(pl.y, qr.y, M.p, c);
+        const uint64_t bx = mont_mul_c(pr.x, rl.x, M.p, c), by = mont_mul_c(pr.y, rl.y, M.p, c);
         *reinterpret_cast<ulonglong2*>(P + L) =
             same ? make_ulonglong2(add_mod(ax, bx, M.p), add_mod(ay, by, M.p))
                  : make_ulonglong2(sub_mod(ax, bx, M.p), sub_mod(ay, by, M.p));
     } else {
-        *reinterpret_cast<ulonglong2*>(P + L) = make_ulonglong2(mont_mul(pl.x, qr.x, M), mont_mul(pl.y, qr.y, M));
-        *reinterpret_cast<ulonglong2*>(P + Rr) = make_ulonglong2(mont_mul(pr.x, rl.x, M), mont_mul(pr.y, rl.y, M));
+        *reinterpret_cast<ulonglong2*>(P + L) = make_ulonglong2(mont_mul_c(pl.x, qr.x, M.p, c), mont_mul_c(pl.y, qr.y, M.p, c));
+        *reinterpret_cast<ulonglong2*>(P + Rr) = make_ulonglong2(mont_mul_c(pr.x, rl.x, M.p, c), mont_mul_c(pr.y, rl.y, M.p, c));
     }
-    *reinterpret_cast<ulonglong2*>(Q + L) = make_ulonglong2(mont_mul(ql.x, qr.x, M), mont_mul(ql.y, qr.y, M));
-    *reinterpret_cast<ulonglong2*>(R + L) = make_ulonglong2(mont_mul(rl.x, rr.x, M), mont_mul(rl.y, rr.y, M));
+    *reinterpret_cast<ulonglong2*>(Q + L) = make_ulonglong2(mont_mul_c(ql.x, qr.x, M.p, c), mont_mul_c(ql.y, qr.y, M.p, c));
+    *reinterpret_cast<ulonglong2*>(R + L) = make_ulonglong2(mont_mul_c(rl.x, rr.x, M.p, c), mont_mul_c(rl.y, rr.y, M.p, c));
 }
 
 // Launch over 3 primes x npar parents x 2^k points (stride even, 2^k >= 2).

@@ -65,6 +65,22 @@ PIC_HD uint64_t mont_mul(uint64_t a, uint64_t b, const Mod64& m)
     return mont_mul(a, b, m.p, m.pinv_neg);
 }
 
+// mont_mul for p = c 2^32 + 1 (c < 2^30): -p^-1 mod 2^64 = c 2^32 - 1, so
+// m = lo (c 2^32 - 1) needs one 32-bit multiply, and m p = m + (m c) 2^32
+// gives hi(m p) from m c (64 x 32 bits) and one carry.
+PIC_HD uint64_t mont_mul_c(uint64_t a, uint64_t b, uint64_t p, uint32_t c)
+{
+    const uint64_t lo = a * b;
+    const uint64_t hi = mulhi64(a, b);
+    const uint64_t m = ((uint64_t)((uint32_t)lo * c) << 32) - lo;
+    const uint64_t x = (uint64_t)(uint32_t)m * c;               // m_lo c
+    const uint64_t y = (uint64_t)(uint32_t)(m >> 32) * c + (x >> 32);  // (m c) >> 32
+    const uint64_t s = (x << 32) + m;                            // low 64 bits of m c 2^32 + m
+    const uint64_t mp_hi = y + (s < m);                          // hi(m p)
+    const uint64_t r = hi + mp_hi + (lo != 0);
+    return r >= p ? r - p : r;
+}
+
 // x * w mod p with ws = floor(w * 2^64 / p); x < 2^64, w < p.
 PIC_HD uint64_t shoup_mul(uint64_t x, uint64_t w, uint64_t ws, uint64_t p)
 {

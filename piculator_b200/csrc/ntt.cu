@@ -1267,7 +1267,8 @@ __global__ void pointwise_mont_kernel(NttBatch B, const uint64_t* __restrict__ o
         const size_t tr = g >> k, i = g & (n - 1);
         const PrimeDev P = pick_prime(B, (int)tr);
         uint64_t* d = B.data + tr * B.stride + i;
-        *d = mont_mul(*d, other[tr * B.stride + i], P.p, P.pinv_neg);
+        *d = P.lazy ? mont_mul_c(*d, other[tr * B.stride + i], P.p, (uint32_t)(P.p >> 32))
+                    : mont_mul(*d, other[tr * B.stride + i], P.p, P.pinv_neg);
     }
 }
 
