@@ -127,13 +127,9 @@ __global__ void bin_split_kernel(uint64_t* __restrict__ out, const DevDesc* __re
             v = x[2 * j];
             if (2 * j + 1 < n) v |= (uint64_t)x[2 * j + 1] << 32;
         }
-        uint64_t r0 = v, r1 = v, r2 = v;
-        while (r0 >= p0) r0 -= p0;
-        while (r1 >= p1) r1 -= p1;
-        while (r2 >= p2) r2 -= p2;
-        out[(0 * m + i) * N + j] = r0;
-        out[(1 * m + i) * N + j] = r1;
-        out[(2 * m + i) * N + j] = r2;
+        out[(0 * m + i) * N + j] = piece_to_strict(v, p0);
+        out[(1 * m + i) * N + j] = piece_to_strict(v, p1);
+        out[(2 * m + i) * N + j] = piece_to_strict(v, p2);
     }
 }
 

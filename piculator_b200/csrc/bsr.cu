@@ -821,13 +821,15 @@ __global__ void __launch_bounds__(256) merge_pointwise_kernel(uint64_t* __restri
     const ulonglong2 ql = *reinterpret_cast<const ulonglong2*>(Q + L), qr = *reinterpret_cast<const ulonglong2*>(Q + Rr);
     const ulonglong2 rl = *reinterpret_cast<const ulonglong2*>(R + L), rr = *reinterpret_cast<const ulonglong2*>(R + Rr);
     if (sgn != nullptr) {
-        // P[2i] = T1 + T2 if the children's P have one sign, T1 - T2 otherwise
+        // P[2i] = T1 + T2 if the children's P have one sign, T1 - T2 otherwise;
+        // the products are in [0, 2p), so both forms stay in [0, 4p), inside
+        // the inverse transform's input range
         const bool same = (sgn[2 * i] != 0) == (sgn[2 * i + 1] != 0);
         const uint64_t ax = mont_mul_c(pl.x, qr.x, M.p, c), ay = mont_mul_c(pl.y, qr.y, M.p, c);
         const uint64_t bx = mont_mul_c(pr.x, rl.x, M.p, c), by = mont_mul_c(pr.y, rl.y, M.p, c);
+        const uint64_t p2 = 2 * M.p;
         *reinterpret_cast<ulonglong2*>(P + L) =
-            same ? make_ulonglong2(add_mod(ax, bx, M.p), add_mod(ay, by, M.p))
-                 : make_ulonglong2(sub_mod(ax, bx, M.p), sub_mod(ay, by, M.p));
+            same ? make_ulonglong2(ax + bx, ay + by) : make_ulonglong2(ax + p2 - bx, ay + p2 - by);
     } else {
         *reinterpret_cast<ulonglong2*>(P + L) = make_ulonglong2(mont_mul_c(pl.x, qr.x, M.p, c), mont_mul_c(pl.y, qr.y, M.p, c));
         *reinterpret_cast<ulonglong2*>(P + Rr) = make_ulonglong2(mont_mul_c(pr.x, rl.x, M.p, c), mont_mul_c(pr.y, rl.y, M.p, c));

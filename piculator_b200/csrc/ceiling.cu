@@ -1,7 +1,7 @@
 // The integer roofline of the NTT passes: the rate of lazy Shoup DIF
 // butterflies (the arithmetic of ntt_rows_fast_kernel / ntt_cols_fast_kernel,
-// mod the first product prime) with operands and twiddles in registers, no
-// memory traffic.  Radix-8 groups, 12 butterflies per group, 8 resident CTAs
+// mod the first product prime: operands in [0, 4p), three-partial-product
+// quotient) with operands and twiddles in registers, no memory traffic.  Radix-8 groups, 12 butterflies per group, 8 resident CTAs
 // of 256 threads per SM.
 #include "common.cuh"
 #include "modarith.cuh"
@@ -13,7 +13,7 @@ __global__ void __launch_bounds__(256) butterfly_ceiling_kernel(uint64_t* out, c
                                                                 int iters)
 {
     const uint32_t c = (uint32_t)(p >> 32);
-    const uint64_t p2 = 2 * p;
+    const uint64_t p4 = 4 * p;
     uint64_t x[8];
     for (int m = 0; m < 8; m++) x[m] = (threadIdx.x * 8 + m + blockIdx.x) % p;
     uint64_t w[7], ws[7];
@@ -30,8 +30,8 @@ __global__ void __launch_bounds__(256) butterfly_ceiling_kernel(uint64_t* out, c
                 if (m & hm) continue;
                 const int ti = (l == 0 ? 0 : (l == 1 ? 4 : 6)) + (m & (hm - 1));
                 uint64_t s = x[m] + x[m + hm];
-                s = s >= p2 ? s - p2 : s;
-                x[m + hm] = shoup_lazy32(x[m] + p2 - x[m + hm], w[ti], ws[ti], c);
+                s = s >= p4 ? s - p4 : s;
+                x[m + hm] = shoup_approx32(x[m] + p4 - x[m + hm], w[ti], ws[ti], c);
                 x[m] = s;
             }
         }

@@ -67,7 +67,9 @@ PIC_HD uint64_t mont_mul(uint64_t a, uint64_t b, const Mod64& m)
 
 // mont_mul for p = c 2^32 + 1 (c < 2^30): -p^-1 mod 2^64 = c 2^32 - 1, so
 // m = lo (c 2^32 - 1) needs one 32-bit multiply, and m p = m + (m c) 2^32
-// gives hi(m p) from m c (64 x 32 bits) and one carry.
+// gives hi(m p) from m c (64 x 32 bits) and one carry.  The result is below
+// a b / 2^64 + p before its one correction: in [0, p) for a b < p 2^64, in
+// [0, 2p) for operands below 4p of a prime below 2^61.
 PIC_HD uint64_t mont_mul_c(uint64_t a, uint64_t b, uint64_t p, uint32_t c)
 {
     const uint64_t lo = a * b;
@@ -89,12 +91,12 @@ PIC_HD uint64_t shoup_mul(uint64_t x, uint64_t w, uint64_t ws, uint64_t p)
     return r >= p ? r - p : r;
 }
 
-#if defined(__CUDACC__)
-// x * w mod p in [0, 2p) for any x < 2^64 (Shoup, ws = floor(w 2^64 / p)).
-// q = floor(x ws / 2^64) from four 32 x 32 partial products; q p mod 2^64 =
-// q + ((q mod 2^32) c) 2^32.
-__device__ __forceinline__ uint64_t shoup_lazy32(uint64_t x, uint64_t w, uint64_t ws, uint32_t c)
+// x * w mod p in [0, 2p) for any x < 2^64 (Shoup, ws = floor(w 2^64 / p)),
+// for the product primes p = c 2^32 + 1: q = floor(x ws / 2^64) from all four
+// 32 x 32 partial products, and q p mod 2^64 = q + ((q mod 2^32) c) 2^32.
+PIC_HD uint64_t shoup_lazy32(uint64_t x, uint64_t w, uint64_t ws, uint32_t c)
 {
+#if defined(__CUDA_ARCH__)
     const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32);
     const uint32_t s0 = (uint32_t)ws, s1 = (uint32_t)(ws >> 32);
     const uint32_t w0 = (uint32_t)w, w1 = (uint32_t)(w >> 32);
@@ -119,9 +121,63 @@ __device__ __forceinline__ uint64_t shoup_lazy32(uint64_t x, uint64_t w, uint64_
         : "=r"(r0), "=r"(r1)
         : "r"(x0), "r"(x1), "r"(s0), "r"(s1), "r"(w0), "r"(w1), "r"(c));
     return ((uint64_t)r1 << 32) | r0;
+#else
+    const uint64_t q = mulhi64(x, ws);
+    return x * w - (q + ((uint64_t)((uint32_t)q * c) << 32));
+#endif
 }
 
+// x * w mod p in [0, 4p) for any x < 2^64, p = c 2^32 + 1 below 2^61 (so
+// 4p < 2^63).  The quotient keeps three of the four partial products of
+// x ws: x1 s1 + hi(x1 s0) + hi(x0 s1) is floor(x ws / 2^64) minus at most 2
+// (the dropped terms sum to less than 3 2^64), and the Shoup quotient itself
+// is floor(x w / p) or one less, so x w - q p lies in [0, 4p).
+PIC_HD uint64_t shoup_approx32(uint64_t x, uint64_t w, uint64_t ws, uint32_t c)
+{
+#if defined(__CUDA_ARCH__)
+    const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32);
+    const uint32_t s0 = (uint32_t)ws, s1 = (uint32_t)(ws >> 32);
+    const uint32_t w0 = (uint32_t)w, w1 = (uint32_t)(w >> 32);
+    uint32_t r0, r1;
+    asm("{\n\t.reg .u32 t0, t1, q0, q1, u1;\n\t"
+        "mul.hi.u32 t0, %2, %5;\n\t"
+        "mad.hi.cc.u32 t0, %3, %4, t0;\n\t"
+        "addc.u32 t1, 0, 0;\n\t"
+        "mad.lo.cc.u32 q0, %3, %5, t0;\n\t"
+        "madc.hi.u32 q1, %3, %5, t1;\n\t"
+        "mul.lo.u32 %0, %2, %6;\n\t"
+        "mul.hi.u32 %1, %2, %6;\n\t"
+        "mad.lo.u32 %1, %2, %7, %1;\n\t"
+        "mad.lo.u32 %1, %3, %6, %1;\n\t"
+        "mad.lo.u32 u1, q0, %8, q1;\n\t"
+        "sub.cc.u32 %0, %0, q0;\n\t"
+        "subc.u32 %1, %1, u1;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"(x0), "r"(x1), "r"(s0), "r"(s1), "r"(w0), "r"(w1), "r"(c));
+    return ((uint64_t)r1 << 32) | r0;
+#else
+    const uint64_t x0 = (uint32_t)x, x1 = x >> 32, s0 = (uint32_t)ws, s1 = ws >> 32;
+    const uint64_t q = x1 * s1 + ((x1 * s0) >> 32) + ((x0 * s1) >> 32);
+    return x * w - (q + ((uint64_t)((uint32_t)q * c) << 32));
 #endif
+}
+
+// A 64-bit piece v < 2^64 < 9p (product primes above 2^64 / 9) brought into
+// [0, 4p) by two conditional subtractions of 4p.
+PIC_HD uint64_t piece_to_lazy(uint64_t v, uint64_t p4)
+{
+    v = v >= p4 ? v - p4 : v;
+    return v >= p4 ? v - p4 : v;
+}
+
+// The same piece reduced to [0, p): [0, 4p) -> [0, 2p) -> [0, p).
+PIC_HD uint64_t piece_to_strict(uint64_t v, uint64_t p)
+{
+    v = piece_to_lazy(v, 4 * p);
+    v = v >= 2 * p ? v - 2 * p : v;
+    return v >= p ? v - p : v;
+}
 
 // ---- host-only helpers (table construction) ------------------------------
 inline uint64_t host_mulmod(uint64_t a, uint64_t b, uint64_t p)

@@ -30,13 +30,9 @@ __global__ void split3_kernel(uint64_t* __restrict__ out, const uint32_t* __rest
             const uint64_t hi = (2 * j + 1 < na) ? a[2 * j + 1] : 0u;
             v = lo | (hi << 32);
         }
-        uint64_t r0 = v, r1 = v, r2 = v;  // v < 2^64 < 5 p
-        while (r0 >= p0) r0 -= p0;
-        while (r1 >= p1) r1 -= p1;
-        while (r2 >= p2) r2 -= p2;
-        out[j] = r0;
-        out[N + j] = r1;
-        out[2 * N + j] = r2;
+        out[j] = piece_to_strict(v, p0);
+        out[N + j] = piece_to_strict(v, p1);
+        out[2 * N + j] = piece_to_strict(v, p2);
     }
 }
 
@@ -52,13 +48,9 @@ __global__ void split3_off_kernel(uint64_t* __restrict__ out, size_t stride, con
             v = a[wi];
             if (wi + 1 < na) v |= (uint64_t)a[wi + 1] << 32;
         }
-        uint64_t r0 = v, r1 = v, r2 = v;
-        while (r0 >= p0) r0 -= p0;
-        while (r1 >= p1) r1 -= p1;
-        while (r2 >= p2) r2 -= p2;
-        out[j] = r0;
-        out[stride + j] = r1;
-        out[2 * stride + j] = r2;
+        out[j] = piece_to_strict(v, p0);
+        out[stride + j] = piece_to_strict(v, p1);
+        out[2 * stride + j] = piece_to_strict(v, p2);
     }
 }
 
@@ -479,8 +471,8 @@ void crt3_to_words_scratch(const uint64_t* y, int k, size_t ncoef, uint32_t* z, 
 // Nm - sa + 1): the product of those pieces, d, gives c_(Nm+j) = d_(W-1+j),
 // and its cyclic length T >= 2W - 1 keeps those indices free of wrap.  For
 // each of the W positions:
-//   y[j] <- y[j] - h (kept nonnegative by adding 2p), y[Nm + j] <- h
-// (inverse outputs arrive in [0, 4p) and are first brought below 2p),
+//   y[j] <- y[j] - h (kept nonnegative by adding p), y[Nm + j] <- h
+// (inverse outputs arrive in [0, 8p) and are first brought below 4p),
 // with h = d_(W-1+j) * Nm / T so that both halves carry the same scale Nm.
 // y items have stride ystride >= Nm + W; tail items have stride T.  `item`
 // selects which children hold products (all for P, the even ones for Q, R).
@@ -498,10 +490,10 @@ __global__ void wrap_fix_kernel(uint64_t* __restrict__ y, size_t ystride, const 
         const size_t child = q * nchild + it * item_mul;
         const uint64_t h = mont_mul(tail[child * T + W - 1 + j], cT, M);  // < p
         uint64_t* yi = y + child * ystride;
-        const uint64_t p2 = 2 * M.p;
-        uint64_t v = yi[j];  // lazy inverse output, < 4p
-        v = v >= p2 ? v - p2 : v;
-        yi[j] = v + p2 - h;  // < 4p < 2^64: the CRT reduces any 64-bit input
+        const uint64_t p4 = 4 * M.p;
+        uint64_t v = yi[j];  // lazy inverse output, < 8p
+        v = v >= p4 ? v - p4 : v;
+        yi[j] = v + M.p - h;  // < 5p < 2^64: the CRT reduces any 64-bit input
         yi[Nm + j] = h;
     }
 }

@@ -12,12 +12,15 @@
 
 namespace pic {
 
-// Three primes c * 2^32 + 1 below 2^62 (2-adicity 33, 34, 37); their product
-// is ~2^186, so a cyclic convolution of 64-bit pieces of length <= 2^30 (any
-// coefficient < 2^158, or a signed difference of two such) is recovered
-// exactly by CRT.
-const uint64_t kProductPrimes[3] = {4611685941117976577ull, 4611685692009873409ull,
-                                    4611685606110527489ull};
+// Three primes c * 2^32 + 1 between 2^64 / 9 and 2^61 (2-adicity 32, 33,
+// 33); their product is ~2^183, so a cyclic convolution of 64-bit pieces of
+// length <= 2^30 (any coefficient < 2^158, or a signed difference of two such)
+// is recovered exactly by CRT.  Below 2^61, 8p < 2^64 leaves room for lazy
+// residues in [0, 4p) (forward) and [0, 8p) (inverse) and for the
+// three-partial-product Shoup quotient; above 2^64 / 9 a 64-bit piece is below
+// 9p and reaches [0, 4p) with two conditional subtractions.
+const uint64_t kProductPrimes[3] = {2305842979148922881ull, 2305842949084151809ull,
+                                    2305842811645198337ull};
 
 // The reference's prime table, NTT.cpp:125-158.  The transform length picks
 // the prime, so natural-order outputs only match if the values match.
@@ -128,8 +131,8 @@ const PrimeTables& prime_tables(uint64_t p)
     d.K = K;
     d.S = S;
     d.IB = IB;
-    // lazy butterflies need 4p < 2^64 and the c * 2^32 + 1 form (mul_p_lo)
-    d.lazy = (p < (1ull << 62) && (p & 0xffffffffull) == 1) ? 1 : 0;
+    // lazy butterflies need 8p < 2^64 and the c * 2^32 + 1 form (mul_p_lo)
+    d.lazy = (p < (1ull << 61) && (p & 0xffffffffull) == 1) ? 1 : 0;
     {
         const unsigned __int128 mu = (~(unsigned __int128)0) / p;  // floor(2^128 / p): p does not divide 2^128
         d.mu_hi = (uint64_t)(mu >> 64);
@@ -257,10 +260,10 @@ static int col_width_log2(int lc)
 
 // ---------------------------------------------------------------------------
 // Butterflies.  Strict: operands and results in [0, p).  Lazy (Harvey 2014,
-// primes below 2^62 so 4p < 2^64): forward operands and results in [0, 2p);
-// inverse operands and results in [0, 4p) (PIC_NTT_DIT4: only the even input
-// is brought back below 2p, one correction per butterfly).  The Shoup product
-// is left in [0, 2p) without its final correction, for any 64-bit input.
+// primes below 2^61 so 8p < 2^64): forward operands and results in [0, 4p);
+// inverse operands and results in [0, 8p) (PIC_NTT_DIT4: only the even input
+// is brought back below 4p, one correction per butterfly).  The Shoup product
+// is left without its final correction, for any 64-bit input.
 
 // q * p mod 2^64.  Lazy primes have the form c * 2^32 + 1, so
 // q p = q + ((q mod 2^32) c) 2^32 (mod 2^64): one 32-bit multiply-add.
@@ -284,10 +287,10 @@ template <bool LAZY>
 __device__ __forceinline__ void bfly_dif(uint64_t& a, uint64_t& b, uint64_t w, uint64_t ws, uint64_t p)
 {
     if (LAZY) {
-        const uint64_t p2 = 2 * p;
+        const uint64_t p4 = 4 * p;
         uint64_t x = a + b;
-        x = x >= p2 ? x - p2 : x;
-        b = shoup_lazy(a + p2 - b, w, ws, p);
+        x = x >= p4 ? x - p4 : x;
+        b = shoup_lazy(a + p4 - b, w, ws, p);
         a = x;
     } else {
         const uint64_t x = a, y = b;
@@ -301,11 +304,11 @@ template <bool LAZY>
 __device__ __forceinline__ void bfly_unit(uint64_t& a, uint64_t& b, uint64_t p)
 {
     if (LAZY) {
-        const uint64_t p2 = 2 * p;
+        const uint64_t p4 = 4 * p;
         uint64_t x = a + b;
-        x = x >= p2 ? x - p2 : x;
-        uint64_t y = a + p2 - b;
-        y = y >= p2 ? y - p2 : y;
+        x = x >= p4 ? x - p4 : x;
+        uint64_t y = a + p4 - b;
+        y = y >= p4 ? y - p4 : y;
         a = x;
         b = y;
     } else {
@@ -315,20 +318,24 @@ __device__ __forceinline__ void bfly_unit(uint64_t& a, uint64_t& b, uint64_t p)
     }
 }
 
-// Inverse-direction unit butterfly: lazy operands in [0, 4p).
+// Inverse-direction unit butterfly: lazy operands in [0, 8p).
 template <bool LAZY>
 __device__ __forceinline__ void bfly_unit_dit(uint64_t& a, uint64_t& b, uint64_t p)
 {
-#if PIC_NTT_DIT4
     if (LAZY) {
-        const uint64_t p2 = 2 * p;
-        const uint64_t x = a >= p2 ? a - p2 : a;
-        const uint64_t y = b >= p2 ? b - p2 : b;
+        const uint64_t p4 = 4 * p;
+        const uint64_t x = a >= p4 ? a - p4 : a;
+        const uint64_t y = b >= p4 ? b - p4 : b;
+#if PIC_NTT_DIT4
         a = x + y;
-        b = x + p2 - y;
+        b = x + p4 - y;
+#else
+        a = x;
+        b = y;
+        bfly_unit<LAZY>(a, b, p);
+#endif
         return;
     }
-#endif
     bfly_unit<LAZY>(a, b, p);
 }
 
@@ -336,19 +343,19 @@ template <bool LAZY>
 __device__ __forceinline__ void bfly_dit(uint64_t& a, uint64_t& b, uint64_t w, uint64_t ws, uint64_t p)
 {
     if (LAZY) {
-        const uint64_t p2 = 2 * p;
+        const uint64_t p4 = 4 * p;
         const uint64_t u = shoup_lazy(b, w, ws, p);
+        const uint64_t x = a >= p4 ? a - p4 : a;
 #if PIC_NTT_DIT4
-        const uint64_t x = a >= p2 ? a - p2 : a;
         a = x + u;
-        b = x + p2 - u;
+        b = x + p4 - u;
 #else
-        uint64_t x = a + u;
-        x = x >= p2 ? x - p2 : x;
-        uint64_t y = a + p2 - u;
-        y = y >= p2 ? y - p2 : y;
-        a = x;
-        b = y;
+        uint64_t s = x + u;
+        s = s >= p4 ? s - p4 : s;
+        uint64_t d = x + p4 - u;
+        d = d >= p4 ? d - p4 : d;
+        a = s;
+        b = d;
 #endif
     } else {
         const uint64_t x = a, y = shoup_mul(b, w, ws, p);
@@ -585,7 +592,7 @@ __global__ void __launch_bounds__(256) ntt_cols_kernel(NttBatch B, int k, int lp
 #endif
 
 struct LazyPrime {
-    uint64_t p, p2;
+    uint64_t p, p4;
     uint32_t c;  // p = c * 2^32 + 1
 };
 
@@ -593,13 +600,13 @@ __device__ __forceinline__ LazyPrime lazy_prime(const PrimeDev& P)
 {
     LazyPrime L;
     L.p = P.p;
-    L.p2 = 2 * P.p;
+    L.p4 = 4 * P.p;
     L.c = (uint32_t)(P.p >> 32);
     return L;
 }
 
 // Piece j of batch item tr from the item's child slot (SplitSrc), reduced to
-// [0, 2p) (a 64-bit piece is below 6p for the lazy primes).
+// [0, 4p) (a 64-bit piece is below 9p for the lazy primes).
 struct SrcRow {
     const uint32_t* x;
     uint32_t n;
@@ -614,7 +621,7 @@ __device__ __forceinline__ SrcRow src_row(const NttBatch& B, int tr)
     return r;
 }
 
-__device__ __forceinline__ uint64_t src_piece(const NttBatch& B, const SrcRow& r, size_t j, uint64_t p2)
+__device__ __forceinline__ uint64_t src_piece_raw(const NttBatch& B, const SrcRow& r, size_t j)
 {
     const size_t wi = 2 * (B.src.first + j);
     uint64_t v = 0;
@@ -622,44 +629,48 @@ __device__ __forceinline__ uint64_t src_piece(const NttBatch& B, const SrcRow& r
         v = __ldg(r.x + wi);
         if (wi + 1 < r.n) v |= (uint64_t)__ldg(r.x + wi + 1) << 32;
     }
-    v = v >= p2 ? v - p2 : v;
-    return v >= p2 ? v - p2 : v;
+    return v;
 }
 
-// Forward (DIF): operands and results in [0, 2p).
+__device__ __forceinline__ uint64_t src_piece(const NttBatch& B, const SrcRow& r, size_t j, uint64_t p4)
+{
+    return piece_to_lazy(src_piece_raw(B, r, j), p4);
+}
+
+// Forward (DIF): operands and results in [0, 4p).
 __device__ __forceinline__ void fbfly_dif(uint64_t& a, uint64_t& b, const ulonglong2 t, const LazyPrime& L)
 {
     uint64_t x = a + b;
-    x = x >= L.p2 ? x - L.p2 : x;
-    b = shoup_lazy32(a + L.p2 - b, t.x, t.y, L.c);
+    x = x >= L.p4 ? x - L.p4 : x;
+    b = shoup_approx32(a + L.p4 - b, t.x, t.y, L.c);
     a = x;
 }
 
 __device__ __forceinline__ void fbfly_unit_dif(uint64_t& a, uint64_t& b, const LazyPrime& L)
 {
     uint64_t x = a + b;
-    x = x >= L.p2 ? x - L.p2 : x;
-    uint64_t y = a + L.p2 - b;
-    y = y >= L.p2 ? y - L.p2 : y;
+    x = x >= L.p4 ? x - L.p4 : x;
+    uint64_t y = a + L.p4 - b;
+    y = y >= L.p4 ? y - L.p4 : y;
     a = x;
     b = y;
 }
 
-// Inverse (DIT): operands and results in [0, 4p).
+// Inverse (DIT): operands and results in [0, 8p).
 __device__ __forceinline__ void fbfly_dit(uint64_t& a, uint64_t& b, const ulonglong2 t, const LazyPrime& L)
 {
-    const uint64_t u = shoup_lazy32(b, t.x, t.y, L.c);
-    const uint64_t x = a >= L.p2 ? a - L.p2 : a;
+    const uint64_t u = shoup_approx32(b, t.x, t.y, L.c);
+    const uint64_t x = a >= L.p4 ? a - L.p4 : a;
     a = x + u;
-    b = x + L.p2 - u;
+    b = x + L.p4 - u;
 }
 
 __device__ __forceinline__ void fbfly_unit_dit(uint64_t& a, uint64_t& b, const LazyPrime& L)
 {
-    const uint64_t x = a >= L.p2 ? a - L.p2 : a;
-    const uint64_t y = b >= L.p2 ? b - L.p2 : b;
+    const uint64_t x = a >= L.p4 ? a - L.p4 : a;
+    const uint64_t y = b >= L.p4 ? b - L.p4 : b;
     a = x + y;
-    b = x + L.p2 - y;
+    b = x + L.p4 - y;
 }
 
 // The B levels of one group (elements base + j + m 2^LST, m < 2^B) with the
@@ -791,8 +802,8 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC>::NT, 1024 / RowsFastSh
             uint64_t v = 0;
             if (LRPC == 0 || row < nrows) {
                 const int tr = (int)row;
-                const uint64_t p2 = 2 * pick_prime(B, tr).p;
-                v = src_piece(B, src_row(B, tr), idx & EMASK, p2);
+                const uint64_t p4 = 4 * pick_prime(B, tr).p;
+                v = src_piece(B, src_row(B, tr), idx & EMASK, p4);
             }
             smem[(idx & ~EMASK) + swz(idx & EMASK)] = v;
         }
@@ -912,12 +923,12 @@ __global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatc
     auto twiddle = [&](uint64_t v, int m, int w) {
         if (T != nullptr) {  // the pass table: one Shoup product, streamed like the data
             const ulonglong2 t = __ldg(T + ((size_t)m << lM) + c0 + w);
-            return shoup_lazy32(v, t.x, t.y, L.c);
+            return shoup_approx32(v, t.x, t.y, L.c);
         }
         const uint64_t k1 = __brev((unsigned)m) >> (32 - LC);
         const uint64_t E = ((uint64_t)(c0 + w) * k1) << esh;
         const ulonglong2 h = __ldg(shi + (E >> S)), l = __ldg(slo + (E & smask));
-        return shoup_lazy32(shoup_lazy32(v, h.x, h.y, L.c), l.x, l.y, L.c);
+        return shoup_approx32(shoup_approx32(v, h.x, h.y, L.c), l.x, l.y, L.c);
     };
     if (!INV && B.src.words != nullptr) {
         // first forward column pass (lpre == 0): the input comes from the
@@ -926,7 +937,7 @@ __global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatc
 #pragma unroll 8
         for (int idx = threadIdx.x; idx < TOT; idx += 256) {
             const int m = idx >> LW, w = idx & WMASK;
-            smem[idx] = src_piece(B, sr, ((size_t)m << lM) + c0 + w, L.p2);
+            smem[idx] = src_piece(B, sr, ((size_t)m << lM) + c0 + w, L.p4);
         }
     } else {
 #pragma unroll 8
@@ -957,9 +968,8 @@ __global__ void src_split_kernel(NttBatch B, int k)
         const int tr = (int)(g >> k);
         const size_t j = g & (N - 1);
         const PrimeDev P = pick_prime(B, tr);
-        uint64_t v = src_piece(B, src_row(B, tr), j, 2 * P.p);
-        while (v >= P.p) v -= P.p;  // strict primes take [0, p)
-        B.data[(size_t)tr * B.stride + j] = v;
+        const uint64_t v = src_piece_raw(B, src_row(B, tr), j);
+        B.data[(size_t)tr * B.stride + j] = P.lazy ? piece_to_strict(v, P.p) : v % P.p;
     }
 }
 

@@ -2,9 +2,10 @@
 // 64-bit primes (< 2^63) on sm_100a.
 //
 // Forward = decimation in frequency, natural order in, bit-reversed order out.
-// For primes c * 2^32 + 1 below 2^62 (lazy butterflies) forward outputs are
-// only reduced to [0, 2p) and inverse outputs to [0, 4p); the Montgomery
-// consumers (pointwise products, CRT) accept any 64-bit operand.
+// For primes c * 2^32 + 1 below 2^61 (lazy butterflies) forward outputs are
+// only reduced to [0, 4p) and inverse outputs to [0, 8p); the consumers
+// (Montgomery pointwise products of operands below 4p, the CRT's Shoup
+// scaling of any 64-bit operand) accept them as they are.
 // Inverse = decimation in time, bit-reversed in, natural out, unscaled.
 // A convolution therefore never permutes: forward, pointwise, inverse.  The
 // natural-order NTT of the reference (NNT::NTT, NTT.cpp:191-223) is forward +
@@ -37,7 +38,7 @@ struct PrimeDev {
     int K;        // outer tables cover roots of order 2^K
     int S;        // outer split: e = hi * 2^S + lo
     int IB;       // inner table order bits (min(K, kInnerBits))
-    int lazy;     // 1 when 4p < 2^64: transforms keep values in [0, 2p)
+    int lazy;     // 1 when 8p < 2^64 and p = c 2^32 + 1: transforms keep values in [0, 4p) / [0, 8p)
     const uint64_t* inner_fwd;  // (w, w') Shoup pairs, w = root_(2^IB)^i, i < 2^(IB-1)
     const uint64_t* inner_inv;  // same for root^-1
     const uint64_t* olo_fwd;    // Montgomery form root_(2^K)^i, i < 2^S
