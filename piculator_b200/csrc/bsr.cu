@@ -1262,7 +1262,7 @@ static size_t ntt_bytes_per_parent(const MergeShape& sh) { return 3 * 2 * 3 * (s
 // operand is transformed once (six forward transforms per parent, four
 // inverse), every product exact.
 static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape& sh, const ProductsOut& o,
-                         cudaStream_t s)
+                         cudaStream_t s, bool use_workspace = false)
 {
     const uint32_t ccP = ch.P.cap, ccQ = ch.Q.cap, ccR = ch.R.cap;
     const uint32_t cmax = std::max(ccP, std::max(ccQ, ccR));
@@ -1277,9 +1277,27 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
     const size_t ncoef = products_ncoef(sh);
     {
         const size_t nc = 2 * np, c0 = 2 * p0;
-        DevBuf<uint64_t> bP(3 * nc * ST, s), bQ(3 * nc * ST, s), bR(3 * nc * ST, s);
-        DevBuf<uint64_t> tP(sh.wrap ? 3 * nc * T : 0, s), tQ(sh.wrap ? 3 * nc * T : 0, s),
-            tR(sh.wrap ? 3 * nc * T : 0, s);
+        // six work arrays: from the persistent workspace when asked (the
+        // top levels), else from the pool
+        const size_t nmain = 3 * nc * ST, ntail = sh.wrap ? 3 * nc * T : 0;
+        const size_t smain = (nmain + 31) & ~(size_t)31, stail = (ntail + 31) & ~(size_t)31;  // 256-byte steps
+        WorkspaceLease ws(use_workspace ? 8 * (3 * smain + 3 * stail) : 0, s);
+        DevBuf<uint64_t> owned[6];
+        uint64_t* arr[6];
+        for (int q = 0; q < 6; q++) {
+            const size_t n = q < 3 ? nmain : ntail;
+            if (ws.ptr) arr[q] = static_cast<uint64_t*>(ws.ptr) + (q < 3 ? q * smain : 3 * smain + (q - 3) * stail);
+            else {
+                owned[q] = DevBuf<uint64_t>(n, s);
+                arr[q] = owned[q].get();
+            }
+        }
+        uint64_t* const PB = arr[0];
+        uint64_t* const QB = arr[1];
+        uint64_t* const RB = arr[2];
+        uint64_t* const PT = arr[3];
+        uint64_t* const QT = arr[4];
+        uint64_t* const RT = arr[5];
         NttBatch fb;
         fb.stride = ST;
         fb.count = (int)(3 * nc);
@@ -1290,8 +1308,8 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         // the children's words are split into residues by each transform's
         // first pass (SplitSrc): main transforms from piece 0, tails from t0
         const Slots* arrays[3] = {&ch.P, &ch.Q, &ch.R};
-        uint64_t* mains[3] = {bP.get(), bQ.get(), bR.get()};
-        uint64_t* tails[3] = {tP.get(), tQ.get(), tR.get()};
+        uint64_t* mains[3] = {PB, QB, RB};
+        uint64_t* tails[3] = {PT, QT, RT};
         for (int a = 0; a < 3; a++) {
             SplitSrc src;
             src.words = arrays[a]->w.get();
@@ -1313,8 +1331,8 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         tb.src = SplitSrc{};
         {
             ProfScope ps(KC_NTT_POINTWISE, 3.0 * 3 * np * (double)(N + T) * 80.0 / 8.0, s);
-            launch_merge_pointwise(bP.get(), bQ.get(), bR.get(), np, k, ST, m0, m1, m2, o.csign, s);
-            if (sh.wrap) launch_merge_pointwise(tP.get(), tQ.get(), tR.get(), np, sh.kt, T, m0, m1, m2, o.csign, s);
+            launch_merge_pointwise(PB, QB, RB, np, k, ST, m0, m1, m2, o.csign, s);
+            if (sh.wrap) launch_merge_pointwise(PT, QT, RT, np, sh.kt, T, m0, m1, m2, o.csign, s);
             PIC_CHECK_LAUNCH();
             count_launch(sh.wrap ? 2 : 1);
         }
@@ -1327,17 +1345,17 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
             eb.count = (int)(3 * np);
             eb.per_prime = (int)np;
             if (comb) {
-                eb.data = bP.get();
+                eb.data = PB;
                 ntt_inverse_dit(eb, k, s);
             } else {
                 NttBatch ib = fb;
-                ib.data = bP.get();
+                ib.data = PB;
                 ntt_inverse_dit(ib, k, s);
             }
-            eb.data = bQ.get();
+            eb.data = QB;
             ntt_inverse_dit(eb, k, s);
             if (needR) {
-                eb.data = bR.get();
+                eb.data = RB;
                 ntt_inverse_dit(eb, k, s);
             }
         }
@@ -1347,26 +1365,26 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
             eb.count = (int)(3 * np);
             eb.per_prime = (int)np;
             if (comb) {
-                eb.data = tP.get();
+                eb.data = PT;
                 ntt_inverse_dit(eb, sh.kt, s);
             } else {
                 NttBatch ib = tb;
-                ib.data = tP.get();
+                ib.data = PT;
                 ntt_inverse_dit(ib, sh.kt, s);
             }
-            eb.data = tQ.get();
+            eb.data = QT;
             ntt_inverse_dit(eb, sh.kt, s);
             if (needR) {
-                eb.data = tR.get();
+                eb.data = RT;
                 ntt_inverse_dit(eb, sh.kt, s);
             }
             ProfScope ps(KC_NTT_POINTWISE, 3.0 * 4 * np * (double)sh.W * 24.0, s);
             const size_t W = sh.W;
-            if (comb) launch_wrap_fix(bP.get(), ST, tP.get(), T, np, 2, nc, N, W, cT, s);
-            else launch_wrap_fix(bP.get(), ST, tP.get(), T, nc, 1, nc, N, W, cT, s);
-            launch_wrap_fix(bQ.get(), ST, tQ.get(), T, np, 2, nc, N, W, cT, s);
+            if (comb) launch_wrap_fix(PB, ST, PT, T, np, 2, nc, N, W, cT, s);
+            else launch_wrap_fix(PB, ST, PT, T, nc, 1, nc, N, W, cT, s);
+            launch_wrap_fix(QB, ST, QT, T, np, 2, nc, N, W, cT, s);
             if (needR)
-                launch_wrap_fix(bR.get(), ST, tR.get(), T, np, 2, nc, N, W, cT, s);
+                launch_wrap_fix(RB, ST, RT, T, np, 2, nc, N, W, cT, s);
             PIC_CHECK_LAUNCH();
             count_launch(needR ? 3 : 2);
         }
@@ -1384,13 +1402,13 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         // T1: residues at bP items 2i (stride 2 ST), T2 at items 2i+1
         const size_t pstride = nc * ST;  // [prime][child][ST]
         if (comb) {
-            ntt3_batch_to_words(bP.get(), 2 * ST, pstride, np, k, o.T1, o.c1, o.l1, s, ncoef, /*offset=*/true);
+            ntt3_batch_to_words(PB, 2 * ST, pstride, np, k, o.T1, o.c1, o.l1, s, ncoef, /*offset=*/true);
         } else {
-            ntt3_batch_to_words(bP.get(), 2 * ST, pstride, np, k, o.T1, o.c1, o.l1, s, ncoef);
-            ntt3_batch_to_words(bP.get() + ST, 2 * ST, pstride, np, k, o.T2, o.c2, o.l2, s, ncoef);
+            ntt3_batch_to_words(PB, 2 * ST, pstride, np, k, o.T1, o.c1, o.l1, s, ncoef);
+            ntt3_batch_to_words(PB + ST, 2 * ST, pstride, np, k, o.T2, o.c2, o.l2, s, ncoef);
         }
-        ntt3_batch_to_words(bQ.get(), 2 * ST, pstride, np, k, o.Q, o.cQ, o.lQ, s, ncoef);
-        if (needR) ntt3_batch_to_words(bR.get(), 2 * ST, pstride, np, k, o.R, o.cR, o.lR, s, ncoef);
+        ntt3_batch_to_words(QB, 2 * ST, pstride, np, k, o.Q, o.cQ, o.lQ, s, ncoef);
+        if (needR) ntt3_batch_to_words(RB, 2 * ST, pstride, np, k, o.R, o.cR, o.lR, s, ncoef);
         if (!comb) {
             fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.T1, o.c1, o.l1, np);
             fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.T2, o.c2, o.l2, np);
@@ -1451,6 +1469,20 @@ static void signed_sum(const uint32_t* A, const uint32_t* lA, uint32_t cA, const
 }
 
 static bool g_combine = true;  // P formed in the transform domain (one inverse, one CRT)
+
+// Device bytes the transforms of one batch of merges may take: a quarter of
+// what the device has left, at most 128 bytes per word of the precision p
+// (12 GB at 1e9 digits; larger batches save little: 0.5 % of the run at
+// twice the size), at least 1 GiB.  Keeping the peak proportional to p lets
+// the pool reserved up front (reserve_pool, 512 bytes per word) hold every
+// call without growing, the top levels' workspace included; at 256 bytes
+// per word the peak outgrew it and runs stalled on pool growth.
+static size_t merge_budget(size_t p)
+{
+    size_t b = device_available_bytes() / 4;
+    b = std::min(b, p * 128);
+    return std::max(b, (size_t)1 << 30);
+}
 
 static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
 {
@@ -1624,6 +1656,8 @@ static bool top_level_merge(const std::vector<BigFloat>& cP, const std::vector<B
                             std::vector<BigFloat>& oQ, std::vector<BigFloat>& oR, cudaStream_t s)
 {
     const size_t nc = cP.size(), np = nc / 2;
+    trace_point("top_merge_begin", s);
+    timeline_mark("top_merge_begin", s);
     struct View {
         const uint32_t* T;
         size_t L;
@@ -1673,13 +1707,15 @@ static bool top_level_merge(const std::vector<BigFloat>& cP, const std::vector<B
     PIC_CUDA(cudaMemcpyAsync(ch.Q.len.get(), lQ.data(), 4 * nc, cudaMemcpyHostToDevice, s));
     PIC_CUDA(cudaMemcpyAsync(ch.R.len.get(), lR.data(), 4 * nc, cudaMemcpyHostToDevice, s));
     PIC_CUDA(cudaMemcpyAsync(ch.sign.get(), sg.data(), nc, cudaMemcpyHostToDevice, s));
+    trace_point("top_merge_children", s);
+    timeline_mark("top_merge_children", s);
     // the products, in parent chunks that fit a quarter of the free memory
     const MergeShape sh = merge_shape(std::max(capP, std::max(capQ, capR)));
     const uint32_t c1 = capP + capQ, c2 = capP + capR, cq = 2 * capQ, cr = 2 * capR;
     auto sT1 = alloc_words(np * c1), sT2 = alloc_words(np * c2), sQ = alloc_words(np * cq);
     std::shared_ptr<WordStore> sR = need_R ? alloc_words(np * cr) : nullptr;
     DevBuf<uint32_t> lens(4 * np, s);
-    size_t chunk = std::max<size_t>(device_available_bytes() / 4, (size_t)1 << 30) / ntt_bytes_per_parent(sh);
+    size_t chunk = merge_budget(p) / ntt_bytes_per_parent(sh);
     if (chunk < 1) chunk = 1;
     for (size_t p0 = 0; p0 < np; p0 += chunk) {
         const size_t n = std::min(chunk, np - p0);
@@ -1698,7 +1734,9 @@ static bool top_level_merge(const std::vector<BigFloat>& cP, const std::vector<B
             o.cR = cr;
             o.lR = lens.get() + 3 * np + p0;
         }
-        ntt_products(ch, p0, n, sh, o, s);
+        ntt_products(ch, p0, n, sh, o, s, /*use_workspace=*/true);
+        trace_point("top_merge_chunk", s);
+        timeline_mark("top_merge_chunk", s);
     }
     std::vector<uint32_t> hl(4 * np, 0);
     PIC_CUDA(cudaMemcpyAsync(hl.data(), lens.get(), 4 * (need_R ? 4 : 3) * np, cudaMemcpyDeviceToHost, s));
@@ -1720,6 +1758,8 @@ static bool top_level_merge(const std::vector<BigFloat>& cP, const std::vector<B
         oQ[i] = product(vQ[L], vQ[R], sQ, sQ->base + i * cq, hl[2 * np + i]);
         oR[i] = need_R ? product(vR[L], vR[R], sR, sR->base + i * cr, hl[3 * np + i]) : BigFloat();
     }
+    trace_point("top_merge_adds", s);
+    timeline_mark("top_merge_adds", s);
     return true;
 }
 
@@ -1779,7 +1819,7 @@ void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, s
         count_launch();
     }
     // merge up to Dtop
-    const size_t free_b = device_available_bytes();
+    const size_t budget = merge_budget(p);
     for (int d = Db - 1; d >= Dtop; d--) {
         const size_t cnt = (size_t)1 << d;
         const double n = ceil((double)T / (double)cnt);
@@ -1791,7 +1831,7 @@ void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, s
         TraceSpan span(s);
         const bool school = cmax <= g_school_max;
         if (school) merge_school(cur, par, s);
-        else merge_ntt(cur, par, s, std::max<size_t>(free_b / 4, (size_t)1 << 30));
+        else merge_ntt(cur, par, s, budget);
         if (tracing())
             fprintf(stderr,
                     "{\"trace\": \"bsr_level\", \"depth\": %d, \"parents\": %zu, \"child_caps\": [%u, %u, %u], "
@@ -1799,6 +1839,7 @@ void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, s
                     d, cnt, cur.P.cap, cur.Q.cap, cur.R.cap, school ? "school" : "ntt3", span.end_ms());
         cur = std::move(par);
         bnd[d + 1].reset();
+        timeline_mark(school ? "bsr_level_school" : "bsr_level_ntt", s);
     }
     // hand the nodes at Dtop to the exact BigFloat recursion
     const size_t cnt = cur.count;

@@ -62,6 +62,27 @@ void* dev_alloc(size_t bytes, cudaStream_t s);
 void dev_free(void* p, size_t bytes, cudaStream_t s);
 // Free device memory plus what the allocation pool holds unused.
 size_t device_available_bytes();
+// Grows the stream-ordered pool (which never releases memory) to hold at
+// least `bytes` as one free block, so that a computation whose peak fits in
+// it never grows the pool in the middle: growth maps and clears new physical
+// memory while the GPU may be idle, a pause of up to some hundred ms.
+// Capped at 90 % of what the device has left.
+void reserve_pool(size_t bytes, cudaStream_t s);
+
+// A grow-only device workspace on the context's stream, kept between calls:
+// the work arrays of the largest transforms always land at the same
+// addresses.  (Blocks of several GB placed afresh by the pool on every call
+// made the same kernels run up to 40 % slower on some calls.)  lease() returns
+// nullptr when `s` is not the context's stream or the workspace is already
+// leased; the caller then allocates as usual.  The lease ends with the object.
+struct WorkspaceLease {
+    void* ptr = nullptr;
+    WorkspaceLease(size_t bytes, cudaStream_t s);
+    ~WorkspaceLease();
+    WorkspaceLease(const WorkspaceLease&) = delete;
+    WorkspaceLease& operator=(const WorkspaceLease&) = delete;
+};
+void workspace_release_all();  // frees the workspace (pic_shutdown)
 
 template <typename T>
 struct DevBuf {
@@ -118,6 +139,13 @@ struct ProfScope {
 // Tracing: when the environment variable PIC_TRACE is set, phases print one
 // JSON line each to stderr with their device time.
 bool tracing();
+// With tracing on: synchronise `s` and print host time and pool occupancy.
+void trace_point(const char* tag, cudaStream_t s);
+// With PIC_TIMELINE set: record a stream-ordered event (no synchronisation);
+// timeline_dump prints the device time between consecutive marks, idle gaps
+// included.
+void timeline_mark(const char* tag, cudaStream_t s);
+void timeline_dump();
 struct TraceSpan {
     cudaEvent_t a = nullptr, b = nullptr;
     cudaStream_t s = nullptr;

@@ -75,7 +75,11 @@ struct PhaseTimer {
     {
         for (auto& x : e) cudaEventDestroy(x);
     }
-    void mark() { PIC_CUDA(cudaEventRecord(e[n++], ctx().stream)); }
+    void mark()
+    {
+        PIC_CUDA(cudaEventRecord(e[n++], ctx().stream));
+        timeline_mark("pi_phase", ctx().stream);
+    }
     double secs(int i, int j)
     {
         float ms = 0;
@@ -95,6 +99,10 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
     const uint64_t launches0 = ctx().launches.load();
     const int saved_mode = get_mul_mode();
     set_mul_mode(mode == PIC_PI_PLAIN ? PIC_MUL_NTT_REF : PIC_MUL_AUTO);
+    // the chosen form peaks below 512 bytes per word of precision (merge
+    // batches of at most 256, live nodes and the top levels' workspace);
+    // hold that much in the pool before the first merge
+    if (mode != PIC_PI_PLAIN) reserve_pool((size_t)p * 512, ctx().stream);
     PhaseTimer tm;
     BigFloat P, Q, R;
     try {
@@ -119,6 +127,7 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
         throw;
     }
     set_mul_mode(saved_mode);
+    timeline_dump();
     if (st) {
         memset(st, 0, sizeof *st);
         st->hex_digits = hex;

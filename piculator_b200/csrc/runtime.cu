@@ -4,6 +4,8 @@
 
 #include <stdlib.h>
 
+#include <chrono>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -58,6 +60,12 @@ void init_context(int device)
     PIC_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t thr = UINT64_MAX;
     PIC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    // every buffer lives on one stream, where reuse in stream order needs no
+    // opportunistic reuse; without it the pool's choice of block does not
+    // depend on how far the GPU has got, so repeated calls get the same
+    // placement
+    int no = 0;
+    PIC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowOpportunistic, &no));
     g_ctx.pinned_words_cap = 1 << 16;
     PIC_CUDA(cudaMallocHost((void**)&g_ctx.pinned_words, g_ctx.pinned_words_cap * sizeof(uint32_t)));
     g_init.store(true);
@@ -67,12 +75,34 @@ void shutdown_context()
 {
     std::lock_guard<std::recursive_mutex> g(g_ctx.lock);
     if (!g_init.load()) return;
+    workspace_release_all();
     cudaStreamSynchronize(g_ctx.stream);
     if (g_ctx.pinned_words) cudaFreeHost(g_ctx.pinned_words);
     g_ctx.pinned_words = nullptr;
     cudaStreamDestroy(g_ctx.stream);
     g_ctx.stream = nullptr;
     g_init.store(false);
+}
+
+bool timeline_on();
+
+// host time spent in the allocator (timeline diagnostics)
+namespace {
+struct AllocStat {
+    double total_ms = 0, max_ms = 0;
+    size_t calls = 0, max_bytes = 0;
+};
+AllocStat g_alloc_stat;
+}  // namespace
+
+static void alloc_stat(double ms, size_t bytes)
+{
+    g_alloc_stat.total_ms += ms;
+    g_alloc_stat.calls++;
+    if (ms > g_alloc_stat.max_ms) {
+        g_alloc_stat.max_ms = ms;
+        g_alloc_stat.max_bytes = bytes;
+    }
 }
 
 void* dev_alloc(size_t bytes, cudaStream_t s)
@@ -83,7 +113,10 @@ void* dev_alloc(size_t bytes, cudaStream_t s)
             throw Error(PIC_ERR_NO_MEMORY, "device allocation failed (injected)");
     }
     void* p = nullptr;
+    const bool tl = timeline_on();
+    const auto t0 = tl ? std::chrono::steady_clock::now() : std::chrono::steady_clock::time_point();
     cudaError_t e = cudaMallocAsync(&p, bytes, s);
+    if (tl) alloc_stat(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(), bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
         char buf[256];
@@ -107,10 +140,79 @@ size_t device_available_bytes()
     return free_b + (reserved > used ? (size_t)(reserved - used) : 0);
 }
 
+void reserve_pool(size_t bytes, cudaStream_t s)
+{
+    cudaMemPool_t pool;
+    PIC_CUDA(cudaDeviceGetDefaultMemPool(&pool, g_ctx.device));
+    uint64_t reserved = 0;
+    PIC_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    if (reserved >= bytes) return;
+    const uint64_t used = g_ctx.bytes_in_use.load();
+    size_t free_b = 0, total_b = 0;
+    PIC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    size_t want = bytes - (size_t)(used < reserved ? used : reserved);
+    const size_t cap = free_b / 10 * 9 + (size_t)(reserved > used ? reserved - used : 0);
+    if (want > cap) want = cap;
+    if (want == 0) return;
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, want, s) != cudaSuccess) {
+        cudaGetLastError();  // no room for one block that size: allocate as needed instead
+        return;
+    }
+    PIC_CUDA(cudaFreeAsync(p, s));
+    PIC_CUDA(cudaStreamSynchronize(s));
+}
+
+namespace {
+struct Workspace {
+    std::mutex lock;
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    bool leased = false;
+};
+Workspace g_ws;
+}  // namespace
+
+WorkspaceLease::WorkspaceLease(size_t bytes, cudaStream_t s)
+{
+    if (s != g_ctx.stream || bytes == 0) return;
+    std::lock_guard<std::mutex> g(g_ws.lock);
+    if (g_ws.leased) return;
+    if (g_ws.bytes < bytes) {
+        if (g_ws.ptr) dev_free(g_ws.ptr, g_ws.bytes, s);  // stream-ordered: earlier users finish first
+        g_ws.ptr = nullptr;
+        g_ws.bytes = 0;
+        g_ws.ptr = dev_alloc(bytes, s);  // throws on no memory, with nothing leased
+        g_ws.bytes = bytes;
+    }
+    g_ws.leased = true;
+    ptr = g_ws.ptr;
+}
+
+WorkspaceLease::~WorkspaceLease()
+{
+    if (!ptr) return;
+    std::lock_guard<std::mutex> g(g_ws.lock);
+    g_ws.leased = false;
+}
+
+void workspace_release_all()
+{
+    std::lock_guard<std::mutex> g(g_ws.lock);
+    if (g_ws.ptr && !g_ws.leased) {
+        dev_free(g_ws.ptr, g_ws.bytes, g_ctx.stream);
+        g_ws.ptr = nullptr;
+        g_ws.bytes = 0;
+    }
+}
+
 void dev_free(void* p, size_t bytes, cudaStream_t s)
 {
     if (!p) return;
+    const bool tl = timeline_on();
+    const auto t0 = tl ? std::chrono::steady_clock::now() : std::chrono::steady_clock::time_point();
     cudaFreeAsync(p, s);
+    if (tl) alloc_stat(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(), 0);
     g_ctx.bytes_in_use.fetch_sub(bytes);
 }
 
@@ -158,6 +260,61 @@ TraceSpan::~TraceSpan()
 {
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
+}
+
+// ---- timeline: stream-ordered events, no synchronisation until the dump -------
+namespace {
+struct TimelineMark {
+    const char* tag;
+    cudaEvent_t e;
+};
+std::vector<TimelineMark> g_timeline;
+}  // namespace
+
+bool timeline_on()
+{
+    static const bool on = getenv("PIC_TIMELINE") != nullptr;
+    return on;
+}
+
+void timeline_mark(const char* tag, cudaStream_t s)
+{
+    if (!timeline_on()) return;
+    TimelineMark m{tag, nullptr};
+    PIC_CUDA(cudaEventCreate(&m.e));
+    PIC_CUDA(cudaEventRecord(m.e, s));
+    g_timeline.push_back(m);
+}
+
+void timeline_dump()
+{
+    if (!timeline_on() || g_timeline.empty()) return;
+    PIC_CUDA(cudaEventSynchronize(g_timeline.back().e));
+    for (size_t i = 1; i < g_timeline.size(); i++) {
+        float ms = 0;
+        PIC_CUDA(cudaEventElapsedTime(&ms, g_timeline[i - 1].e, g_timeline[i].e));
+        fprintf(stderr, "{\"timeline\": \"%s\", \"ms\": %.3f}\n", g_timeline[i].tag, ms);
+    }
+    for (auto& m : g_timeline) cudaEventDestroy(m.e);
+    g_timeline.clear();
+    fprintf(stderr, "{\"timeline_alloc\": {\"calls\": %zu, \"total_ms\": %.3f, \"max_ms\": %.3f, \"max_bytes\": %zu}}\n",
+            g_alloc_stat.calls, g_alloc_stat.total_ms, g_alloc_stat.max_ms, g_alloc_stat.max_bytes);
+    g_alloc_stat = AllocStat();
+}
+
+void trace_point(const char* tag, cudaStream_t s)
+{
+    if (!tracing()) return;
+    PIC_CUDA(cudaStreamSynchronize(s));
+    static const auto t0 = std::chrono::steady_clock::now();
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    cudaMemPool_t pool;
+    PIC_CUDA(cudaDeviceGetDefaultMemPool(&pool, g_ctx.device));
+    uint64_t reserved = 0, used_pool = 0;
+    PIC_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    PIC_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used_pool));
+    fprintf(stderr, "{\"trace\": \"point\", \"tag\": \"%s\", \"host_ms\": %.3f, \"pool_reserved_gb\": %.3f, "
+            "\"pool_used_gb\": %.3f}\n", tag, ms, reserved / 1e9, used_pool / 1e9);
 }
 
 // ---- live kernel timing ------------------------------------------------------
