@@ -70,6 +70,12 @@ constexpr int kCvtThreads = 256;
 constexpr int kCvtLPT = 2;  // 64-bit limbs per thread
 constexpr size_t kCvtLPC = (size_t)kCvtThreads * kCvtLPT;
 constexpr size_t kCvtWPC = 2 * kCvtLPC;
+// The CRT conversion needs three coefficients below its first limb, so a CTA
+// of 256 threads computes 512 coefficients (two per thread, no thread a
+// third) and owns the 509 limbs they complete.
+constexpr size_t kCrtSlots = (size_t)kCvtThreads * kCvtLPT;
+constexpr size_t kCrtLPC = kCrtSlots - 3;
+constexpr size_t kCrtWPC = 2 * kCrtLPC;
 
 struct Crt3Consts {
     uint64_t p[3];
@@ -108,8 +114,9 @@ __device__ __forceinline__ void crt3(const Crt3Consts& C, uint64_t y0, uint64_t 
     uint64_t t = sub_mod(r2, r0m2, C.p[2]);
     t = sub_mod(t, crt_mul(v1, C.p0m2, C.p[2], C.c[2]), C.p[2]);
     const uint64_t v2 = crt_mul(t, C.inv012, C.p[2], C.c[2]);
-    // p0 * v1 + r0
-    uint64_t a0 = C.p[0] * v1, a1 = mulhi64(C.p[0], v1);
+    // p0 * v1 + r0 = v1 + (c0 v1) 2^32 + r0 with two 32 x 32 products
+    const uint64_t x = (uint64_t)C.c[0] * (uint32_t)v1, y = (uint64_t)C.c[0] * (uint32_t)(v1 >> 32);
+    uint64_t a0 = v1 + (x << 32), a1 = (x >> 32) + y + (a0 < v1);
     a0 += r0;
     a1 += (a0 < r0);
     // (p0 p1) * v2
@@ -164,14 +171,15 @@ __device__ __forceinline__ void add128(uint64_t& lo, uint64_t& hi, uint64_t v)
 
 // Three-prime residues y[q * pstride + j] -> words.  Limb i (64 bits)
 // collects x_i.l0 + x_(i-1).l1 + x_(i-2).l2 (< 3 * 2^64).  One CTA handles
-// limbs [i0, i0 + kCvtLPC) of one product.
+// limbs [i0, i0 + kCrtLPC) of one product; slot t of xs holds coefficient
+// i0 - 3 + t.
 __device__ __forceinline__ void crt3_block(const uint64_t* __restrict__ Y, size_t pstride, size_t ncoef,
                                            const Crt3Consts& C, uint32_t* __restrict__ z, size_t zw, int64_t i0,
                                            uint32_t* agg_slot)
 {
-    __shared__ uint64_t xs[(kCvtLPC + 3) * 3];
+    __shared__ uint64_t xs[kCrtSlots * 3];
     const int64_t climit = (int64_t)((zw + 1) / 2);  // limbs this product needs
-    for (int t = threadIdx.x; t < (int)kCvtLPC + 3; t += blockDim.x) {
+    for (int t = threadIdx.x; t < (int)kCrtSlots; t += blockDim.x) {
         const int64_t j = i0 - 3 + t;
         uint64_t l0 = 0, l1 = 0, l2 = 0;
         if (j >= 0 && (size_t)j < ncoef && j < climit)
@@ -185,25 +193,32 @@ __device__ __forceinline__ void crt3_block(const uint64_t* __restrict__ Y, size_
     uint32_t gen[kCvtLPT];
 #pragma unroll
     for (int u = 0; u < kCvtLPT; u++) {
-        const int li = threadIdx.x * kCvtLPT + u + 3;  // xs slot of coefficient i
-        uint64_t slo = xs[3 * li], shi = 0;
-        add128(slo, shi, xs[3 * (li - 1) + 1]);
-        add128(slo, shi, xs[3 * (li - 2) + 2]);
-        uint64_t plo = xs[3 * (li - 1)], phi = 0;
-        add128(plo, phi, xs[3 * (li - 2) + 1]);
-        add128(plo, phi, xs[3 * (li - 3) + 2]);
-        const uint64_t d = slo + phi;
-        dig[u] = d;
-        gen[u] = d < slo;
+        const int l = threadIdx.x * kCvtLPT + u;  // limb i0 + l, xs slot l + 3
+        dig[u] = 0;
+        gen[u] = 0;
+        if (l < (int)kCrtLPC) {
+            const int li = l + 3;
+            uint64_t slo = xs[3 * li], shi = 0;
+            add128(slo, shi, xs[3 * (li - 1) + 1]);
+            add128(slo, shi, xs[3 * (li - 2) + 2]);
+            uint64_t plo = xs[3 * (li - 1)], phi = 0;
+            add128(plo, phi, xs[3 * (li - 2) + 1]);
+            add128(plo, phi, xs[3 * (li - 3) + 2]);
+            const uint64_t d = slo + phi;
+            dig[u] = d;
+            gen[u] = d < slo;
+        }
     }
-    limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw, agg_slot);
+    // words past this CTA's limbs belong to the next CTA
+    const size_t zend = 2 * ((size_t)i0 + kCrtLPC);
+    limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw < zend ? zw : zend, agg_slot);
 }
 
 __global__ void __launch_bounds__(kCvtThreads) crt3_k1(const uint64_t* __restrict__ Y, size_t N, size_t ncoef,
                                                        Crt3Consts C, uint32_t* __restrict__ z, size_t zw,
                                                        uint32_t* agg)
 {
-    crt3_block(Y, N, ncoef, C, z, zw, (int64_t)blockIdx.x * (int64_t)kCvtLPC, agg + blockIdx.x);
+    crt3_block(Y, N, ncoef, C, z, zw, (int64_t)blockIdx.x * (int64_t)kCrtLPC, agg + blockIdx.x);
 }
 
 // Batched: product i has residues at Y + i * istride (+ q * pstride), zlen[i]
@@ -216,7 +231,7 @@ __global__ void __launch_bounds__(kCvtThreads) crt3_batch_k1(const uint64_t* __r
 {
     const size_t prod = blockIdx.x / cpp, lc = blockIdx.x % cpp;
     crt3_block(Y + prod * istride, pstride, ncoef, C, z + prod * (size_t)zcap, zlen[prod],
-               (int64_t)lc * (int64_t)kCvtLPC, agg + blockIdx.x);
+               (int64_t)lc * (int64_t)kCrtLPC, agg + blockIdx.x);
 }
 
 // Coefficients c_j at bit offsets bits * j (8 <= bits <= 16) -> words.  Limb
@@ -302,6 +317,8 @@ __global__ void __launch_bounds__(kCvtThreads) coefbits_k1(Loader ld, size_t nco
     limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw, agg + blockIdx.x);
 }
 
+// Carries between the CTAs of a coefficient-bits conversion (kCvtLPC limbs
+// per CTA; the CRT conversions own kCrtLPC and ripple with kCrtWPC).
 static void finish_scan(uint32_t* z, size_t zw, uint32_t* agg, size_t nctas, cudaStream_t s)
 {
     carry_scan_aggregates(agg, nctas, nullptr, s);
@@ -408,13 +425,14 @@ void ntt3_inverse_to_words(uint64_t* y, int k, size_t ncoef, int depth, uint32_t
     ntt_inverse_dit(ntt3_batch(y, k), k, s);
     const Crt3Consts C = make_crt3(k, depth);
     const size_t nlimbs = (zw + 1) / 2;
-    const size_t nctas = (nlimbs + kCvtLPC - 1) / kCvtLPC;
+    const size_t nctas = (nlimbs + kCrtLPC - 1) / kCrtLPC;
     DevBuf<uint32_t> agg(nctas, s);
     ProfScope ps(KC_CRT, 24.0 * (double)ncoef + 4.0 * (double)zw, s);
     crt3_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(y, (size_t)1 << k, ncoef, C, z, zw, agg.get());
     PIC_CHECK_LAUNCH();
     count_launch();
-    finish_scan(z, zw, agg.get(), nctas, s);
+    carry_scan_aggregates(agg.get(), nctas, nullptr, s);
+    carry_ripple(z, zw, kCrtWPC, agg.get(), nctas, kCarryAdd, s);
 }
 
 void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
@@ -425,7 +443,7 @@ void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size
     Crt3Consts C = make_crt3(k, 1);
     if (offset)
         for (int q = 0; q < 3; q++) C.off[q] = host_powmod(2, 159, C.p[q]);
-    const size_t cpp = (((size_t)zcap + 1) / 2 + kCvtLPC - 1) / kCvtLPC;
+    const size_t cpp = (((size_t)zcap + 1) / 2 + kCrtLPC - 1) / kCrtLPC;
     const size_t nctas = count * cpp;
     DevBuf<uint32_t> agg(nctas, s);
     {
@@ -436,7 +454,7 @@ void ntt3_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size
         count_launch();
     }
     carry_scan_segments(agg.get(), count, cpp, s);
-    carry_ripple_batch(z, zcap, zlen, kCvtWPC, agg.get(), count, cpp, s);
+    carry_ripple_batch(z, zcap, zlen, kCrtWPC, agg.get(), count, cpp, s);
 }
 
 // Pieces used by the allocation-free product (noalloc.cu): the same split and
@@ -449,7 +467,7 @@ void split3_into(uint64_t* out, int k, const uint32_t* a, size_t na, const uint6
     count_launch();
 }
 
-size_t crt3_scratch_ctas(size_t zw) { return ((zw + 1) / 2 + kCvtLPC - 1) / kCvtLPC; }
+size_t crt3_scratch_ctas(size_t zw) { return ((zw + 1) / 2 + kCrtLPC - 1) / kCrtLPC; }
 
 void crt3_to_words_scratch(const uint64_t* y, int k, size_t ncoef, uint32_t* z, size_t zw, uint32_t* agg,
                            cudaStream_t s)
@@ -460,7 +478,7 @@ void crt3_to_words_scratch(const uint64_t* y, int k, size_t ncoef, uint32_t* z, 
     PIC_CHECK_LAUNCH();
     count_launch();
     carry_scan_aggregates(agg, nctas, nullptr, s);
-    carry_ripple(z, zw, kCvtWPC, agg, nctas, kCarryAdd, s);
+    carry_ripple(z, zw, kCrtWPC, agg, nctas, kCarryAdd, s);
 }
 
 // Wrapped products.  A product of operands of sa and sb pieces has
@@ -573,7 +591,8 @@ static void mul_ntt3_wrapped(uint32_t* z, const uint32_t* a, size_t na, const ui
     crt3_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(A.get(), ST, L, C, z, zw, agg.get());
     PIC_CHECK_LAUNCH();
     count_launch();
-    finish_scan(z, zw, agg.get(), nctas, s);
+    carry_scan_aggregates(agg.get(), nctas, nullptr, s);
+    carry_ripple(z, zw, kCrtWPC, agg.get(), nctas, kCarryAdd, s);
 }
 
 void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s)
