@@ -77,6 +77,10 @@ void shutdown_context()
     if (!g_init.load()) return;
     workspace_release_all();
     cudaStreamSynchronize(g_ctx.stream);
+    // hand the pool's unused memory back to the device (buffers other
+    // threads still hold keep theirs)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, g_ctx.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     if (g_ctx.pinned_words) cudaFreeHost(g_ctx.pinned_words);
     g_ctx.pinned_words = nullptr;
     cudaStreamDestroy(g_ctx.stream);
