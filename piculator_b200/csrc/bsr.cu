@@ -1801,6 +1801,7 @@ void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, s
             count_launch();
         }
     }
+    timeline_mark("bsr_bounds", s);
     // bottom level
     Level cur;
     {
@@ -1818,6 +1819,7 @@ void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, s
         PIC_CHECK_LAUNCH();
         count_launch();
     }
+    timeline_mark("bsr_bottom", s);
     // merge up to Dtop
     const size_t budget = merge_budget(p);
     for (int d = Db - 1; d >= Dtop; d--) {
