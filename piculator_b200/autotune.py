@@ -3,14 +3,18 @@
 Size classes and what is chosen for each:
   * NTT transform length 2^k (k = 10..27): row-pass bits (11, 12, 13), radix
     of the register rounds (8 or 16) and column-tile width (automatic or
-    4..32 columns), timed on three-prime products of that length;
+    4..32 columns), timed on three-prime products of that length; with
+    --batched, the geometry of k = 14..27 is timed instead where the pi run
+    uses it, on the batched merges of whole runs (one run per candidate,
+    every merge level timed by stream-ordered events and attributed to its
+    transform length);
   * single products by length: the form (schoolbook, three-prime NTT, FP64
     FFT, or the one-prime reference layout) -- i.e. the prime count and
     transform family -- as crossover thresholds;
   * binary splitting: the child length below which a level merges with the
     CTA schoolbook instead of batched NTTs, timed on whole 1e9-digit pi runs.
 
-    python -m piculator_b200.autotune [--quick] [--out PATH]
+    python -m piculator_b200.autotune [--quick] [--batched] [--out PATH]
 
 `piculator_b200.init()` applies the file it finds next to this module.
 Every candidate computes the same words (products are exact); only time
@@ -92,6 +96,63 @@ def tune_ntt(timer: Timer, ks, quick: bool) -> dict:
     return out
 
 
+def _timeline_ms_by_k(stderr: str) -> dict:
+    """Device ms per transform length from the last computation's timeline
+    (the lines PIC_TIMELINE prints; the merges that end at a mark carry k)."""
+    groups, cur = [], []
+    for line in stderr.splitlines():
+        line = line.strip()
+        if not line.startswith("{"):
+            continue
+        d = json.loads(line)
+        if "timeline" in d:
+            cur.append(d)
+        elif "timeline_alloc" in d:
+            groups.append(cur)
+            cur = []
+    out: dict = {}
+    for d in groups[-1] if groups else []:
+        if "k" in d:
+            out[d["k"]] = out.get(d["k"], 0.0) + d["ms"]
+    return out
+
+
+def tune_ntt_batched(digits: int, ks=range(14, 28)) -> dict:
+    """NTT geometry per length, timed on the batched merges of whole pi runs:
+    each candidate is applied to every length at once, the second of two runs
+    is timed, and each length takes the candidate whose merge levels of that
+    length were fastest (a level's wrapped tail product, usually two lengths
+    shorter, runs under the same candidate)."""
+    import subprocess
+    import sys
+    import tempfile
+    cands = [(row, lw) for row in (11, 12, 13) for lw in (0, 3, 5)]
+    ms: dict = {}
+    env = dict(os.environ, PIC_TIMELINE="1")
+    for row, lw in cands:
+        tab = {"ntt": {str(k): {"row_bits": row, "col_width_log2": lw, "radix_log2": 3} for k in ks}}
+        with tempfile.NamedTemporaryFile("w", suffix=".json", delete=False) as f:
+            json.dump(tab, f)
+            path = f.name
+        try:
+            r = subprocess.run([sys.executable, "-m", "piculator_b200.cli", "pi", "--digits", str(digits),
+                                "--repeat", "2", "--tuning", path], env=env, capture_output=True, text=True,
+                               check=True)
+        finally:
+            os.unlink(path)
+        for k, v in _timeline_ms_by_k(r.stderr).items():
+            ms.setdefault(k, {})[(row, lw)] = v
+        print(f"ntt batched {row}/{lw}: { {k: round(v[(row, lw)], 2) for k, v in sorted(ms.items())} }", flush=True)
+    out = {}
+    for k, by in sorted(ms.items()):
+        if k not in ks:
+            continue
+        (row, lw), best = min(by.items(), key=lambda kv: kv[1])
+        out[str(k)] = {"row_bits": row, "col_width_log2": lw, "radix_log2": 3, "ms_batched": best}
+        P.set_ntt_geometry(k, row, lw, 3)
+    return out
+
+
 def tune_products(timer: Timer) -> dict:
     torch = timer.torch
     rows = []
@@ -140,6 +201,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--quick", action="store_true")
     ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--batched", action="store_true",
+                    help="time the geometry of k >= 14 on the merges of whole pi runs")
     args = ap.parse_args()
     P.init(0, tuned=False)
     timer = Timer()
@@ -150,6 +213,8 @@ def main():
     except Exception:
         pass
     result["ntt"] = tune_ntt(timer, range(10, 28) if not args.quick else (14, 18, 22, 24, 26), args.quick)
+    if args.batched:
+        result["ntt"].update(tune_ntt_batched(10_000_000 if args.quick else 1_000_000_000))
     prod = tune_products(timer)
     result["products"] = prod
     P.set_tuning(P.TUNE_MUL_SCHOOL_MAX, prod["school_max_words"])

@@ -1,6 +1,7 @@
 """Command-line driver for the B200 engine.
 
     python -m piculator_b200.cli pi  --digits 1e9 [--repeat 2] [--form chosen|plain] [--out pi.txt]
+                                     [--tuning FILE]
     python -m piculator_b200.cli mul --words 8388608 [--mode ntt3] [--repeat 3]
 
 `pi` runs the reference's Pi() (PI.h:138-212) on the GPU: it prints one JSON
@@ -78,12 +79,15 @@ def main() -> None:
     p.add_argument("--form", choices=("chosen", "plain"), default="chosen")
     p.add_argument("--out", default=None, help="write the pi.txt text here")
     p.add_argument("--md5", action="store_true", help="print the md5 of the text")
+    p.add_argument("--tuning", default=None, help="a tuning file applied over the default one")
     m = sub.add_parser("mul", help="time an isolated product of two splitmix64 operands")
     m.add_argument("--words", default="8388608")
     m.add_argument("--mode", default="ntt3", choices=("auto", "school", "ntt3", "fft", "ntt_ref"))
     m.add_argument("--repeat", type=int, default=3)
     args = ap.parse_args()
     P.init(0)
+    if getattr(args, "tuning", None):
+        P.apply_tuning(args.tuning)
     if args.cmd == "pi":
         cmd_pi(args)
     else:

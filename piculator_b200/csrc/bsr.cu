@@ -1736,7 +1736,7 @@ static bool top_level_merge(const std::vector<BigFloat>& cP, const std::vector<B
         }
         ntt_products(ch, p0, n, sh, o, s, /*use_workspace=*/true);
         trace_point("top_merge_chunk", s);
-        timeline_mark("top_merge_chunk", s);
+        timeline_mark("top_merge_chunk", s, sh.k);
     }
     std::vector<uint32_t> hl(4 * np, 0);
     PIC_CUDA(cudaMemcpyAsync(hl.data(), lens.get(), 4 * (need_R ? 4 : 3) * np, cudaMemcpyDeviceToHost, s));
@@ -1841,7 +1841,7 @@ void bsr_chosen(BigFloat& P, BigFloat& Q, BigFloat& R, uint32_t a, uint32_t b, s
                     d, cnt, cur.P.cap, cur.Q.cap, cur.R.cap, school ? "school" : "ntt3", span.end_ms());
         cur = std::move(par);
         bnd[d + 1].reset();
-        timeline_mark(school ? "bsr_level_school" : "bsr_level_ntt", s);
+        timeline_mark(school ? "bsr_level_school" : "bsr_level_ntt", s, school ? -1 : merge_shape(cmax).k);
     }
     // hand the nodes at Dtop to the exact BigFloat recursion
     const size_t cnt = cur.count;

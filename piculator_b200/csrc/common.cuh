@@ -144,7 +144,9 @@ void trace_point(const char* tag, cudaStream_t s);
 // With PIC_TIMELINE set: record a stream-ordered event (no synchronisation);
 // timeline_dump prints the device time between consecutive marks, idle gaps
 // included.
-void timeline_mark(const char* tag, cudaStream_t s);
+// `k` (when >= 0) is printed with the mark: the log2 transform length of the
+// merges that end there.
+void timeline_mark(const char* tag, cudaStream_t s, int k = -1);
 void timeline_dump();
 struct TraceSpan {
     cudaEvent_t a = nullptr, b = nullptr;

@@ -271,6 +271,7 @@ namespace {
 struct TimelineMark {
     const char* tag;
     cudaEvent_t e;
+    int k;
 };
 std::vector<TimelineMark> g_timeline;
 }  // namespace
@@ -281,10 +282,10 @@ bool timeline_on()
     return on;
 }
 
-void timeline_mark(const char* tag, cudaStream_t s)
+void timeline_mark(const char* tag, cudaStream_t s, int k)
 {
     if (!timeline_on()) return;
-    TimelineMark m{tag, nullptr};
+    TimelineMark m{tag, nullptr, k};
     PIC_CUDA(cudaEventCreate(&m.e));
     PIC_CUDA(cudaEventRecord(m.e, s));
     g_timeline.push_back(m);
@@ -297,7 +298,11 @@ void timeline_dump()
     for (size_t i = 1; i < g_timeline.size(); i++) {
         float ms = 0;
         PIC_CUDA(cudaEventElapsedTime(&ms, g_timeline[i - 1].e, g_timeline[i].e));
-        fprintf(stderr, "{\"timeline\": \"%s\", \"ms\": %.3f}\n", g_timeline[i].tag, ms);
+        if (g_timeline[i].k >= 0)
+            fprintf(stderr, "{\"timeline\": \"%s\", \"k\": %d, \"ms\": %.3f}\n", g_timeline[i].tag, g_timeline[i].k,
+                    ms);
+        else
+            fprintf(stderr, "{\"timeline\": \"%s\", \"ms\": %.3f}\n", g_timeline[i].tag, ms);
     }
     for (auto& m : g_timeline) cudaEventDestroy(m.e);
     g_timeline.clear();

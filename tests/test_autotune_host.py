@@ -1,0 +1,29 @@
+"""Host logic of the autotuner's batched geometry stage: the per-length
+device times it reads from the timeline the library prints."""
+from __future__ import annotations
+
+import json
+
+from piculator_b200 import autotune
+
+
+def _lines(marks):
+    return "\n".join(json.dumps(m) for m in marks)
+
+
+def test_timeline_ms_by_k_takes_the_last_computation():
+    first = [{"timeline": "bsr_level_ntt", "k": 14, "ms": 99.0}, {"timeline_alloc": {"calls": 1}}]
+    second = [
+        {"timeline": "bsr_level_school", "ms": 5.0},
+        {"timeline": "bsr_level_ntt", "k": 14, "ms": 10.0},
+        {"timeline": "bsr_level_ntt", "k": 15, "ms": 20.0},
+        {"timeline": "top_merge_chunk", "k": 15, "ms": 7.5},
+        {"timeline": "pi_phase", "ms": 3.0},
+        {"timeline_alloc": {"calls": 2}},
+    ]
+    text = "noise\n" + _lines(first) + "\n" + _lines(second) + "\n"
+    assert autotune._timeline_ms_by_k(text) == {14: 10.0, 15: 27.5}
+
+
+def test_timeline_ms_by_k_empty():
+    assert autotune._timeline_ms_by_k("") == {}
