@@ -274,6 +274,7 @@ struct TimelineMark {
     int k;
 };
 std::vector<TimelineMark> g_timeline;
+std::mutex g_timeline_lock;
 }  // namespace
 
 bool timeline_on()
@@ -288,12 +289,15 @@ void timeline_mark(const char* tag, cudaStream_t s, int k)
     TimelineMark m{tag, nullptr, k};
     PIC_CUDA(cudaEventCreate(&m.e));
     PIC_CUDA(cudaEventRecord(m.e, s));
+    std::lock_guard<std::mutex> g(g_timeline_lock);
     g_timeline.push_back(m);
 }
 
 void timeline_dump()
 {
-    if (!timeline_on() || g_timeline.empty()) return;
+    if (!timeline_on()) return;
+    std::lock_guard<std::mutex> g(g_timeline_lock);
+    if (g_timeline.empty()) return;
     PIC_CUDA(cudaEventSynchronize(g_timeline.back().e));
     for (size_t i = 1; i < g_timeline.size(); i++) {
         float ms = 0;
