@@ -7,11 +7,13 @@ BigFloat methods (BigFloat.cpp) and NNT class (NTT.cpp) through
 oracle/_ref/libpicref.so for the rest.  Inputs are seeded splitmix64 streams,
 so the fixtures can be regenerated bit for bit:
 
-    python tests/golden/make_golden.py [--big]
+    python tests/golden/make_golden.py [--big] [--odd]
 
 --big adds the 10M- and 100M-digit pi runs (minutes of CPU); --huge also the
 1e9-digit run (about two hours on 8 cores; its entry keeps the thread count
-and time of the run that produced it).
+and time of the run that produced it); --odd the 3,141,593- and
+27,182,818-digit runs.  Entries already in the file for sizes not generated
+this time are kept.
 """
 from __future__ import annotations
 
@@ -49,10 +51,13 @@ def run_pi(digits: int, threads: int) -> tuple[bytes, dict]:
     return data, timing
 
 
-def gen_pi(big: bool, huge: bool = False) -> dict:
+def gen_pi(big: bool, huge: bool = False, odd: bool = False) -> dict:
     out = {}
     sizes = [10_000, 100_000, 1_000_000] + ([10_000_000, 100_000_000] if big or huge else [])
     sizes += [1_000_000_000] if huge else []
+    # sizes that are not powers of ten: other term counts, precisions and
+    # top-level shapes of the binary splitting
+    sizes += [3_141_593, 27_182_818] if odd else []
     for d in sizes:
         data, t = run_pi(d, os.cpu_count() or 1)
         out[str(d)] = {"md5": md5(data), "bytes": len(data), "head": data[:80].decode(),
@@ -162,10 +167,11 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--big", action="store_true")
     ap.add_argument("--huge", action="store_true")
+    ap.add_argument("--odd", action="store_true", help="also pi at 3,141,593 and 27,182,818 digits")
     args = ap.parse_args()
     ref = Reference()
     fixtures = {
-        "pi": gen_pi(args.big, args.huge),
+        "pi": gen_pi(args.big, args.huge, args.odd),
         "products": gen_products(ref),
         "ntt": gen_ntt(ref),
         "bigfloat": gen_bigfloat(ref),

@@ -35,6 +35,17 @@ def test_pi_large_matches_reference(pic, golden, digits):
     assert hashlib.md5(text).hexdigest() == g["md5"]
 
 
+@pytest.mark.parametrize("digits", [3_141_593, 27_182_818])
+def test_pi_odd_sizes_match_reference(pic, golden, digits):
+    """Digit counts that are not powers of ten: other term counts, working
+    precisions and top-level merge shapes, pi.txt equal to the reference's."""
+    text, _ = pic.pi_hex(digits, pic.PI_CHOSEN)
+    g = golden["pi"][str(digits)]
+    assert len(text) == g["bytes"]
+    assert text[-80:].decode() == g["tail"]
+    assert hashlib.md5(text).hexdigest() == g["md5"]
+
+
 def test_pi_oracle_agrees_small(pic, oracle):
     text, _ = pic.pi_hex(20_000, pic.PI_CHOSEN)
     assert text == oracle.pi_hex(20_000)
