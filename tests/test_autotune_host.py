@@ -27,3 +27,23 @@ def test_timeline_ms_by_k_takes_the_last_computation():
 
 def test_timeline_ms_by_k_empty():
     assert autotune._timeline_ms_by_k("") == {}
+
+
+def test_committed_tuning_table_is_well_formed():
+    """The table init() applies: every NTT length 2^10..2^27 with a geometry
+    the library accepts (row bits 8..13, column width 0..6, radix 2..4) and
+    the product and binary-splitting thresholds."""
+    import os
+
+    import piculator_b200 as P
+    assert os.path.exists(P.TUNING_FILE)
+    with open(P.TUNING_FILE) as f:
+        t = json.load(f)
+    for k in range(10, 28):
+        g = t["ntt"][str(k)]
+        assert 8 <= g["row_bits"] <= 13
+        assert 0 <= g["col_width_log2"] <= 6
+        assert 2 <= g["radix_log2"] <= 4
+    assert t["products"]["school_max_words"] >= 0
+    assert t["products"]["fft_max_words"] >= 0
+    assert t["bsr"]["bsr_school_max_words"] > 0
