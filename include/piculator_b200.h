@@ -75,6 +75,10 @@ pic_status pic_measure_butterfly_rate(double* gbfly_per_s);
 /* Test hook: make the next n device allocations fail with PIC_ERR_NO_MEMORY
  * (host-side fault injection; no GPU fault is involved). */
 void pic_debug_fail_allocations(int n);
+/* Test hook: how many allocations the library has made so far -- pool
+ * allocations, direct cudaMalloc of twiddle tables, pinned host staging.
+ * No reference counterpart (lets tests prove a path allocates nothing). */
+uint64_t pic_debug_allocation_count(void);
 
 /* ---- NTT.h:4-9 -- natural-order NTT mod the reference's prime for k ------ */
 /* T, A: device arrays of 2^k uint64 residues.  Same results word for word
@@ -108,6 +112,14 @@ pic_status pic_int_to_fft(double* T, int k, const uint32_t* A, size_t AL,
 pic_status pic_fft_to_int(const double* T, int k, uint32_t* A, size_t AL,
                           pic_stream s);                               /* FFT.h:9 */
 double pic_fft_last_max_err(void);
+/* FFT products whose largest rounding distance passed the acceptance
+ * threshold (0.25 unless PIC_TUNE_FFT_ACCEPT_PPM lowers it) and were
+ * recomputed with the exact three-prime NTT, since pic_init.  No reference
+ * counterpart: the reference never checks its FFT's rounding (FFT.cpp:520-571). */
+uint64_t pic_fft_recompute_count(void);
+/* Multi-word products formed since pic_init, whatever the kernel (pic_mul
+ * calls, batched products, four per binary-splitting merge). */
+uint64_t pic_product_count(void);
 
 /* ---- whole products (the core of BigFloat::mul, BigFloat.cpp:413-487) ---- */
 /* z[0 .. na+nb) = a * b exactly, device words, little-endian base 2^32.
@@ -238,7 +250,10 @@ enum {
     PIC_TUNE_BSR_WRAP = 4,       /* 1: binary-splitting NTT merges use wrapped products (default) */
     PIC_TUNE_BSR_SMALL_MERGE = 5, /* short schoolbook levels: 0 CTA, 1 + warp, 2 + thread per parent (default) */
     PIC_TUNE_MUL_WRAP = 6,        /* 1: three-prime products use the wrapped form when it is shorter (default) */
-    PIC_TUNE_BSR_COMBINE = 7      /* 1: binary-splitting NTT merges form P in the transform domain (default) */
+    PIC_TUNE_BSR_COMBINE = 7,     /* 1: binary-splitting NTT merges form P in the transform domain (default) */
+    PIC_TUNE_FFT_ACCEPT_PPM = 8   /* FFT products whose max rounding distance exceeds value * 1e-6 are
+                                     recomputed with NTT3 (default 250000 = 0.25; lower it to test the
+                                     recompute path) */
 };
 pic_status pic_set_tuning(int knob, int64_t value);
 int64_t pic_get_tuning(int knob);

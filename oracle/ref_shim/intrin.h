@@ -24,11 +24,17 @@ static inline uint64_t _umul128(uint64_t a, uint64_t b, uint64_t* hi)
     return (uint64_t)r;
 }
 
+/* MSVC's _udiv128 is the single x86-64 instruction DIV r/m64 (RDX:RAX / d),
+ * which faults when the quotient does not fit in 64 bits.  The same
+ * instruction here, rather than an unsigned __int128 division (a libgcc call
+ * several times slower), so the reference's modmul (NTT.cpp:85-90, 277-282)
+ * runs at the speed its author measured.  Every call site passes hi < d. */
 static inline uint64_t _udiv128(uint64_t hi, uint64_t lo, uint64_t d, uint64_t* rem)
 {
-    unsigned __int128 n = ((unsigned __int128)hi << 64) | lo;
-    *rem = (uint64_t)(n % d);
-    return (uint64_t)(n / d);
+    uint64_t q, r;
+    __asm__("divq %4" : "=a"(q), "=d"(r) : "a"(lo), "d"(hi), "rm"(d) : "cc");
+    *rem = r;
+    return q;
 }
 
 #define _mm_malloc(size, align) _mm_malloc((size), 64)

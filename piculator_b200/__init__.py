@@ -77,6 +77,7 @@ _SIGS = {
     "pic_synchronize": ([], C.c_int),
     "pic_device_bytes_in_use": ([], C.c_uint64),
     "pic_debug_fail_allocations": ([C.c_int], None),
+    "pic_debug_allocation_count": ([], C.c_uint64),
     "pic_default_stream": ([], C.c_void_p),
     "pic_profile_begin": ([], C.c_int),
     "pic_profile_end": ([C.POINTER(KernelStat), C.c_int, C.POINTER(C.c_int)], C.c_int),
@@ -96,6 +97,8 @@ _SIGS = {
     "pic_int_to_fft": ([_DP, C.c_int, _U32P, C.c_size_t, _P], C.c_int),
     "pic_fft_to_int": ([_DP, C.c_int, _U32P, C.c_size_t, _P], C.c_int),
     "pic_fft_last_max_err": ([], C.c_double),
+    "pic_fft_recompute_count": ([], C.c_uint64),
+    "pic_product_count": ([], C.c_uint64),
     "pic_mul": ([_U32P, _U32P, C.c_size_t, _U32P, C.c_size_t, C.c_int, _P], C.c_int),
     "pic_mul_batch": ([C.POINTER(MulDesc), C.c_size_t, C.c_int, _P], C.c_int),
     "pic_mul_noalloc": ([_U32P, _U32P, C.c_size_t, _U32P, C.c_size_t, _P], C.c_int),
@@ -339,7 +342,7 @@ class Transform:
 
 
 (TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS, TUNE_BSR_WRAP,
- TUNE_BSR_SMALL_MERGE, TUNE_MUL_WRAP, TUNE_BSR_COMBINE) = range(8)
+ TUNE_BSR_SMALL_MERGE, TUNE_MUL_WRAP, TUNE_BSR_COMBINE, TUNE_FFT_ACCEPT_PPM) = range(9)
 
 
 def butterfly_rate() -> float:

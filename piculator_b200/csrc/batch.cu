@@ -256,6 +256,7 @@ static std::unique_ptr<Plan> build_plan(const pic_mul_desc* d, size_t count, int
     P->sizes = sig;
     P->desc = DevBuf<DevDesc>(count, s);
     PIC_CUDA(cudaMallocHost((void**)&P->host_desc, sizeof(DevDesc) * count));
+    ctx().alloc_calls.fetch_add(1);
     P->counter = DevBuf<uint32_t>(1, s);
     std::map<int, Bin> bins;
     for (size_t i = 0; i < count; i++) {
@@ -290,6 +291,7 @@ static std::unique_ptr<Plan> build_plan(const pic_mul_desc* d, size_t count, int
 
 void mul_batch(const pic_mul_desc* d, size_t count, int mode, cudaStream_t s)
 {
+    count_products(count);
     if (count == 0) return;
     std::vector<uint32_t> sig;
     sig.reserve(2 * count + 1);

@@ -1490,6 +1490,7 @@ static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
     const uint32_t cmax = std::max(ccP, std::max(ccQ, ccR));
     const MergeShape sh = merge_shape(cmax);
     const size_t ncoef = products_ncoef(sh);
+    count_products(4 * par.count);  // P0 Q1, P1 R0, Q0 Q1, R0 R1 per parent (PI.h:110-112)
     // combined form: P = sL (T1 +- T2) converted once as V + K (the CRT adds
     // 2^159 to every coefficient so the signed ones stay exact), then
     // P = sL (V + K) - sL K with the exact signed sum
@@ -1569,6 +1570,7 @@ static void merge_school(Level& ch, Level& par, cudaStream_t s)
     if (smem > 48 * 1024)
         PIC_CUDA(cudaFuncSetAttribute(merge_school_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const uint32_t cmax = std::max(m.ccP, std::max(m.ccQ, m.ccR));
+    count_products(4 * par.count);  // P0 Q1, P1 R0, Q0 Q1, R0 R1 per parent (PI.h:110-112)
     ProfScope ps(KC_BSR, 4.0 * (double)par.count * 2.0 * (m.ccP + m.ccQ + m.ccR), s);
     if (g_small_merge >= 2 && (launch_merge_thread<16, 16, 12>(m, s) || launch_merge_thread<20, 20, 14>(m, s) ||
                                launch_merge_thread<28, 28, 20>(m, s))) {
@@ -1715,6 +1717,7 @@ static bool top_level_merge(const std::vector<BigFloat>& cP, const std::vector<B
     auto sT1 = alloc_words(np * c1), sT2 = alloc_words(np * c2), sQ = alloc_words(np * cq);
     std::shared_ptr<WordStore> sR = need_R ? alloc_words(np * cr) : nullptr;
     DevBuf<uint32_t> lens(4 * np, s);
+    count_products((need_R ? 4 : 3) * np);
     size_t chunk = merge_budget(p) / ntt_bytes_per_parent(sh);
     if (chunk < 1) chunk = 1;
     for (size_t p0 = 0; p0 < np; p0 += chunk) {

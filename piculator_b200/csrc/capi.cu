@@ -113,6 +113,8 @@ uint64_t pic_device_bytes_in_use(void) { return ctx().bytes_in_use.load(); }
 
 void pic_debug_fail_allocations(int n) { ctx().fail_allocs.store(n); }
 
+uint64_t pic_debug_allocation_count(void) { return ctx().alloc_calls.load(); }
+
 pic_stream pic_default_stream(void) { return initialized() ? (pic_stream)ctx().stream : nullptr; }
 
 pic_status pic_profile_begin(void)
@@ -289,6 +291,10 @@ pic_status pic_fft_to_int(const double* T, int k, uint32_t* A, size_t AL, pic_st
 }
 
 double pic_fft_last_max_err(void) { return fft_last_max_err(); }
+
+uint64_t pic_fft_recompute_count(void) { return ctx().fft_recomputes.load(); }
+
+uint64_t pic_product_count(void) { return ctx().products.load(); }
 
 // ---- products -----------------------------------------------------------------
 pic_status pic_mul(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int mode,
@@ -568,6 +574,10 @@ pic_status pic_set_tuning(int knob, int64_t value)
             PIC_REQUIRE(value <= 2, PIC_ERR_INVALID, "small-merge mode is 0, 1 or 2");
             bsr_set_small_merge((int)value);
             break;
+        case PIC_TUNE_FFT_ACCEPT_PPM:
+            PIC_REQUIRE(value <= 500000, PIC_ERR_INVALID, "FFT acceptance is at most 500000 ppm (0.5)");
+            mul_set_fft_accept((double)value * 1e-6);
+            break;
         default: throw Error(PIC_ERR_INVALID, "unknown tuning knob");
         }
     });
@@ -599,6 +609,7 @@ int64_t pic_get_tuning(int knob)
     case PIC_TUNE_BSR_SMALL_MERGE: return bsr_small_merge();
     case PIC_TUNE_MUL_WRAP: return mul_wrap() ? 1 : 0;
     case PIC_TUNE_BSR_COMBINE: return bsr_combine() ? 1 : 0;
+    case PIC_TUNE_FFT_ACCEPT_PPM: return (int64_t)llround(mul_fft_accept() * 1e6);
     }
     return -1;
 }

@@ -44,6 +44,9 @@ struct Context {
     std::atomic<uint64_t> launches{0};   // kernel launches issued by the library
     std::atomic<uint64_t> bytes_in_use{0};
     std::atomic<int> fail_allocs{0};     // fault-injection hook
+    std::atomic<uint64_t> alloc_calls{0};  // device allocations made (pool and direct)
+    std::atomic<uint64_t> products{0};     // multi-word products formed (any kernel)
+    std::atomic<uint64_t> fft_recomputes{0};  // FFT products redone with the NTT
     uint32_t* pinned_words = nullptr;    // small pinned staging for metadata reads
     size_t pinned_words_cap = 0;
 };
@@ -54,11 +57,15 @@ void require_init();
 cudaStream_t resolve(pic_stream s);
 
 inline void count_launch(uint64_t n = 1) { ctx().launches.fetch_add(n, std::memory_order_relaxed); }
+inline void count_products(uint64_t n) { ctx().products.fetch_add(n, std::memory_order_relaxed); }
 
 // ---- device memory -----------------------------------------------------------
 // Stream-ordered allocations from the device's default memory pool (release
 // threshold raised at init so freed blocks stay cached for reuse).
 void* dev_alloc(size_t bytes, cudaStream_t s);
+// cudaMalloc for the long-lived tables (twiddles), counted with the pool
+// allocations; returns cudaSuccess or the error, which it clears.
+cudaError_t raw_dev_alloc(void** p, size_t bytes);
 void dev_free(void* p, size_t bytes, cudaStream_t s);
 // Free device memory plus what the allocation pool holds unused.
 size_t device_available_bytes();

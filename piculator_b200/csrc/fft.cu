@@ -28,7 +28,7 @@ static FftTables g_fft;
 static double2* upload2(const std::vector<double2>& v)
 {
     double2* d = nullptr;
-    PIC_CUDA(cudaMalloc(&d, v.size() * sizeof(double2)));
+    PIC_CUDA(raw_dev_alloc((void**)&d, v.size() * sizeof(double2)));
     PIC_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(double2), cudaMemcpyHostToDevice));
     return d;
 }

@@ -759,6 +759,7 @@ int mul_auto_mode(size_t na, size_t nb)
 }
 
 static std::atomic<uint64_t> g_fft_err_bits{0};
+static std::atomic<uint64_t> g_fft_err_max_bits{0};  // largest since fft_reset_max_err
 double fft_last_max_err()
 {
     uint64_t b = g_fft_err_bits.load();
@@ -766,18 +767,38 @@ double fft_last_max_err()
     memcpy(&d, &b, sizeof d);
     return d;
 }
+double fft_max_err_seen()
+{
+    uint64_t b = g_fft_err_max_bits.load();
+    double d;
+    memcpy(&d, &b, sizeof d);
+    return d;
+}
+void fft_reset_max_err() { g_fft_err_max_bits.store(0); }
 void fft_note_max_err(double e)
 {
     uint64_t b;
     memcpy(&b, &e, sizeof b);
     g_fft_err_bits.store(b);
+    // nonnegative doubles order like their bit patterns
+    uint64_t cur = g_fft_err_max_bits.load();
+    while (b > cur && !g_fft_err_max_bits.compare_exchange_weak(cur, b)) {
+    }
 }
+
+// Largest accepted distance to the nearest integer of an FFT product's
+// coefficients; past it the product is recomputed with the three-prime NTT.
+// 0.25 is the production value; tests lower it to force the recompute.
+static double g_fft_accept = 0.25;
+void mul_set_fft_accept(double max_dist) { g_fft_accept = max_dist; }
+double mul_fft_accept() { return g_fft_accept; }
 
 void mul_dispatch(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int mode,
                   cudaStream_t s)
 {
     PIC_REQUIRE(na > 0 && nb > 0, PIC_ERR_INVALID, "empty operand");
     if (mode == PIC_MUL_AUTO) mode = mul_auto_mode(na, nb);
+    count_products(1);
     switch (mode) {
     case PIC_MUL_SCHOOL:
         if (na + nb <= kSchoolMaxWords) {
@@ -790,7 +811,12 @@ void mul_dispatch(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, 
     case PIC_MUL_NTT3: mul_ntt3(z, a, na, b, nb, s); return;
     case PIC_MUL_FFT: {
         double e = 0;
-        if (!mul_fft(z, a, na, b, nb, s, &e)) mul_ntt3(z, a, na, b, nb, s);
+        if (!mul_fft(z, a, na, b, nb, s, &e) || e > g_fft_accept) {
+            // the NTT is the oracle: a product whose rounding distance passed
+            // the acceptance threshold is redone exactly
+            ctx().fft_recomputes.fetch_add(1);
+            mul_ntt3(z, a, na, b, nb, s);
+        }
         return;
     }
     default: throw Error(PIC_ERR_INVALID, "unknown multiply mode");

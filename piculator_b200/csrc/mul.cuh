@@ -91,5 +91,11 @@ double fft_coef_to_words(const double2* T, size_t ncoef, double scale, int bits,
 
 double fft_last_max_err();
 void fft_note_max_err(double e);
+// Largest FFT rounding distance noted since the last reset (pi statistics).
+double fft_max_err_seen();
+void fft_reset_max_err();
+// FFT acceptance threshold (max distance to the nearest integer; default 0.25).
+void mul_set_fft_accept(double max_dist);
+double mul_fft_accept();
 
 }  // namespace pic

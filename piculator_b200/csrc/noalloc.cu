@@ -16,9 +16,12 @@
 //   product); longer products are rejected with PIC_ERR_LENGTH.
 // All calls share the arrays: two calls that overlap on the GPU (different
 // streams, or different host threads on one device) race and corrupt each
-// other's results.  Every buffer is fully written before it is read within a
-// call (the split writes all 2^k residues including the zero padding), so no
-// clearing is needed between calls.
+// other's results.  Every buffer is fully written before it is read within
+// a call (the split writes all 2^k residues including the zero padding), so
+// no clearing is needed between calls.  The tables hold only the two-level
+// roots, not the per-level and per-pass tables of pic_mul (pass tables are
+// allocated on first use), so these transforms run on the general NTT
+// kernels: the same words as pic_mul, somewhat slower.
 #include <stdio.h>
 
 #include <mutex>
@@ -94,11 +97,16 @@ NoallocDevice g_noalloc[64];
 // addresses (host code may not use the symbols' host-side stand-ins) and fill
 // the twiddle tables.  Runs inside the first pic_mul_noalloc call on each
 // device; it synchronises that stream, so the first call belongs outside any
-// stream capture.
+// stream capture.  The addresses and tables belong to the calling thread's
+// current device, so that device, the stream's device and the library's
+// device must all be the same one (else PIC_ERR_INVALID).
 static const NoallocDevice& noalloc_setup(cudaStream_t s)
 {
-    int dev = 0;
+    int dev = 0, sdev = 0;
     PIC_CUDA(cudaGetDevice(&dev));
+    PIC_CUDA(cudaStreamGetDevice(s, &sdev));
+    PIC_REQUIRE(dev == ctx().device && sdev == ctx().device, PIC_ERR_INVALID,
+                "pic_mul_noalloc: the current device and the stream's device must be the one given to pic_init");
     PIC_REQUIRE(dev >= 0 && dev < 64, PIC_ERR_INVALID, "device index out of range");
     std::lock_guard<std::mutex> g(g_noalloc_lock);
     NoallocDevice& d = g_noalloc[dev];

@@ -72,7 +72,7 @@ static std::map<uint64_t, PrimeTables*> g_tabs;
 static uint64_t* upload(const std::vector<uint64_t>& v)
 {
     uint64_t* d = nullptr;
-    PIC_CUDA(cudaMalloc(&d, v.size() * sizeof(uint64_t)));
+    PIC_CUDA(raw_dev_alloc((void**)&d, v.size() * sizeof(uint64_t)));
     PIC_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
     return d;
 }
@@ -1039,17 +1039,22 @@ static bool launch_rows_fast(const NttBatch& b, int k, int lr, cudaStream_t s)
 
 // Pass twiddle tables for root orders up to 2^kPassTableMaxBits (at most
 // 6 x 16 x 2^24 bytes per order for the three product primes): built on the
-// device on first use per (prime, direction, order, column height), kept for
-// the process; never built while the stream is being captured (the pass then
-// forms its twiddles from the two-level tables).
+// device on first use per (device, prime, direction, order, column height),
+// kept for the process; never built while the stream is being captured (the
+// pass then forms its twiddles from the two-level tables).  A table enters
+// the cache only after its build kernel has finished (the building stream is
+// synchronised), so a pass on any other stream that finds it in the cache
+// reads a complete table.
 constexpr int kPassTableMaxBits = 24;
 static std::mutex g_pass_lock;
-static std::map<std::tuple<uint64_t, int, int, int>, ulonglong2*> g_pass_tables;
+static std::map<std::tuple<int, uint64_t, int, int, int>, ulonglong2*> g_pass_tables;
 
 static const ulonglong2* pass_table(const PrimeDev& P, bool inv, int lblock, int lc, cudaStream_t s)
 {
     if (lblock > kPassTableMaxBits) return nullptr;
-    const auto key = std::make_tuple(P.p, inv ? 1 : 0, lblock, lc);
+    int dev = 0;
+    PIC_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, P.p, inv ? 1 : 0, lblock, lc);
     std::lock_guard<std::mutex> g(g_pass_lock);
     auto it = g_pass_tables.find(key);
     if (it != g_pass_tables.end()) return it->second;
@@ -1057,14 +1062,13 @@ static const ulonglong2* pass_table(const PrimeDev& P, bool inv, int lblock, int
     PIC_CUDA(cudaStreamIsCapturing(s, &cs));
     if (cs != cudaStreamCaptureStatusNone) return nullptr;
     ulonglong2* d = nullptr;
-    if (cudaMalloc(&d, sizeof(ulonglong2) << lblock) != cudaSuccess) {
-        cudaGetLastError();
+    if (raw_dev_alloc((void**)&d, sizeof(ulonglong2) << lblock) != cudaSuccess)
         return nullptr;  // no room: the pass keeps the two-level tables
-    }
     const size_t n = (size_t)1 << lblock;
     pass_table_kernel<<<grid_for(n, 256), 256, 0, s>>>(d, P, inv ? 1 : 0, lblock, lc);
     PIC_CHECK_LAUNCH();
     count_launch();
+    PIC_CUDA(cudaStreamSynchronize(s));  // complete before any other stream can find it
     g_pass_tables[key] = d;
     return d;
 }

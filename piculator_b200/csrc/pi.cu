@@ -97,6 +97,9 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
     pi_sizes(decimal_digits, &hex, &p, &terms);
     if ((uint32_t)terms != terms) throw Error(PIC_ERR_LIMIT, "Limit Exceeded");  // PI.h:150-151
     const uint64_t launches0 = ctx().launches.load();
+    const uint64_t products0 = ctx().products.load();
+    const uint64_t recompute0 = ctx().fft_recomputes.load();
+    fft_reset_max_err();
     const int saved_mode = get_mul_mode();
     set_mul_mode(mode == PIC_PI_PLAIN ? PIC_MUL_NTT_REF : PIC_MUL_AUTO);
     // the chosen form peaks below 512 bytes per word of precision (merge
@@ -139,7 +142,9 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
         st->seconds_final_mul = tm.secs(3, 4);
         st->seconds_total = tm.secs(0, 4);
         st->kernel_launches = ctx().launches.load() - launches0;
-        st->fft_max_err = fft_last_max_err();
+        st->products = ctx().products.load() - products0;
+        st->fft_max_err = fft_max_err_seen();
+        st->fft_recomputes = ctx().fft_recomputes.load() - recompute0;
     }
     return P;
 }

@@ -128,7 +128,19 @@ void* dev_alloc(size_t bytes, cudaStream_t s)
         throw Error(PIC_ERR_NO_MEMORY, buf);
     }
     g_ctx.bytes_in_use.fetch_add(bytes);
+    g_ctx.alloc_calls.fetch_add(1);
     return p;
+}
+
+cudaError_t raw_dev_alloc(void** p, size_t bytes)
+{
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return e;
+    }
+    g_ctx.alloc_calls.fetch_add(1);
+    return e;
 }
 
 size_t device_available_bytes()
@@ -163,6 +175,7 @@ void reserve_pool(size_t bytes, cudaStream_t s)
         cudaGetLastError();  // no room for one block that size: allocate as needed instead
         return;
     }
+    g_ctx.alloc_calls.fetch_add(1);
     PIC_CUDA(cudaFreeAsync(p, s));
     PIC_CUDA(cudaStreamSynchronize(s));
 }

@@ -14,6 +14,12 @@ so the fixtures can be regenerated bit for bit:
 and time of the run that produced it); --odd the 3,141,593- and
 27,182,818-digit runs.  Entries already in the file for sizes not generated
 this time are kept.
+
+    python tests/golden/make_golden.py --big-products
+
+only adds the isolated products of 2^24 and 2^27 words (the reference's NTT
+at k = 27 and k = 30; about 26 GB of host memory and several minutes for
+2^27) to the existing file, leaving every other entry as it is.
 """
 from __future__ import annotations
 
@@ -24,6 +30,7 @@ import os
 import subprocess
 import sys
 import tempfile
+import time
 
 import numpy as np
 
@@ -108,6 +115,24 @@ def gen_products(ref: Reference) -> dict:
     return cases
 
 
+def gen_big_products(ref: Reference) -> list:
+    """BigFloat::mul(x, 0) of 2^24- and 2^27-word splitmix64 operands (seeds
+    42 / 43): the reference's NTT path (BigFloat.cpp:416-441) at k = 27 and
+    k = 30.  Stored as md5 of the product words, length and top word."""
+    out = []
+    for lg in [24, 27]:
+        n = 1 << lg
+        a = random_words(42, n)
+        b = random_words(43, n)
+        t0 = time.time()
+        z = ref.mul(BF(True, 0, a), BF(True, 0, b), 0, threads=os.cpu_count() or 1)
+        out.append({"log2n": lg, "md5": words_md5(z.words), "L": z.L, "top": int(z.words[-1]),
+                    "ref_seconds": round(time.time() - t0, 2), "threads": os.cpu_count() or 1})
+        print(f"product 2^{lg}: {out[-1]['md5']} ({out[-1]['ref_seconds']} s)", flush=True)
+        del z
+    return out
+
+
 def gen_ntt(ref: Reference) -> dict:
     """NNT::NTT / iNTT (NTT.cpp:74-84) outputs at k = 11..16."""
     out = []
@@ -168,8 +193,19 @@ def main():
     ap.add_argument("--big", action="store_true")
     ap.add_argument("--huge", action="store_true")
     ap.add_argument("--odd", action="store_true", help="also pi at 3,141,593 and 27,182,818 digits")
+    ap.add_argument("--big-products", action="store_true",
+                    help="only add the 2^24- and 2^27-word products to the existing file")
     args = ap.parse_args()
     ref = Reference()
+    path = os.path.join(HERE, "reference_golden.json")
+    if args.big_products:
+        fixtures = json.load(open(path))
+        big = gen_big_products(ref)
+        iso = [e for e in fixtures["products"]["isolated"] if e["log2n"] not in (24, 27)]
+        fixtures["products"]["isolated"] = sorted(iso + big, key=lambda e: e["log2n"])
+        json.dump(fixtures, open(path, "w"), indent=1, sort_keys=True)
+        print("wrote", path)
+        return
     fixtures = {
         "pi": gen_pi(args.big, args.huge, args.odd),
         "products": gen_products(ref),
@@ -177,11 +213,12 @@ def main():
         "bigfloat": gen_bigfloat(ref),
         "generator": "tests/golden/make_golden.py (reference compiled from its own sources)",
     }
-    path = os.path.join(HERE, "reference_golden.json")
     if os.path.exists(path):
         old = json.load(open(path))
         for d, v in old.get("pi", {}).items():
             fixtures["pi"].setdefault(d, v)
+        fixtures["products"]["isolated"] += [e for e in old["products"]["isolated"]
+                                             if e["log2n"] in (24, 27)]
     json.dump(fixtures, open(path, "w"), indent=1, sort_keys=True)
     print("wrote", path)
 

@@ -68,6 +68,42 @@ def test_isolated_products_golden(pic, golden, lg, mode):
     assert L == rec["L"] and _md5(z[:L]) == rec["md5"]
 
 
+@pytest.fixture(scope="module")
+def big_operands():
+    cache = {}
+
+    def get(lg):
+        if lg not in cache:
+            cache.clear()
+            n = 1 << lg
+            cache[lg] = (random_words(42, n), random_words(43, n))
+        return cache[lg]
+    return get
+
+
+# The isolated-multiply workload at its two largest sizes: 2^24 and 2^27
+# words per operand, the reference's NTT at k = 27 and k = 30
+# (BigFloat.cpp:380-441).  The fixture holds the md5 of the reference's own
+# product words.  The FP64 FFT has no proven piece width at these lengths.
+@pytest.mark.parametrize("lg", [24, 27])
+@pytest.mark.parametrize("mode", ["ntt3", "ntt_ref", "auto"])
+def test_isolated_products_golden_large(pic, golden, big_operands, lg, mode):
+    rec = [r for r in golden["products"]["isolated"] if r["log2n"] == lg][0]
+    a, b = big_operands(lg)
+    z = pic.mul_host(a, b, mode)
+    L = z.size - (1 if z[-1] == 0 else 0)
+    assert L == rec["L"] and int(z[L - 1]) == rec["top"]
+    assert _md5(z[:L]) == rec["md5"]
+
+
+def test_fft_beyond_proven_bound_is_refused(pic):
+    n = 1 << 24
+    a = np.ones(n, dtype=np.uint32)
+    with pytest.raises(pic.PicError) as e:
+        pic.mul_host(a, a, "fft")
+    assert e.value.status == pic.ERR_LENGTH
+
+
 @pytest.mark.parametrize("lg", [22, 24])
 def test_large_products_fingerprint(pic, lg):
     """Mod-prime fingerprints where Python-int products would be slow:
@@ -155,6 +191,32 @@ def test_mul_batch_uneven(pic, torch_cuda, oracle):
 
 def test_fft_error_is_logged(pic):
     a, b = random_words(1, 1 << 15), random_words(2, 1 << 15)
+    n0 = pic.lib().pic_fft_recompute_count()
     pic.mul_host(a, b, "fft")
     e = pic.lib().pic_fft_last_max_err()
     assert 0.0 < e < 0.25
+    assert pic.lib().pic_fft_recompute_count() == n0
+
+
+@pytest.mark.parametrize("n", [1 << 12, 1 << 15, 100000])
+def test_fft_recompute_past_threshold(pic, n):
+    """With the acceptance threshold lowered below the products' rounding
+    distance, every FFT product takes the NTT recompute branch: the words are
+    still exact and the recompute counter moves by one per product."""
+    L = pic.lib()
+    a, b = random_words(3 * n, n), random_words(3 * n + 1, n - 7)
+    want = _int(a) * _int(b)
+    saved = pic.get_tuning(pic.TUNE_FFT_ACCEPT_PPM)
+    assert saved == 250000
+    try:
+        pic.set_tuning(pic.TUNE_FFT_ACCEPT_PPM, 0)
+        n0 = L.pic_fft_recompute_count()
+        z = pic.mul_host(a, b, "fft")
+        assert L.pic_fft_last_max_err() > 0.0
+        assert L.pic_fft_recompute_count() == n0 + 1
+        assert _int(z) == want
+    finally:
+        pic.set_tuning(pic.TUNE_FFT_ACCEPT_PPM, saved)
+    n1 = L.pic_fft_recompute_count()
+    assert _int(pic.mul_host(a, b, "fft")) == want
+    assert L.pic_fft_recompute_count() == n1

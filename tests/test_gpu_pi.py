@@ -49,3 +49,27 @@ def test_pi_odd_sizes_match_reference(pic, golden, digits):
 def test_pi_oracle_agrees_small(pic, oracle):
     text, _ = pic.pi_hex(20_000, pic.PI_CHOSEN)
     assert text == oracle.pi_hex(20_000)
+
+
+def test_pi_precision_selected_form_counts_fft_products(pic, golden):
+    """The precision-selected form with the FP64 FFT serving every product up
+    to 4 M words (the binary-splitting top levels and the Newton steps):
+    pi.txt is still the reference's, the statistics report the products and
+    the FFT's largest rounding distance; with the acceptance threshold at 0
+    every FFT product is recomputed with the NTT and the text is unchanged."""
+    saved_fft = pic.get_tuning(pic.TUNE_MUL_FFT_MAX)
+    saved_acc = pic.get_tuning(pic.TUNE_FFT_ACCEPT_PPM)
+    try:
+        pic.set_tuning(pic.TUNE_MUL_FFT_MAX, 1 << 22)
+        text, st = pic.pi_hex(1_000_000, pic.PI_CHOSEN)
+        assert hashlib.md5(text).hexdigest() == golden["pi"]["1000000"]["md5"]
+        assert st["products"] > 0
+        assert 0.0 < st["fft_max_err"] < 0.25
+        assert st["fft_recomputes"] == 0
+        pic.set_tuning(pic.TUNE_FFT_ACCEPT_PPM, 0)
+        text, st = pic.pi_hex(100_000, pic.PI_CHOSEN)
+        assert hashlib.md5(text).hexdigest() == golden["pi"]["100000"]["md5"]
+        assert st["fft_recomputes"] > 0
+    finally:
+        pic.set_tuning(pic.TUNE_MUL_FFT_MAX, saved_fft)
+        pic.set_tuning(pic.TUNE_FFT_ACCEPT_PPM, saved_acc)
