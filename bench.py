@@ -14,9 +14,17 @@ the timed region).  Multi-GPU runs are independent replicas (the path has no
 exchange step); the reported time is the max over ranks.
 
 --impl reference times the reference's own CPU program (oracle/_ref/picref_pi,
-built from the reference sources) on this host's cores instead: each step is a
-bounded pi run at --ref-sample digits, extrapolated to --digits with the
-scaling exponent measured between two sample sizes in the same run.
+built from the reference sources) on this host's cores instead.  The first
+warm-up step is a whole reference run at 10^8 digits, measured; every other
+step is a bounded run at --ref-sample digits.  The 10^9 value is the measured
+10^8 time on this host times the ratio of the reference's own 10^9 and 10^8
+runs (both measured, same program and thread count, recorded in
+tests/golden/reference_golden.json).  Power laws fitted between two smaller
+sizes underestimate that ratio: the reference switches from its FFT to its
+much slower NTT only near 10^8 digits (BigFloat.cpp:386).
+
+--gpus N without a torchrun environment re-launches this script under
+torch.distributed.run with N processes (one per GPU, independent replicas).
 """
 from __future__ import annotations
 
@@ -44,10 +52,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--digits", type=int, default=1_000_000_000)
     ap.add_argument("--form", choices=["chosen", "plain"], default="chosen")
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--impl", choices=["ours", "reference", "replica-check"], default="ours",
+                    help="replica-check: the launcher's self-test (no GPU, gloo ranks, no computation)")
     ap.add_argument("--plain-digits", type=int, default=1_000_000,
                     help="size at which the plain per-product form is timed beside the chosen form")
     ap.add_argument("--ref-sample", type=int, default=10_000_000)
+    ap.add_argument("--ref-calibration", type=int, default=100_000_000,
+                    help="size of the reference arm's measured calibration run")
+    ap.add_argument("--no-isolated", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
@@ -133,14 +145,19 @@ def run_reference_pi(digits: int, threads: int) -> float:
     return float(json.loads(r.stderr.strip().splitlines()[-1])["pi_s"])
 
 
-def cpu_reference_estimate(target_digits: int, sample: int, threads: int):
-    """Reference CPU time at `sample` digits and a scaled estimate for the
-    target, exponent fitted between sample/10 and sample."""
-    t_small = run_reference_pi(sample // 10, threads)
-    t_big = run_reference_pi(sample, threads)
-    expo = math.log10(max(t_big, 1e-6) / max(t_small, 1e-6))
-    est = t_big * (target_digits / sample) ** expo
-    return est, t_big, t_small, expo
+def golden_pi():
+    return json.load(open(os.path.join(ROOT, "tests", "golden", "reference_golden.json")))["pi"]
+
+
+def reference_ratio(hi: int, lo: int):
+    """t(hi) / t(lo) of two whole reference runs at the same thread count,
+    measured when the golden fixtures were generated (None if either is
+    missing)."""
+    g = golden_pi()
+    a, b = g.get(str(hi)), g.get(str(lo))
+    if not a or not b or "ref_seconds" not in a or "ref_seconds" not in b or a.get("threads") != b.get("threads"):
+        return None
+    return a["ref_seconds"] / b["ref_seconds"], a["threads"], a["ref_seconds"], b["ref_seconds"]
 
 
 def max_over_ranks(values, dist=None, device="cpu"):
@@ -165,29 +182,64 @@ def reference_arm(args):
                           "oracle/_ref/picref_pi was not built (reference sources absent at build time)"}))
         return
     threads = os.cpu_count() or 1
-    sample = args.ref_sample
-    t_small = run_reference_pi(sample // 10, threads)  # calibration for the scaling exponent
-    times = []
+    sample, calib = args.ref_sample, args.ref_calibration
+    ratio = reference_ratio(args.digits, calib)
+    times, t_calib = [], None
     for i in range(args.warmup + args.steps):
+        if i == 0 and ratio is not None and calib != args.digits:
+            t_calib = run_reference_pi(calib, threads)  # warm-up 0: the measured calibration run
+            continue
         t = run_reference_pi(sample, threads)
         if i >= args.warmup:
             times.append(t)
-    t_big = statistics.mean(times)
-    expo = math.log10(t_big / t_small)
-    value = t_big * (args.digits / sample) ** expo
+    t_step = statistics.mean(times)
+    if t_calib is not None:
+        # value = t(calib) on this host x t_ref(digits) / t_ref(calib)
+        value = t_calib * ratio[0]
+        basis = (f"reference Pi() measured here at {calib} digits ({t_calib:.1f} s, {threads} threads) x "
+                 f"{ratio[0]:.2f}, the ratio of the reference's own {args.digits}- and {calib}-digit runs "
+                 f"({ratio[2]:.0f} s / {ratio[3]:.1f} s at {ratio[1]} threads, golden fixtures); timed steps "
+                 f"are {sample}-digit runs ({t_step:.2f} s mean)")
+    else:
+        value = t_step * (args.digits / sample)
+        basis = f"reference Pi() at {sample} digits per step, scaled linearly to {args.digits} digits"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_big * 1000.0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1000.0,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic", "config": {"workload": f"pi_{args.digits:.0e}_digits", "digits": args.digits,
                                         "parallelism": "replicas"},
+        "measured": {f"pi_{sample:.0e}_s": t_step, f"pi_{calib:.0e}_s": t_calib, "threads": threads},
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference",
-                         "sample": f"reference Pi() at {sample} digits per step ({t_big:.2f} s mean), "
-                                   f"scaled to {args.digits} digits with exponent {expo:.3f} fitted "
-                                   f"against {sample // 10} digits ({t_small:.2f} s)"},
+                         "sample": basis},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def replica_check(args):
+    """The multi-process launcher's self-test: every rank joins a gloo group
+    on 127.0.0.1, times a fixed amount of host work and rank 0 prints the
+    bench line with n_gpus = the number of ranks and the max over ranks."""
+    import datetime
+
+    import torch.distributed as dist
+    rank, _, world = rank_info()
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    t0 = time.perf_counter()
+    acc = 0
+    for i in range(200_000 * (rank + 1)):
+        acc += i * i
+    dt = time.perf_counter() - t0
+    (worst,) = max_over_ranks([dt], dist if world > 1 else None)
+    if rank == 0:
+        print(json.dumps({"impl": "replica-check", "metric": METRIC, "value": worst, "unit": "s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "per_rank_max_of": world}))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def int_roof(P, torch, L, stream):
@@ -264,6 +316,61 @@ def batched_products(P, torch, L, stream, count: int = 8192, top: int = 8192, se
     return {"products": count, "sizes": "log-uniform 1..8192 limbs, splitmix64 seed 7",
             "batched_ms": batched, "one_launch_sequence_per_product_ms": single,
             "speedup": single / batched}
+
+
+def isolated_products(P, torch, L, stream):
+    """The isolated-multiply workload: two N-limb operands (splitmix64 seeds 42
+    and 43), N = 2^12 ... 2^27, exact three-prime NTT product through pic_mul
+    (inputs resident in HBM), its words checked against the reference's md5;
+    where a proven FP64 piece width exists, the FFT product's time and its
+    largest rounding distance.  B_mul = bytes of the transforms (two forward,
+    one inverse; 16 B per point and pass, three primes) + 4 (na + nb + nz)."""
+    import hashlib
+
+    import numpy as np
+
+    from oracle.ffi import random_words
+    gold = {r["log2n"]: r for r in json.load(open(os.path.join(
+        ROOT, "tests", "golden", "reference_golden.json")))["products"]["isolated"]}
+    out = []
+    for lg in (12, 16, 20, 24, 27):
+        n = 1 << lg
+        a = torch.from_numpy(random_words(42, n).view(np.int32)).cuda()
+        b = torch.from_numpy(random_words(43, n).view(np.int32)).cuda()
+        z = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+        rec = {"log2n": lg}
+        for mode in ("ntt3", "fft"):
+            if mode == "fft" and lg > 20:
+                continue
+            P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, mode)
+            torch.cuda.synchronize()
+            reps = 20 if lg <= 20 else 3
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, mode)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            w = z.cpu().numpy().view(np.uint32)
+            L_ = w.size - (1 if w[-1] == 0 else 0)
+            ok = hashlib.md5(w[:L_].tobytes()).hexdigest() == gold[lg]["md5"] if lg in gold else None
+            rec[mode] = {"ms": ms, "matches_reference": ok}
+            if mode == "ntt3":
+                pieces = 2 * (n // 2) - 1
+                k = max(1, (pieces - 1).bit_length())
+                # passes of the tuned geometry: one up to 2^13 points, else
+                # ceil((k - row bits) / 11) column passes and the row pass
+                passes = 1 if k <= 13 else 1 + -(-(k - P.get_ntt_geometry(k)[0]) // 11)
+                b_mul = 3 * 3 * passes * 16.0 * (1 << k) + 4.0 * 4 * n
+                rec[mode]["B_mul_GB"] = b_mul / 1e9
+                rec[mode]["GBps"] = b_mul / (ms * 1e-3) / 1e9
+            else:
+                rec[mode]["max_err"] = L.pic_fft_last_max_err()
+        out.append(rec)
+        del a, b, z
+    torch.cuda.empty_cache()
+    return out
 
 
 # ----------------------------------------------------------------- our arm ----
@@ -344,6 +451,14 @@ def ours(args):
     f1.synchronize()
     e2e_s = f0.elapsed_time(f1) / 1000.0 / args.steps
     text_head = bytes(host[:32].tolist()).decode(errors="replace")
+    # after the timed region: the text of the last step against the reference's pi.txt
+    digits_check = None
+    if rank == 0:
+        import hashlib
+        md5 = hashlib.md5(host[: outlen.value].numpy().tobytes()).hexdigest()
+        g = golden_pi().get(str(args.digits))
+        digits_check = {"md5": md5, "reference_md5": g["md5"] if g else None,
+                        "matches_reference": (md5 == g["md5"]) if g else None}
 
     # max over ranks
     dev_s, e2e_s = max_over_ranks([dev_s, e2e_s], dist, device="cuda")
@@ -396,23 +511,55 @@ def ours(args):
         c_wall, c_dev, c_l = one(P.PI_CHOSEN)
         p_wall, p_dev, p_l = one(P.PI_PLAIN)
         plain = {"digits": args.plain_digits, "chosen_s": c_wall, "plain_s": p_wall,
-                 "speedup": p_wall / c_wall, "chosen_launches": c_l, "plain_launches": p_l}
+                 "speedup": p_wall / c_wall, "chosen_launches": c_l, "plain_launches": p_l,
+                 "plain_form": "the reference's recursion node by node, every product one three-prime NTT "
+                               "launch sequence (pic_mul, NTT3), leaves by scalar multiplies"}
 
     batch = None
     if not args.no_batch and rank == 0:
         batch = batched_products(P, torch, L, stream)
 
+    iso = None
+    if not args.no_isolated and rank == 0:
+        iso = isolated_products(P, torch, L, stream)
+
+    # the GPU's time at 10^8 digits, beside the reference arm's measured 10^8 run
+    pi_1e8 = None
+    if rank == 0 and args.digits > 100_000_000:
+        h = C.c_void_p()
+        st2 = P.PiStats()
+        for _ in range(2):
+            P.check(L.pic_pi_compute(100_000_000, P.PI_CHOSEN, C.byref(h), C.byref(st2)))
+            L.pic_bf_free(h)
+        pi_1e8 = st2.seconds_total
+
     cpu = None
+    like = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         from oracle.ffi import REF_PI
+        sample = min(args.ref_sample, args.digits)
+        ratio = reference_ratio(args.digits, sample)
         if os.path.exists(REF_PI):
             threads = os.cpu_count() or 1
-            sample = min(args.ref_sample, args.digits)
-            est, t_big, t_small, expo = cpu_reference_estimate(args.digits, sample, threads)
-            cpu = {"value": est, "unit": "s", "cores": threads, "kind": "reference",
-                   "sample": f"reference Pi() at {sample} digits ({t_big:.2f} s), scaled to {args.digits} "
-                             f"digits with exponent {expo:.3f} fitted against {sample // 10} digits "
-                             f"({t_small:.2f} s)"}
+            t_ref = run_reference_pi(sample, threads)
+            # the GPU's own time on the same sample, for a measured ratio
+            h = C.c_void_p()
+            st2 = P.PiStats()
+            P.check(L.pic_pi_compute(sample, P.PI_CHOSEN, C.byref(h), C.byref(st2)))
+            L.pic_bf_free(h)
+            P.check(L.pic_pi_compute(sample, P.PI_CHOSEN, C.byref(h), C.byref(st2)))
+            L.pic_bf_free(h)
+            like = {"digits": sample, "reference_s": t_ref, "reference_threads": threads,
+                    "gpu_s": st2.seconds_total, "ratio": t_ref / st2.seconds_total}
+            if ratio is not None:
+                est = t_ref * ratio[0]
+                basis = (f"reference Pi() measured here at {sample} digits ({t_ref:.2f} s) x {ratio[0]:.1f}, "
+                         f"the ratio of the reference's own {args.digits}- and {sample}-digit runs "
+                         f"({ratio[2]:.0f} s / {ratio[3]:.1f} s at {ratio[1]} threads, golden fixtures)")
+            else:
+                est = t_ref * args.digits / sample
+                basis = f"reference Pi() measured here at {sample} digits, scaled linearly"
+            cpu = {"value": est, "unit": "s", "cores": threads, "kind": "reference", "sample": basis}
 
     if rank == 0:
         mean_phase = {k: statistics.mean(p[k] for p in phases)
@@ -430,13 +577,17 @@ def ours(args):
                        "l2": "working set larger than L2 (126 MB) in the dominant products"},
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(outlen.value), "text_head": text_head},
+            "digits_check": digits_check,
             "gpu_launches": int(launches),
             "roofline": roofline,
             "int_roofline": int_roofline,
             "cpu_baseline": cpu,
+            "measured_vs_reference": like,
+            "pi_1e8_s": pi_1e8,
             "clocks": clk,
             "plain_vs_chosen": plain,
             "batched_products": batch,
+            "isolated_products": iso,
             "phases": mean_phase,
             "kernels": kstats,
         }
@@ -446,10 +597,29 @@ def ours(args):
         dist.destroy_process_group()
 
 
+def relaunch(args) -> int:
+    """--gpus N > 1 outside torchrun: N replicas under torch.distributed.run
+    on 127.0.0.1, each rank on its own GPU; rank 0 prints the line."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch(args))
+    _, _, world = rank_info()
+    if args.gpus != world:
+        raise SystemExit(f"--gpus {args.gpus} but {world} ranks were launched")
     if args.impl == "reference":
         reference_arm(args)
+    elif args.impl == "replica-check":
+        replica_check(args)
     else:
         ours(args)
 

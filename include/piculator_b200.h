@@ -206,7 +206,8 @@ pic_status pic_transform_free(pic_transform t);                    /* deleteNTT,
 /* ---- Pi (PI.h:138-212) ---------------------------------------------------- */
 enum {
     PIC_PI_CHOSEN = 0, /* batched binary-splitting levels + tuned products */
-    PIC_PI_PLAIN = 1   /* one BigFloat::mul per product, reference-layout NTT */
+    PIC_PI_PLAIN = 1   /* one BigFloat::mul per product, each its own three-prime
+                          NTT launch sequence (no batching, no schoolbook) */
 };
 typedef struct {
     uint64_t hex_digits;   /* PI.h:141 */

@@ -2,7 +2,8 @@
 //
 // Two forms:
 //  * plain  (PIC_PI_PLAIN): the reference's recursion node by node, every
-//    product one reference-layout NTT multiply (launch sequence per product);
+//    product one three-prime NTT multiply (its own launch sequence, no
+//    batching across products, no schoolbook);
 //  * chosen (PIC_PI_CHOSEN): the lower binary-splitting levels evaluated level
 //    by level in batched launches (bsr.cu), the upper levels and the Newton
 //    phases through the tuned multiply.
@@ -101,7 +102,7 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
     const uint64_t recompute0 = ctx().fft_recomputes.load();
     fft_reset_max_err();
     const int saved_mode = get_mul_mode();
-    set_mul_mode(mode == PIC_PI_PLAIN ? PIC_MUL_NTT_REF : PIC_MUL_AUTO);
+    set_mul_mode(mode == PIC_PI_PLAIN ? PIC_MUL_NTT3 : PIC_MUL_AUTO);
     // the chosen form peaks below 512 bytes per word of precision (merge
     // batches of at most 256, live nodes and the top levels' workspace);
     // hold that much in the pool before the first merge

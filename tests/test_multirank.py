@@ -45,3 +45,32 @@ def test_max_over_ranks_gloo():
 def test_max_over_ranks_single_process_is_identity():
     import bench
     assert bench.max_over_ranks([3.0, 4.0]) == [3.0, 4.0]
+
+
+@pytest.mark.parametrize("n", [2, 3])
+def test_bench_gpus_flag_launches_n_replicas(n):
+    """`bench.py --gpus N` outside torchrun re-launches itself as N ranks
+    (torch.distributed.run on 127.0.0.1); with the launcher's self-test arm
+    (gloo, no GPU) rank 0 prints one line whose n_gpus is N."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", str(n), "--impl",
+                        "replica-check", "--steps", "1", "--warmup", "0"],
+                       capture_output=True, text=True, timeout=240, env=env, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    assert lines[0]["n_gpus"] == n and lines[0]["per_rank_max_of"] == n
+
+
+def test_bench_rejects_rank_count_mismatch():
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--impl",
+                        "replica-check"], capture_output=True, text=True, timeout=120, env=env, cwd=root)
+    assert r.returncode != 0 and "ranks were launched" in r.stderr
