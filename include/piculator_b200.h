@@ -36,7 +36,8 @@ typedef enum {
     PIC_ERR_NO_MEMORY = 6,       /* device or pinned-host allocation failed */
     PIC_ERR_NOT_INITIALIZED = 7, /* pic_init has not succeeded */
     PIC_ERR_IO = 8,              /* "Cannot Create File" PI.h:42 */
-    PIC_ERR_TIMEOUT = 9          /* a bounded device-side wait gave up */
+    PIC_ERR_TIMEOUT = 9,         /* a bounded device-side wait gave up */
+    PIC_ERR_STOPPED = 10         /* stopped by pic_debug_stop_after_phase (checkpoint tests) */
 } pic_status;
 
 typedef void* pic_stream; /* a cudaStream_t */
@@ -235,6 +236,26 @@ pic_status pic_pi_hex(uint64_t decimal_digits, int mode, char* out, size_t cap,
  * handle (free it with pic_bf_free; pic_bf_to_hex gives the text). */
 pic_status pic_pi_compute(uint64_t decimal_digits, int mode, pic_bf* out,
                           pic_pi_stats* stats);
+
+/* Checkpoint / resume.  No reference counterpart: the reference keeps its
+ * state in RAM only (PI.h:165-166) and a failed run starts over.  With a
+ * directory set, pic_pi_hex / pic_pi_compute write <dir>/pi_<digits>.ckpt at
+ * the end of each phase of Pi() -- 1: binary splitting and the combination
+ * of PI.h:179-181 (P, Q), 2: the division of PI.h:189 (P), 3: the inverse
+ * square root of PI.h:194 (P, Q) -- replacing the previous file only once the
+ * new one is complete; with PIC_CKPT_RESUME a computation of the same digit
+ * count starts after the newest phase found there.  A file that fails its
+ * checks is reported (PIC_ERR_IO), never used.  dir = NULL turns it off. */
+enum { PIC_CKPT_WRITE = 1, PIC_CKPT_RESUME = 2 };
+pic_status pic_pi_set_checkpoint(const char* dir, int flags);
+/* Reads a checkpoint file on the host (no GPU needed): its digit count,
+ * working precision and phase; verify != 0 also checks every stored number
+ * against its hash.  PIC_ERR_IO if it is not a valid checkpoint. */
+pic_status pic_checkpoint_inspect(const char* path, uint64_t* digits, uint64_t* p_words,
+                                  uint32_t* phase, int verify);
+/* Test hook: after writing the checkpoint of `phase` (1..3), the computation
+ * stops with PIC_ERR_STOPPED, as a crash right after it would (0 = never). */
+void pic_debug_stop_after_phase(int phase);
 
 /* Binary splitting over [a, b) at precision p (Pi_BSR, PI.h:64-136): the
  * batched form (PIC_PI_CHOSEN) or the node-by-node recursion (PIC_PI_PLAIN).

@@ -24,7 +24,9 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "piculator_b200.h")
 
 # pic_status (include/piculator_b200.h)
 OK, ERR_INVALID, ERR_LENGTH, ERR_DIVIDE_BY_ZERO, ERR_LIMIT, ERR_CUDA, ERR_NO_MEMORY, \
-    ERR_NOT_INITIALIZED, ERR_IO, ERR_TIMEOUT = range(10)
+    ERR_NOT_INITIALIZED, ERR_IO, ERR_TIMEOUT, ERR_STOPPED = range(11)
+# checkpoint flags (pic_pi_set_checkpoint)
+CKPT_WRITE, CKPT_RESUME = 1, 2
 # product modes
 MUL_AUTO, MUL_NTT_REF, MUL_NTT3, MUL_FFT, MUL_SCHOOL = range(5)
 MUL_MODES = {"auto": MUL_AUTO, "ntt_ref": MUL_NTT_REF, "ntt3": MUL_NTT3, "fft": MUL_FFT,
@@ -78,6 +80,10 @@ _SIGS = {
     "pic_device_bytes_in_use": ([], C.c_uint64),
     "pic_debug_fail_allocations": ([C.c_int], None),
     "pic_debug_allocation_count": ([], C.c_uint64),
+    "pic_pi_set_checkpoint": ([C.c_char_p, C.c_int], C.c_int),
+    "pic_checkpoint_inspect": ([C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                C.POINTER(C.c_uint32), C.c_int], C.c_int),
+    "pic_debug_stop_after_phase": ([C.c_int], None),
     "pic_default_stream": ([], C.c_void_p),
     "pic_profile_begin": ([], C.c_int),
     "pic_profile_end": ([C.POINTER(KernelStat), C.c_int, C.POINTER(C.c_int)], C.c_int),
@@ -397,3 +403,16 @@ def pi_hex(digits: int, form: int = PI_CHOSEN, want_text: bool = True):
         return buf.raw[: n.value], st.as_dict()
     check(lib().pic_pi_hex(digits, form, None, 0, None, C.byref(st)))
     return None, st.as_dict()
+
+
+def set_checkpoint(directory: str | None, flags: int = CKPT_WRITE | CKPT_RESUME) -> None:
+    """pic_pi_set_checkpoint: write / resume pi computations in `directory`
+    (None turns checkpoints off)."""
+    check(lib().pic_pi_set_checkpoint(directory.encode() if directory else None, flags if directory else 0))
+
+
+def checkpoint_inspect(path: str, verify: bool = True) -> dict:
+    """Header of a checkpoint file (host only): digits, p_words, phase."""
+    d, pw, ph = C.c_uint64(), C.c_uint64(), C.c_uint32()
+    check(lib().pic_checkpoint_inspect(path.encode(), C.byref(d), C.byref(pw), C.byref(ph), int(verify)))
+    return {"digits": d.value, "p_words": pw.value, "phase": ph.value}

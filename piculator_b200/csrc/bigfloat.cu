@@ -308,7 +308,12 @@ BigFloat invsqrt(uint32_t x, size_t p, int threads)
     if (p == 2) s = 1;
     BigFloat T = invsqrt(x, s, threads);
     BigFloat temp = T.mul(T, p, threads);        // r0^2
-    temp = temp.mul(BigFloat(x), 0, threads);    // r0^2 * x (a full product, p = 0)
+    // r0^2 * x: the reference forms it as temp.mul(BigFloat(x), 0), an exact
+    // product with a one-word operand (BigFloat.cpp:562).  mul(uint32) gives
+    // the same words, length, sign and exponent (BigFloat.cpp:156-183: exact
+    // product, one carry word kept only when nonzero, as mul drops one zero
+    // top word, :411-412) with one linear pass instead of three transforms.
+    temp = temp.mul(x);
     temp = temp.sub(BigFloat(1), p);             // r0^2 * x - 1
     temp = temp.mul(2147483648u);                // (r0^2 * x - 1) / 2
     temp.exp--;

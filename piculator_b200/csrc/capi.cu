@@ -12,6 +12,7 @@
 #include "mul.cuh"
 #include "ntt.cuh"
 #include "bsr.cuh"
+#include "checkpoint.cuh"
 #include "pi.cuh"
 #include "transform.cuh"
 
@@ -97,6 +98,7 @@ const char* pic_status_string(pic_status s)
     case PIC_ERR_NOT_INITIALIZED: return "not initialised";
     case PIC_ERR_IO: return "Cannot Create File";
     case PIC_ERR_TIMEOUT: return "device wait timed out";
+    case PIC_ERR_STOPPED: return "stopped after a checkpoint";
     }
     return "unknown status";
 }
@@ -631,6 +633,25 @@ pic_status pic_pi_compute(uint64_t decimal_digits, int mode, pic_bf* out, pic_pi
         if (stats) *stats = local;
     });
 }
+
+pic_status pic_pi_set_checkpoint(const char* dir, int flags)
+{
+    return guarded([&] {
+        PIC_REQUIRE((flags & ~(PIC_CKPT_WRITE | PIC_CKPT_RESUME)) == 0, PIC_ERR_INVALID, "unknown checkpoint flags");
+        checkpoint_configure(dir, flags);
+    });
+}
+
+pic_status pic_checkpoint_inspect(const char* path, uint64_t* digits, uint64_t* p_words, uint32_t* phase, int verify)
+{
+    return guarded([&] {
+        PIC_REQ_PTR(path);
+        if (checkpoint_inspect_file(path, digits, p_words, phase, verify != 0, nullptr) != 0)
+            throw Error(PIC_ERR_IO, std::string("checkpoint ") + path + ": cannot open");
+    });
+}
+
+void pic_debug_stop_after_phase(int phase) { checkpoint_debug_stop_after(phase); }
 
 pic_status pic_pi_hex(uint64_t decimal_digits, int mode, char* out, size_t cap, size_t* out_len,
                       pic_pi_stats* stats)

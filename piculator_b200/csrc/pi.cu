@@ -15,6 +15,7 @@
 
 #include "bigfloat.hpp"
 #include "bsr.cuh"
+#include "checkpoint.cuh"
 #include "common.cuh"
 #include "mul.cuh"
 #include "pi.cuh"
@@ -110,19 +111,31 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
     PhaseTimer tm;
     BigFloat P, Q, R;
     try {
+        // a resumed computation starts after the newest phase on disk; the
+        // phases it skips are timed as zero
+        const int done = checkpoint_resume(decimal_digits, p, &P, &Q);
         tm.mark();
-        if (mode == PIC_PI_PLAIN) bsr_recursive(P, Q, R, 0, (uint32_t)terms, (size_t)p);
-        else bsr_chosen(P, Q, R, 0, (uint32_t)terms, (size_t)p, /*need_root_R=*/false);
-        if (tracing()) {
-            PIC_CUDA(cudaStreamSynchronize(ctx().stream));
-            fprintf(stderr, "{\"trace\": \"bsr_done\"}\n");
+        if (done < 1) {
+            if (mode == PIC_PI_PLAIN) bsr_recursive(P, Q, R, 0, (uint32_t)terms, (size_t)p);
+            else bsr_chosen(P, Q, R, 0, (uint32_t)terms, (size_t)p, /*need_root_R=*/false);
+            if (tracing()) {
+                PIC_CUDA(cudaStreamSynchronize(ctx().stream));
+                fprintf(stderr, "{\"trace\": \"bsr_done\"}\n");
+            }
+            P = Q.mul(13591409u).add(P, (size_t)p);  // PI.h:180-181
+            Q = Q.mul(4270934400u);
+            checkpoint_save(1, decimal_digits, p, terms, &P, &Q);
         }
-        P = Q.mul(13591409u).add(P, (size_t)p);  // PI.h:180-181
-        Q = Q.mul(4270934400u);
         tm.mark();
-        P = Q.div(P, (size_t)p);                 // PI.h:189
+        if (done < 2) {
+            P = Q.div(P, (size_t)p);                 // PI.h:189
+            checkpoint_save(2, decimal_digits, p, terms, &P, nullptr);
+        }
         tm.mark();
-        Q = invsqrt(10005, (size_t)p);           // PI.h:194
+        if (done < 3) {
+            Q = invsqrt(10005, (size_t)p);           // PI.h:194
+            checkpoint_save(3, decimal_digits, p, terms, &P, &Q);
+        }
         tm.mark();
         P = P.mul(Q, (size_t)p);                 // PI.h:199
         tm.mark();
