@@ -183,6 +183,13 @@ pic_status pic_bf_from_u32(pic_bf* out, uint32_t x, int sign); /* BigFloat.cpp:6
 pic_status pic_bf_free(pic_bf x);
 pic_status pic_bf_info(pic_bf x, int* sign, int64_t* exp, size_t* L);
 pic_status pic_bf_to_words(pic_bf x, uint32_t* words_host, size_t cap);
+/* Device-to-device word copies, for callers that move numbers between GPUs
+ * themselves (the multi-GPU binary splitting sends them over NCCL).  dst and
+ * src are device pointers on the library's device; the copies are ordered on
+ * s after the library's pending work.  No reference counterpart. */
+pic_status pic_bf_to_device(pic_bf x, uint32_t* dst, size_t cap, pic_stream s);
+pic_status pic_bf_from_device(pic_bf* out, int sign, int64_t exp, const uint32_t* src,
+                              size_t L, pic_stream s);
 pic_status pic_bf_negate(pic_bf x);                                  /* :150 */
 pic_status pic_bf_mul_u32(pic_bf* out, pic_bf a, uint32_t x);        /* :156 */
 pic_status pic_bf_add(pic_bf* out, pic_bf a, pic_bf b, size_t p);    /* :288 */

@@ -115,6 +115,8 @@ _SIGS = {
     "pic_bf_info": ([C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_size_t)],
                     C.c_int),
     "pic_bf_to_words": ([C.c_void_p, _U32P, C.c_size_t], C.c_int),
+    "pic_bf_to_device": ([C.c_void_p, _U32P, C.c_size_t, _P], C.c_int),
+    "pic_bf_from_device": ([C.POINTER(C.c_void_p), C.c_int, C.c_int64, _U32P, C.c_size_t, _P], C.c_int),
     "pic_bf_negate": ([C.c_void_p], C.c_int),
     "pic_bf_mul_u32": ([C.POINTER(C.c_void_p), C.c_void_p, C.c_uint32], C.c_int),
     "pic_bf_add": ([C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p, C.c_size_t], C.c_int),

@@ -3,6 +3,11 @@
     python -m piculator_b200.cli pi  --digits 1e9 [--repeat 2] [--form chosen|plain] [--out pi.txt]
                                      [--tuning FILE]
     python -m piculator_b200.cli mul --words 8388608 [--mode ntt3] [--repeat 3]
+    torchrun --nproc-per-node N -m piculator_b200.cli pi --digits 1e9 --distributed
+
+`pi --distributed` (under torchrun, one process per GPU, NCCL) splits the
+binary splitting over the ranks (piculator_b200/shard.py); rank 0 prints the
+line and writes the text.
 
 `pi` runs the reference's Pi() (PI.h:138-212) on the GPU: it prints one JSON
 line of phase times per run and, with --out, writes the same pi.txt text the
@@ -50,6 +55,37 @@ def cmd_pi(args) -> None:
             f.write(text)
 
 
+def cmd_pi_distributed(args) -> None:
+    import datetime
+    import os
+
+    import torch
+    import torch.distributed as dist
+
+    from piculator_b200.shard import DeviceBackend, pi_distributed
+    digits = int(float(args.digits))
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        for r in range(args.repeat):
+            dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            text = pi_distributed(DeviceBackend(), dist, digits, P.pi_sizes)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            dist.barrier()
+            if dist.get_rank() == 0:
+                line = {"run": r, "digits": digits, "ranks": dist.get_world_size(), "wall_s": round(wall, 4)}
+                if args.md5:
+                    line["md5"] = hashlib.md5(text).hexdigest()
+                print(json.dumps(line), flush=True)
+                if args.out:
+                    with open(args.out, "wb") as f:
+                        f.write(text)
+    finally:
+        dist.destroy_process_group()
+
+
 def cmd_mul(args) -> None:
     import torch
 
@@ -80,15 +116,24 @@ def main() -> None:
     p.add_argument("--out", default=None, help="write the pi.txt text here")
     p.add_argument("--md5", action="store_true", help="print the md5 of the text")
     p.add_argument("--tuning", default=None, help="a tuning file applied over the default one")
+    p.add_argument("--distributed", action="store_true",
+                   help="split the binary splitting over the torchrun ranks (one GPU each)")
     m = sub.add_parser("mul", help="time an isolated product of two splitmix64 operands")
     m.add_argument("--words", default="8388608")
     m.add_argument("--mode", default="ntt3", choices=("auto", "school", "ntt3", "fft", "ntt_ref"))
     m.add_argument("--repeat", type=int, default=3)
     args = ap.parse_args()
-    P.init(0)
+    import os
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if getattr(args, "distributed", False):
+        import torch
+        torch.cuda.set_device(local)
+    P.init(local)
     if getattr(args, "tuning", None):
         P.apply_tuning(args.tuning)
-    if args.cmd == "pi":
+    if args.cmd == "pi" and args.distributed:
+        cmd_pi_distributed(args)
+    elif args.cmd == "pi":
         cmd_pi(args)
     else:
         cmd_mul(args)

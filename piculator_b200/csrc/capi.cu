@@ -396,6 +396,51 @@ pic_status pic_bf_to_words(pic_bf x, uint32_t* words, size_t cap)
     });
 }
 
+// Orders `to` after all work queued so far on `from` (no host wait).
+static void stream_after(cudaStream_t to, cudaStream_t from)
+{
+    if (to == from) return;
+    cudaEvent_t e;
+    PIC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    PIC_CUDA(cudaEventRecord(e, from));
+    PIC_CUDA(cudaStreamWaitEvent(to, e, 0));
+    PIC_CUDA(cudaEventDestroy(e));
+}
+
+pic_status pic_bf_to_device(pic_bf x, uint32_t* dst, size_t cap, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(x);
+        const size_t L = x->v.get_precision();
+        PIC_REQUIRE(cap >= L, PIC_ERR_INVALID, "capacity too small");
+        PIC_REQUIRE(L == 0 || dst, PIC_ERR_INVALID, "dst is NULL");
+        if (!L) return;
+        const cudaStream_t cs = resolve(s);
+        stream_after(cs, ctx().stream);  // the words are written on the library's stream
+        PIC_CUDA(cudaMemcpyAsync(dst, x->v.device_words(), L * sizeof(uint32_t), cudaMemcpyDeviceToDevice, cs));
+        stream_after(ctx().stream, cs);  // later library work may not free the words before the copy
+    });
+}
+
+pic_status pic_bf_from_device(pic_bf* out, int sign, int64_t exp, const uint32_t* src, size_t L, pic_stream s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(out);
+        PIC_REQUIRE(L == 0 || src, PIC_ERR_INVALID, "src is NULL");
+        if (L == 0) {
+            *out = wrap(BigFloat());
+            return;
+        }
+        auto st = alloc_words(L);
+        stream_after(ctx().stream, resolve(s));  // src is complete on the caller's stream
+        PIC_CUDA(cudaMemcpyAsync(st->base, src, L * sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx().stream));
+        stream_after(resolve(s), ctx().stream);  // the caller may reuse src after this point on s
+        *out = wrap(BigFloat::from_device(sign != 0, exp, st, st->base, L));
+    });
+}
+
 pic_status pic_bf_negate(pic_bf x)
 {
     return guarded([&] {
@@ -550,7 +595,7 @@ pic_status pic_bsr(uint32_t a, uint32_t b, size_t p, int mode, pic_bf* P, pic_bf
         PIC_REQUIRE(b > a, PIC_ERR_INVALID, "empty range");
         PIC_REQUIRE(mode == PIC_PI_CHOSEN || mode == PIC_PI_PLAIN, PIC_ERR_INVALID, "unknown mode");
         BigFloat p_, q_, r_;
-        with_mode(mode == PIC_PI_PLAIN ? PIC_MUL_NTT_REF : PIC_MUL_AUTO, [&] {
+        with_mode(mode == PIC_PI_PLAIN ? PIC_MUL_NTT3 : PIC_MUL_AUTO, [&] {
             if (mode == PIC_PI_PLAIN) bsr_recursive(p_, q_, r_, a, b, p);
             else bsr_chosen(p_, q_, r_, a, b, p);
         });
