@@ -200,6 +200,10 @@ pic_status pic_bf_div(pic_bf* out, pic_bf a, pic_bf b, size_t p, int mode); /* :
 pic_status pic_bf_invsqrt(pic_bf* out, uint32_t x, size_t p, int mode); /* :516 */
 int pic_bf_ucmp(pic_bf a, pic_bf b);                                  /* :123 */
 pic_status pic_bf_to_hex(pic_bf x, size_t digits, char* buf, size_t cap); /* :95 */
+/* to_string_dec (BigFloat.cpp:83): the top word in decimal, '.', then the
+ * first `digits` decimal digits of the fraction below it -- the reference's
+ * text exactly, computed in O(M(n) log n) instead of its O(n^2) loop. */
+pic_status pic_bf_to_dec(pic_bf x, size_t digits, char* buf, size_t cap); /* :83 */
 
 /* ---- Transform.h:5-33 -- transform-domain operands ----------------------- */
 /* A pic_transform holds one operand's forward transform (three-prime form)

@@ -127,6 +127,7 @@ _SIGS = {
     "pic_bf_invsqrt": ([C.POINTER(C.c_void_p), C.c_uint32, C.c_size_t, C.c_int], C.c_int),
     "pic_bf_ucmp": ([C.c_void_p, C.c_void_p], C.c_int),
     "pic_bf_to_hex": ([C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t], C.c_int),
+    "pic_bf_to_dec": ([C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t], C.c_int),
     "pic_transform_create": ([C.POINTER(C.c_void_p), C.c_void_p, C.c_size_t, C.c_int], C.c_int),
     "pic_transform_mul": ([C.c_void_p, C.c_void_p], C.c_int),
     "pic_transform_to_bf": ([C.POINTER(C.c_void_p), C.c_void_p], C.c_int),
@@ -324,6 +325,12 @@ class DeviceBigFloat:
     def to_hex(self, digits: int) -> bytes:
         buf = C.create_string_buffer(digits + 32)
         check(lib().pic_bf_to_hex(self.h, digits, buf, digits + 32))
+        return buf.value
+
+    def to_dec(self, digits: int) -> bytes:
+        """to_string_dec (BigFloat.cpp:83-94)."""
+        buf = C.create_string_buffer(digits + 32)
+        check(lib().pic_bf_to_dec(self.h, digits, buf, digits + 32))
         return buf.value
 
 

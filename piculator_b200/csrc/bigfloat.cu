@@ -5,6 +5,7 @@
 #include <sstream>
 
 #include "bigfloat.hpp"
+#include "radix.cuh"
 #include "linear.cuh"
 #include "mul.cuh"
 
@@ -373,21 +374,11 @@ std::string BigFloat::to_string_hex(size_t digits) const
 
 std::string BigFloat::to_string_dec(size_t digits) const
 {
-    // BigFloat.cpp:83-94: repeatedly clear the top word and multiply by 10^9.
-    std::vector<uint32_t> w = words();
-    std::stringstream s;
-    s << w[L - 1] << '.';
-    BigFloat temp = *this;
-    for (size_t i = 0; i < (digits + 8) / 9; i++) {
-        std::vector<uint32_t> t = temp.words();
-        t[temp.L - 1] = 0;
-        temp = from_host(temp.sign, temp.exp, t.data(), temp.L);
-        temp = temp.mul(1000000000u);
-        char buf[16];
-        snprintf(buf, sizeof buf, "%09u", temp.word_at(temp.exp + (int64_t)temp.L - 1));
-        s << buf;
-    }
-    return s.str().substr(0, 2 + digits);
+    // BigFloat.cpp:83-94 prints the fraction below the top word nine digits at
+    // a time by clearing the top word and multiplying by 10^9 (O(n^2)); the
+    // same digits come from one exact product and a divide-and-conquer split
+    // by powers of 10^9 (radix.cu).
+    return to_string_dec_fast(*this, digits);
 }
 
 }  // namespace pic

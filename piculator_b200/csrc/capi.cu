@@ -441,6 +441,18 @@ pic_status pic_bf_from_device(pic_bf* out, int sign, int64_t exp, const uint32_t
     });
 }
 
+pic_status pic_bf_to_dec(pic_bf x, size_t digits, char* buf, size_t cap)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(x);
+        PIC_REQ_PTR(buf);
+        const std::string s = x->v.to_string_dec(digits);
+        PIC_REQUIRE(s.size() + 1 <= cap, PIC_ERR_INVALID, "buffer too small");
+        memcpy(buf, s.c_str(), s.size() + 1);
+    });
+}
+
 pic_status pic_bf_negate(pic_bf x)
 {
     return guarded([&] {

@@ -19,7 +19,13 @@ this time are kept.
 
 only adds the isolated products of 2^24 and 2^27 words (the reference's NTT
 at k = 27 and k = 30; about 26 GB of host memory and several minutes for
-2^27) to the existing file, leaving every other entry as it is.
+2^27) to the existing file, leaving every other entry as it is;
+
+    python tests/golden/make_golden.py --dec
+
+only adds the decimal-output fixtures: BigFloat::to_string_dec
+(BigFloat.cpp:83-94) of splitmix64 numbers and edge cases, and of Pi()'s
+final number at 10^4 .. 10^6 digits (oracle/_ref/picref_dec).
 """
 from __future__ import annotations
 
@@ -39,6 +45,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from oracle.ffi import REF_PI, BF, Reference, random_words, splitmix64_np  # noqa: E402
+
+REF_DEC = os.path.join(os.path.dirname(REF_PI), "picref_dec")
 
 
 def md5(b: bytes) -> str:
@@ -133,6 +141,53 @@ def gen_big_products(ref: Reference) -> list:
     return out
 
 
+def ref_dec_words(sign: bool, exp: int, words: np.ndarray, digits: int) -> bytes:
+    """to_string_dec(digits) of a BigFloat, by the reference program."""
+    with tempfile.NamedTemporaryFile(suffix=".bf", delete=False) as f:
+        f.write(np.array([1 if sign else 0], dtype="<i4").tobytes())
+        f.write(np.array([exp], dtype="<i8").tobytes())
+        f.write(np.array([words.size], dtype="<u8").tobytes())
+        f.write(np.ascontiguousarray(words, dtype="<u4").tobytes())
+        path = f.name
+    try:
+        return subprocess.run([REF_DEC, "words", path, str(digits)], capture_output=True, check=True).stdout
+    finally:
+        os.unlink(path)
+
+
+def gen_dec() -> dict:
+    """BigFloat::to_string_dec (BigFloat.cpp:83-94): the text for seeded and
+    edge-case numbers, and md5 / head / tail for Pi()'s number."""
+    cases = []
+    specs = [(5, 0), (5, 1), (5, 8), (5, 9), (5, 10), (5, 100), (1, 30), (2, 9), (3, 50), (40, 300),
+             (200, 1900), (1000, 9000), (2500, 25000), (20000, 190000)]
+    for i, (L, digits) in enumerate(specs):
+        w = random_words(7000 + i, L)
+        w[-1] = (w[-1] % 7) + 1 if i % 3 else w[-1]  # one-char and multi-char integer parts
+        text = ref_dec_words(True, -L + 1, w, digits)
+        rec = {"seed": 7000 + i, "L": L, "digits": digits, "top_mod7": bool(i % 3)}
+        if len(text) <= 4000:
+            rec["text"] = text.decode()
+        rec["md5"] = md5(text)
+        rec["len"] = len(text)
+        cases.append(rec)
+    edge = []
+    for name, w in [("ones", np.full(300, 0xFFFFFFFF, dtype=np.uint32)),
+                    ("zeros_below_top", np.array([0] * 299 + [3], dtype=np.uint32)),
+                    ("single_low_bit", np.array([1] + [0] * 298 + [3], dtype=np.uint32))]:
+        text = ref_dec_words(True, 0, w, 3000)
+        edge.append({"kind": name, "digits": 3000, "md5": md5(text), "len": len(text), "tail": text[-60:].decode()})
+    pi = {}
+    for d in (10_000, 100_000, 1_000_000):
+        t0 = time.time()
+        text = subprocess.run([REF_DEC, "pi", str(d), str(os.cpu_count() or 1)], capture_output=True,
+                              check=True).stdout
+        pi[str(d)] = {"md5": md5(text), "len": len(text), "head": text[:80].decode(), "tail": text[-80:].decode(),
+                      "ref_seconds": round(time.time() - t0, 2)}
+        print(f"pi dec {d}: {pi[str(d)]['md5']} ({pi[str(d)]['ref_seconds']} s)", flush=True)
+    return {"numbers": cases, "edge": edge, "pi": pi}
+
+
 def gen_ntt(ref: Reference) -> dict:
     """NNT::NTT / iNTT (NTT.cpp:74-84) outputs at k = 11..16."""
     out = []
@@ -195,9 +250,16 @@ def main():
     ap.add_argument("--odd", action="store_true", help="also pi at 3,141,593 and 27,182,818 digits")
     ap.add_argument("--big-products", action="store_true",
                     help="only add the 2^24- and 2^27-word products to the existing file")
+    ap.add_argument("--dec", action="store_true", help="only add the decimal-output fixtures")
     args = ap.parse_args()
     ref = Reference()
     path = os.path.join(HERE, "reference_golden.json")
+    if args.dec:
+        fixtures = json.load(open(path))
+        fixtures["dec"] = gen_dec()
+        json.dump(fixtures, open(path, "w"), indent=1, sort_keys=True)
+        print("wrote", path)
+        return
     if args.big_products:
         fixtures = json.load(open(path))
         big = gen_big_products(ref)
@@ -219,6 +281,8 @@ def main():
             fixtures["pi"].setdefault(d, v)
         fixtures["products"]["isolated"] += [e for e in old["products"]["isolated"]
                                              if e["log2n"] in (24, 27)]
+        if "dec" in old:
+            fixtures["dec"] = old["dec"]
     json.dump(fixtures, open(path, "w"), indent=1, sort_keys=True)
     print("wrote", path)
 
