@@ -523,6 +523,26 @@ def ours(args):
     if not args.no_isolated and rank == 0:
         iso = isolated_products(P, torch, L, stream)
 
+    # the two product forms of the same computation, cross-checked: NTT only,
+    # and precision-selected (FP64 FFT for products up to 4 M words where its
+    # proven piece width allows, NTT recompute past a rounding distance of 0.25)
+    forms = None
+    if rank == 0:
+        import hashlib
+        saved = P.get_tuning(P.TUNE_MUL_FFT_MAX)
+        forms = {}
+        try:
+            for name, fmax in (("ntt_only", 0), ("precision_selected", 1 << 22)):
+                P.set_tuning(P.TUNE_MUL_FFT_MAX, fmax)
+                text, st2 = P.pi_hex(args.digits, form)
+                forms[name] = {"md5": hashlib.md5(text).hexdigest(), "seconds": st2["seconds_total"],
+                               "fft_max_err": st2["fft_max_err"], "fft_recomputes": st2["fft_recomputes"],
+                               "products": st2["products"]}
+                del text
+        finally:
+            P.set_tuning(P.TUNE_MUL_FFT_MAX, saved)
+        forms["equal"] = forms["ntt_only"]["md5"] == forms["precision_selected"]["md5"]
+
     # the GPU's time at 10^8 digits, beside the reference arm's measured 10^8 run
     pi_1e8 = None
     if rank == 0 and args.digits > 100_000_000:
@@ -588,6 +608,7 @@ def ours(args):
             "plain_vs_chosen": plain,
             "batched_products": batch,
             "isolated_products": iso,
+            "forms": forms,
             "phases": mean_phase,
             "kernels": kstats,
         }

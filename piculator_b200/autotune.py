@@ -117,20 +117,21 @@ def _timeline_ms_by_k(stderr: str) -> dict:
     return out
 
 
-def tune_ntt_batched(digits: int, ks=range(14, 28)) -> dict:
+def tune_ntt_batched(digits: int, ks=range(14, 28), radices=(3, 4)) -> dict:
     """NTT geometry per length, timed on the batched merges of whole pi runs:
     each candidate is applied to every length at once, the second of two runs
     is timed, and each length takes the candidate whose merge levels of that
     length were fastest (a level's wrapped tail product, usually two lengths
-    shorter, runs under the same candidate)."""
+    shorter, runs under the same candidate).  Radix 16 (radix_log2 4) applies
+    to the row passes of 2^11 .. 2^13 points; column passes stay radix 8."""
     import subprocess
     import sys
     import tempfile
-    cands = [(row, lw) for row in (11, 12, 13) for lw in (0, 3, 5)]
+    cands = [(row, lw, rb) for row in (11, 12, 13) for lw in (0, 3, 5) for rb in radices]
     ms: dict = {}
     env = dict(os.environ, PIC_TIMELINE="1")
-    for row, lw in cands:
-        tab = {"ntt": {str(k): {"row_bits": row, "col_width_log2": lw, "radix_log2": 3} for k in ks}}
+    for row, lw, rb in cands:
+        tab = {"ntt": {str(k): {"row_bits": row, "col_width_log2": lw, "radix_log2": rb} for k in ks}}
         with tempfile.NamedTemporaryFile("w", suffix=".json", delete=False) as f:
             json.dump(tab, f)
             path = f.name
@@ -141,15 +142,16 @@ def tune_ntt_batched(digits: int, ks=range(14, 28)) -> dict:
         finally:
             os.unlink(path)
         for k, v in _timeline_ms_by_k(r.stderr).items():
-            ms.setdefault(k, {})[(row, lw)] = v
-        print(f"ntt batched {row}/{lw}: { {k: round(v[(row, lw)], 2) for k, v in sorted(ms.items())} }", flush=True)
+            ms.setdefault(k, {})[(row, lw, rb)] = v
+        print(f"ntt batched {row}/{lw}/{rb}: { {k: round(v[(row, lw, rb)], 2) for k, v in sorted(ms.items())} }",
+              flush=True)
     out = {}
     for k, by in sorted(ms.items()):
         if k not in ks:
             continue
-        (row, lw), best = min(by.items(), key=lambda kv: kv[1])
-        out[str(k)] = {"row_bits": row, "col_width_log2": lw, "radix_log2": 3, "ms_batched": best}
-        P.set_ntt_geometry(k, row, lw, 3)
+        (row, lw, rb), best = min(by.items(), key=lambda kv: kv[1])
+        out[str(k)] = {"row_bits": row, "col_width_log2": lw, "radix_log2": rb, "ms_batched": best}
+        P.set_ntt_geometry(k, row, lw, rb)
     return out
 
 
@@ -203,7 +205,17 @@ def main():
     ap.add_argument("--out", default=DEFAULT_OUT)
     ap.add_argument("--batched", action="store_true",
                     help="time the geometry of k >= 14 on the merges of whole pi runs")
+    ap.add_argument("--only-batched", action="store_true",
+                    help="rerun only the batched geometry stage over the table in --out")
     args = ap.parse_args()
+    if args.only_batched:
+        P.init(0, tuned=True)
+        result = json.load(open(args.out))
+        result["ntt"].update(tune_ntt_batched(1_000_000_000))
+        with open(args.out, "w") as f:
+            json.dump(result, f, indent=1)
+        print("wrote", args.out)
+        return
     P.init(0, tuned=False)
     timer = Timer()
     result = {"gpu": None}

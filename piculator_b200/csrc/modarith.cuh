@@ -132,9 +132,37 @@ PIC_HD uint64_t shoup_lazy32(uint64_t x, uint64_t w, uint64_t ws, uint32_t c)
 // x ws: x1 s1 + hi(x1 s0) + hi(x0 s1) is floor(x ws / 2^64) minus at most 2
 // (the dropped terms sum to less than 3 2^64), and the Shoup quotient itself
 // is floor(x w / p) or one less, so x w - q p lies in [0, 4p).
+#ifndef PIC_SHOUP_WIDE
+#define PIC_SHOUP_WIDE 0
+#endif
 PIC_HD uint64_t shoup_approx32(uint64_t x, uint64_t w, uint64_t ws, uint32_t c)
 {
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && PIC_SHOUP_WIDE
+    // the same three partial products and corrections, with the 64-bit
+    // accumulations as 32 x 32 -> 64 multiply-adds (mad.wide.u32)
+    const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32);
+    const uint32_t s0 = (uint32_t)ws, s1 = (uint32_t)(ws >> 32);
+    const uint32_t w0 = (uint32_t)w, w1 = (uint32_t)(w >> 32);
+    uint32_t r0, r1;
+    asm("{\n\t.reg .u32 t0, t1, q0, q1, u1;\n\t.reg .u64 t, q, xw;\n\t"
+        "mul.hi.u32 t0, %2, %5;\n\t"
+        "mad.hi.cc.u32 t0, %3, %4, t0;\n\t"
+        "addc.u32 t1, 0, 0;\n\t"
+        "mov.b64 t, {t0, t1};\n\t"
+        "mad.wide.u32 q, %3, %5, t;\n\t"
+        "mov.b64 {q0, q1}, q;\n\t"
+        "mul.wide.u32 xw, %2, %6;\n\t"
+        "mov.b64 {%0, %1}, xw;\n\t"
+        "mad.lo.u32 %1, %2, %7, %1;\n\t"
+        "mad.lo.u32 %1, %3, %6, %1;\n\t"
+        "mad.lo.u32 u1, q0, %8, q1;\n\t"
+        "sub.cc.u32 %0, %0, q0;\n\t"
+        "subc.u32 %1, %1, u1;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"(x0), "r"(x1), "r"(s0), "r"(s1), "r"(w0), "r"(w1), "r"(c));
+    return ((uint64_t)r1 << 32) | r0;
+#elif defined(__CUDA_ARCH__)
     const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32);
     const uint32_t s0 = (uint32_t)ws, s1 = (uint32_t)(ws >> 32);
     const uint32_t w0 = (uint32_t)w, w1 = (uint32_t)(w >> 32);

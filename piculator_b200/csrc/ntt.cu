@@ -717,28 +717,28 @@ __device__ __forceinline__ void group_fast(uint64_t (&x)[1 << B], int j, const L
     }
 }
 
-// Radix-8 rounds of a 2^LOGN transform (plus one radix-2 or radix-4 round when
-// 3 does not divide LOGN, at the smallest stride); forward rounds run from the
+// Radix-2^RB rounds of a 2^LOGN transform (plus one smaller round when RB
+// does not divide LOGN, at the smallest stride); forward rounds run from the
 // largest stride down, inverse rounds the other way.
-template <int LOGN>
+template <int LOGN, int RB = 3>
 struct RoundPlan {
-    static constexpr int NF = LOGN / 3, REM = LOGN % 3, NR = NF + (REM ? 1 : 0);
+    static constexpr int NF = LOGN / RB, REM = LOGN % RB, NR = NF + (REM ? 1 : 0);
     template <int RR>
     struct At {
-        static constexpr int B = RR < NF ? 3 : REM;
-        static constexpr int LB = LOGN - 3 * RR;  // log2 sub-block size
-        static constexpr int LST = LB - B;        // log2 stride inside a group
+        static constexpr int B = RR < NF ? RB : REM;
+        static constexpr int LB = LOGN - RB * RR;  // log2 sub-block size
+        static constexpr int LST = LB - B;         // log2 stride inside a group
     };
 };
 
 // Row layout: transform t of the CTA at s + (t << LR), element e at swz(e).
 // With several transforms per CTA (LRPC > 0, single-pass lengths), each
 // group takes the prime of its own transform: a CTA may straddle primes.
-template <bool INV, int LR, int LRPC, int NT, int R>
+template <bool INV, int LR, int LRPC, int NT, int RB, int R>
 __device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const NttBatch& Bt, size_t row0,
                                                 const LazyPrime& L0, const ulonglong2* __restrict__ tw0)
 {
-    using Plan = RoundPlan<LR>;
+    using Plan = RoundPlan<LR, RB>;
     constexpr int RR = INV ? Plan::NR - 1 - R : R;
     using A = typename Plan::template At<RR>;
     constexpr int B = A::B, LB = A::LB, LST = A::LST;
@@ -767,24 +767,28 @@ __device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const 
         for (int m = 0; m < (1 << B); m++) ptr[swz(base + (m << LST))] = x[m];
     }
     __syncthreads();
-    if constexpr (R + 1 < Plan::NR) rows_fast_round<INV, LR, LRPC, NT, R + 1>(s, Bt, row0, L0, tw0);
+    if constexpr (R + 1 < Plan::NR) rows_fast_round<INV, LR, LRPC, NT, RB, R + 1>(s, Bt, row0, L0, tw0);
 }
 
-template <int LR, int LRPC>
+// One thread per group of a full round: 2^(LR + LRPC - RB) threads, at most
+// 512.  Radix-16 groups hold 16 residues per thread, so that form runs one
+// CTA of up to 512 threads per SM with room for 128 registers a thread.
+template <int LR, int LRPC, int RB = 3>
 struct RowsFastShape {
     static constexpr int TOT = 1 << (LR + LRPC);
-    static constexpr int NT = (TOT >> 3) > 512 ? 512 : (TOT >> 3);
+    static constexpr int NT = (TOT >> RB) > 512 ? 512 : ((TOT >> RB) < 32 ? 32 : (TOT >> RB));
+    static constexpr int MINB = RB == 3 ? 1024 / NT : 1;
 };
 
 // Contiguous row pass: 2^LRPC rows of 2^LR points per CTA.  LRPC > 0 only
 // for single-pass lengths (k = LR, one row per transform); the last CTA may
 // hold fewer than 2^LRPC transforms.
-template <bool INV, int LR, int LRPC>
-__global__ void __launch_bounds__(RowsFastShape<LR, LRPC>::NT, 1024 / RowsFastShape<LR, LRPC>::NT)
+template <bool INV, int LR, int LRPC, int RB>
+__global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape<LR, LRPC, RB>::MINB)
     ntt_rows_fast_kernel(NttBatch B, int k)
 {
     extern __shared__ uint64_t smem[];
-    constexpr int TOT = RowsFastShape<LR, LRPC>::TOT, NT = RowsFastShape<LR, LRPC>::NT;
+    constexpr int TOT = RowsFastShape<LR, LRPC, RB>::TOT, NT = RowsFastShape<LR, LRPC, RB>::NT;
     constexpr int EMASK = (1 << LR) - 1;
     const int lrow = k - LR;  // log2 rows per transform
     const size_t rmask = ((size_t)1 << lrow) - 1;
@@ -819,7 +823,7 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC>::NT, 1024 / RowsFastSh
         }
     }
     __syncthreads();
-    rows_fast_round<INV, LR, LRPC, NT, 0>(smem, B, row0, L,
+    rows_fast_round<INV, LR, LRPC, NT, RB, 0>(smem, B, row0, L,
                                           reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
 #pragma unroll
     for (int i = 0; i < TOT / NT; i++) {
@@ -989,10 +993,11 @@ static void set_smem(K kern, size_t smem)
 }
 
 // The fast kernels serve batches of lazy primes whose inner tables have order
-// 2^13, with the default radix-8 rounds.
+// 2^13.  Column passes run radix-8 rounds; row passes radix-8, or radix-16
+// (rbits 4) for rows of 2^11 .. 2^13 points.
 static bool fast_ok(const NttBatch& b, int k)
 {
-    if (!PIC_NTT_FAST || g_geom[k].rbits != 3) return false;
+    if (!PIC_NTT_FAST || (g_geom[k].rbits != 3 && g_geom[k].rbits != 4)) return false;
     for (int q = 0; q * b.per_prime < b.count; q++)
         if (!b.prime[q].lazy || b.prime[q].IB != 13 || b.prime[q].lvl_fwd == nullptr ||
             (q > 0 && (b.prime[q].slo_fwd == nullptr) != (b.prime[0].slo_fwd == nullptr)))
@@ -1002,22 +1007,30 @@ static bool fast_ok(const NttBatch& b, int k)
 
 constexpr int fast_lrpc(int lr) { return lr < 11 ? 11 - lr : 0; }
 
-template <bool INV, int LR>
+template <bool INV, int LR, int RB = 3>
 static void launch_rows_fast_t(const NttBatch& b, int k, cudaStream_t s)
 {
     constexpr int LRPC = fast_lrpc(LR);
-    using Sh = RowsFastShape<LR, LRPC>;
+    using Sh = RowsFastShape<LR, LRPC, RB>;
     const size_t rows = (size_t)b.count << (k - LR);
     const size_t grid = (rows + ((size_t)1 << LRPC) - 1) >> LRPC;
     const size_t smem = sizeof(uint64_t) * Sh::TOT;
-    set_smem(ntt_rows_fast_kernel<INV, LR, LRPC>, smem);
-    ntt_rows_fast_kernel<INV, LR, LRPC><<<(unsigned)grid, Sh::NT, smem, s>>>(b, k);
+    set_smem(ntt_rows_fast_kernel<INV, LR, LRPC, RB>, smem);
+    ntt_rows_fast_kernel<INV, LR, LRPC, RB><<<(unsigned)grid, Sh::NT, smem, s>>>(b, k);
 }
 
 template <bool INV>
 static bool launch_rows_fast(const NttBatch& b, int k, int lr, cudaStream_t s)
 {
     if (!(lr == k || lr >= 11)) return false;
+    if (g_geom[k].rbits == 4) {
+        switch (lr) {
+        case 11: launch_rows_fast_t<INV, 11, 4>(b, k, s); return true;
+        case 12: launch_rows_fast_t<INV, 12, 4>(b, k, s); return true;
+        case 13: launch_rows_fast_t<INV, 13, 4>(b, k, s); return true;
+        default: break;  // shorter rows keep radix-8 rounds
+        }
+    }
     switch (lr) {
     case 1: launch_rows_fast_t<INV, 1>(b, k, s); break;
     case 2: launch_rows_fast_t<INV, 2>(b, k, s); break;

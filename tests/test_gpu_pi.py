@@ -73,3 +73,23 @@ def test_pi_precision_selected_form_counts_fft_products(pic, golden):
     finally:
         pic.set_tuning(pic.TUNE_MUL_FFT_MAX, saved_fft)
         pic.set_tuning(pic.TUNE_FFT_ACCEPT_PPM, saved_acc)
+
+
+@pytest.mark.slow
+def test_pi_1e9_two_forms_cross_checked(pic, golden):
+    """Pi to 1e9 digits twice: the NTT-only form and the precision-selected
+    form (FP64 FFT for every product up to 4 M words where its proven piece
+    width allows -- the early Newton steps); both texts equal the reference's
+    pi.txt and each other."""
+    saved = pic.get_tuning(pic.TUNE_MUL_FFT_MAX)
+    try:
+        pic.set_tuning(pic.TUNE_MUL_FFT_MAX, 0)
+        t1, s1 = pic.pi_hex(1_000_000_000, pic.PI_CHOSEN)
+        pic.set_tuning(pic.TUNE_MUL_FFT_MAX, 1 << 22)
+        t2, s2 = pic.pi_hex(1_000_000_000, pic.PI_CHOSEN)
+    finally:
+        pic.set_tuning(pic.TUNE_MUL_FFT_MAX, saved)
+    g = golden["pi"]["1000000000"]["md5"]
+    assert hashlib.md5(t1).hexdigest() == g
+    assert t1 == t2
+    assert s1["fft_max_err"] == 0.0 and 0.0 < s2["fft_max_err"] < 0.25
