@@ -372,29 +372,32 @@ void dec_digits(const BigFloat& x, size_t groups, char* d_out)
             dec_sub(nxt.get() + ccap, 2 * ccap, cur.get(), cap, Z.get(), zs, zs, ccap, count, s);
         }
         {
-            // the quotient estimate is q or q - 1: items with r >= T take one more step
+            // the quotient estimate is q or q - 1: items with r >= T take one
+            // more step (checked again; more than one step means a reciprocal
+            // far off its bound, reported rather than looped on)
             const size_t cpi = (ccap + kDecWPC - 1) / kDecWPC;
             DevBuf<unsigned long long> hi(count, s);
             DevBuf<uint8_t> ge(count, s);
             DevBuf<unsigned int> nge(1, s);
-            PIC_CUDA(cudaMemsetAsync(hi.get(), 0, 8 * count, s));
-            PIC_CUDA(cudaMemsetAsync(nge.get(), 0, 4, s));
-            dec_diff_kernel<<<(unsigned)(count * cpi), 256, 0, s>>>(nxt.get() + ccap, 2 * ccap, dv.T.w(), tw, ccap,
-                                                                    cpi, hi.get());
-            dec_ge_kernel<<<grid_for(count, 256), 256, 0, s>>>(nxt.get() + ccap, 2 * ccap, dv.T.w(), tw, hi.get(),
-                                                               count, ge.get(), nge.get());
-            PIC_CHECK_LAUNCH();
-            count_launch(2);
-            uint32_t n_ge = 0;
-            read_words(&n_ge, (const uint32_t*)nge.get(), 1, s);
-            if (n_ge) {
+            DevBuf<uint32_t> fin(1, s), d1(1, s);
+            const uint32_t one = 1;
+            PIC_CUDA(cudaMemcpyAsync(d1.get(), &one, 4, cudaMemcpyHostToDevice, s));
+            for (int round = 0;; round++) {
+                PIC_CUDA(cudaMemsetAsync(hi.get(), 0, 8 * count, s));
+                PIC_CUDA(cudaMemsetAsync(nge.get(), 0, 4, s));
+                dec_diff_kernel<<<(unsigned)(count * cpi), 256, 0, s>>>(nxt.get() + ccap, 2 * ccap, dv.T.w(), tw,
+                                                                        ccap, cpi, hi.get());
+                dec_ge_kernel<<<grid_for(count, 256), 256, 0, s>>>(nxt.get() + ccap, 2 * ccap, dv.T.w(), tw,
+                                                                   hi.get(), count, ge.get(), nge.get());
+                PIC_CHECK_LAUNCH();
+                count_launch(2);
+                uint32_t n_ge = 0;
+                read_words(&n_ge, (const uint32_t*)nge.get(), 1, s);
+                if (n_ge == 0) break;
+                PIC_REQUIRE(round < 2, PIC_ERR_INVALID, "decimal split: quotient estimate off by more than one");
                 std::vector<uint8_t> h(count);
                 PIC_CUDA(cudaMemcpyAsync(h.data(), ge.get(), count, cudaMemcpyDeviceToHost, s));
                 PIC_CUDA(cudaStreamSynchronize(s));
-                DevBuf<uint32_t> fin(1, s);
-                const uint32_t one = 1;
-                DevBuf<uint32_t> d1(1, s);
-                PIC_CUDA(cudaMemcpyAsync(d1.get(), &one, 4, cudaMemcpyHostToDevice, s));
                 for (size_t i = 0; i < count; i++) {
                     if (!h[i]) continue;
                     uint32_t* q = nxt.get() + 2 * i * ccap;
@@ -404,7 +407,6 @@ void dec_digits(const BigFloat& x, size_t groups, char* d_out)
                     lin_addsub(q, ccap, WordView{q, 0, (int64_t)ccap}, WordView{d1.get(), 0, 1}, 0, false, fin.get(),
                                s);
                 }
-                PIC_CUDA(cudaStreamSynchronize(s));
             }
         }
         cur = std::move(nxt);
