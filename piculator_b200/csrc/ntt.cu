@@ -837,11 +837,11 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape
 
 // Column tile: 2^LC rows x 2^LW columns, element (m, w) at s[(m << LW) + w];
 // consecutive threads take consecutive columns.
-template <bool INV, int LC, int LW, int R>
+template <bool INV, int LC, int LW, int RB, int R>
 __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const LazyPrime& L,
                                                 const ulonglong2* __restrict__ tw)
 {
-    using Plan = RoundPlan<LC>;
+    using Plan = RoundPlan<LC, RB>;
     constexpr int RR = INV ? Plan::NR - 1 - R : R;
     using A = typename Plan::template At<RR>;
     constexpr int B = A::B, LB = A::LB, LST = A::LST;
@@ -861,7 +861,7 @@ __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const 
         for (int m = 0; m < (1 << B); m++) s[((base + (m << LST)) << LW) + w] = x[m];
     }
     __syncthreads();
-    if constexpr (R + 1 < Plan::NR) cols_fast_round<INV, LC, LW, R + 1>(s, L, tw);
+    if constexpr (R + 1 < Plan::NR) cols_fast_round<INV, LC, LW, RB, R + 1>(s, L, tw);
 }
 
 // floor(x 2^64 / p) for x < p: q' = floor(x mu / 2^64) with mu = floor(2^128 /
@@ -903,8 +903,10 @@ __global__ void pass_table_kernel(ulonglong2* __restrict__ out, PrimeDev P, int 
 // twiddle root_(2^lblock)^((c0 + w) k1) is applied as two Shoup products
 // with the two-level outer tables: forward after the column DIF, inverse
 // before the column DIT.
-template <bool INV, int LC, int LW>
-__global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatch B, int k, int lpre, PassTw pt)
+// RB 4: radix-16 rounds, 16 residues per thread, two CTAs per SM.
+template <bool INV, int LC, int LW, int RB>
+__global__ void __launch_bounds__(256, RB == 4 ? 2 : (INV ? 3 : 4))
+    ntt_cols_fast_kernel(NttBatch B, int k, int lpre, PassTw pt)
 {
     extern __shared__ uint64_t smem[];
     constexpr int TOT = 1 << (LC + LW), WMASK = (1 << LW) - 1;
@@ -953,7 +955,7 @@ __global__ void __launch_bounds__(256, INV ? 3 : 4) ntt_cols_fast_kernel(NttBatc
         }
     }
     __syncthreads();
-    cols_fast_round<INV, LC, LW, 0>(smem, L, reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
+    cols_fast_round<INV, LC, LW, RB, 0>(smem, L, reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
 #pragma unroll 8
     for (int idx = threadIdx.x; idx < TOT; idx += 256) {
         const int m = idx >> LW, w = idx & WMASK;
@@ -993,8 +995,8 @@ static void set_smem(K kern, size_t smem)
 }
 
 // The fast kernels serve batches of lazy primes whose inner tables have order
-// 2^13.  Column passes run radix-8 rounds; row passes radix-8, or radix-16
-// (rbits 4) for rows of 2^11 .. 2^13 points.
+// 2^13.  Passes run radix-8 rounds, or with rbits 4 radix-16 rounds for rows
+// of 2^11 .. 2^13 points and columns of 2^8 .. 2^11 rows.
 static bool fast_ok(const NttBatch& b, int k)
 {
     if (!PIC_NTT_FAST || (g_geom[k].rbits != 3 && g_geom[k].rbits != 4)) return false;
@@ -1086,7 +1088,7 @@ static const ulonglong2* pass_table(const PrimeDev& P, bool inv, int lblock, int
     return d;
 }
 
-template <bool INV, int LC, int LW>
+template <bool INV, int LC, int LW, int RB>
 static void launch_cols_fast_t(const NttBatch& b, int k, int lpre, size_t grid, cudaStream_t s)
 {
     constexpr size_t smem = sizeof(uint64_t) << (LC + LW);
@@ -1097,19 +1099,19 @@ static void launch_cols_fast_t(const NttBatch& b, int k, int lpre, size_t grid, 
         all = all && pt.t[q] != nullptr;
     }
     if (!all) pt = PassTw{};  // one form for every prime of the launch
-    set_smem(ntt_cols_fast_kernel<INV, LC, LW>, smem);
-    ntt_cols_fast_kernel<INV, LC, LW><<<(unsigned)grid, 256, smem, s>>>(b, k, lpre, pt);
+    set_smem(ntt_cols_fast_kernel<INV, LC, LW, RB>, smem);
+    ntt_cols_fast_kernel<INV, LC, LW, RB><<<(unsigned)grid, 256, smem, s>>>(b, k, lpre, pt);
 }
 
-template <bool INV, int LC>
+template <bool INV, int LC, int RB = 3>
 static bool launch_cols_fast_lc(const NttBatch& b, int k, int lpre, int lw, size_t grid, cudaStream_t s)
 {
     switch (lw) {
-    case 2: if constexpr (LC + 2 <= 13) { launch_cols_fast_t<INV, LC, 2>(b, k, lpre, grid, s); return true; } break;
-    case 3: if constexpr (LC + 3 <= 13) { launch_cols_fast_t<INV, LC, 3>(b, k, lpre, grid, s); return true; } break;
-    case 4: if constexpr (LC + 4 <= 13) { launch_cols_fast_t<INV, LC, 4>(b, k, lpre, grid, s); return true; } break;
-    case 5: if constexpr (LC + 5 <= 13) { launch_cols_fast_t<INV, LC, 5>(b, k, lpre, grid, s); return true; } break;
-    case 6: if constexpr (LC + 6 <= 13) { launch_cols_fast_t<INV, LC, 6>(b, k, lpre, grid, s); return true; } break;
+    case 2: if constexpr (LC + 2 <= 13) { launch_cols_fast_t<INV, LC, 2, RB>(b, k, lpre, grid, s); return true; } break;
+    case 3: if constexpr (LC + 3 <= 13) { launch_cols_fast_t<INV, LC, 3, RB>(b, k, lpre, grid, s); return true; } break;
+    case 4: if constexpr (LC + 4 <= 13) { launch_cols_fast_t<INV, LC, 4, RB>(b, k, lpre, grid, s); return true; } break;
+    case 5: if constexpr (LC + 5 <= 13) { launch_cols_fast_t<INV, LC, 5, RB>(b, k, lpre, grid, s); return true; } break;
+    case 6: if constexpr (LC + 6 <= 13) { launch_cols_fast_t<INV, LC, 6, RB>(b, k, lpre, grid, s); return true; } break;
     default: break;
     }
     return false;
@@ -1118,6 +1120,15 @@ static bool launch_cols_fast_lc(const NttBatch& b, int k, int lpre, int lw, size
 template <bool INV>
 static bool launch_cols_fast(const NttBatch& b, int k, int lpre, int lc, int lw, size_t grid, cudaStream_t s)
 {
+    if (g_geom[k].rbits == 4) {  // radix-16 rounds for the tall columns of long transforms
+        switch (lc) {
+        case 8: return launch_cols_fast_lc<INV, 8, 4>(b, k, lpre, lw, grid, s);
+        case 9: return launch_cols_fast_lc<INV, 9, 4>(b, k, lpre, lw, grid, s);
+        case 10: return launch_cols_fast_lc<INV, 10, 4>(b, k, lpre, lw, grid, s);
+        case 11: return launch_cols_fast_lc<INV, 11, 4>(b, k, lpre, lw, grid, s);
+        default: break;
+        }
+    }
     switch (lc) {
     case 1: return launch_cols_fast_lc<INV, 1>(b, k, lpre, lw, grid, s);
     case 2: return launch_cols_fast_lc<INV, 2>(b, k, lpre, lw, grid, s);
