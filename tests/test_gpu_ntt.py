@@ -137,3 +137,22 @@ def test_fft_forward_matches_oracle_convention(pic, torch_cuda, oracle):
     torch.cuda.synchronize()
     want = oracle.fft(k, x)
     assert np.allclose(t.cpu().numpy(), want, rtol=1e-9, atol=1e-8)
+
+
+@pytest.mark.parametrize("k", [10, 15])
+def test_fft_matches_reference_fft(pic, torch_cuda, reference, k):
+    """pic_fft_forward / pic_fft_inverse against the reference's own AVX
+    fft_forward / fft_inverse (FFT.cpp:64-463, compiled from its sources):
+    same sign convention, bit-reversed order and unscaled inverse, to FP64
+    rounding (rtol 1e-9)."""
+    torch = torch_cuda
+    rng = np.random.default_rng(40 + k)
+    x = rng.standard_normal(2 << k)
+    L = pic.lib()
+    for inv in (False, True):
+        t = torch.from_numpy(x.copy()).cuda()
+        f = L.pic_fft_inverse if inv else L.pic_fft_forward
+        pic.check(f(t.data_ptr(), k, _stream(torch)))
+        torch.cuda.synchronize()
+        want = reference.fft(k, x, inverse=inv)
+        assert np.allclose(t.cpu().numpy(), want, rtol=1e-9, atol=1e-8 * (1 << (k // 2)))
