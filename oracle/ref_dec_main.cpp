@@ -3,13 +3,15 @@
  * reference sources by oracle/Makefile into oracle/_ref/picref_dec.  Test
  * infrastructure only (the golden fixtures of the decimal conversion).
  *
- *   picref_dec words <file> <digits>   the number stored in <file>
+ *   picref_dec words <file> <digits> <out>   the number stored in <file>
  *       (int32 sign, int64 exp, uint64 L, then L uint32 words, little-endian)
- *   picref_dec pi <digits> <threads>   Pi()'s final number: the reference's
- *       Pi_BSR, combination, division, inverse square root and final product
- *       in Pi()'s order (PI.h:141-199); Pi() itself prints it in hex
+ *   picref_dec pi <digits> <threads> <out>   Pi()'s final number: the
+ *       reference's Pi_BSR, combination, division, inverse square root and
+ *       final product in Pi()'s order (PI.h:141-199); Pi() itself prints it
+ *       in hex
  *
- * prints to_string_dec(digits) on stdout. */
+ * writes to_string_dec(digits) into the file <out> (stdout carries the
+ * reference's own progress lines, PI.h:114-135). */
 #define private public
 #include "BigFloat.h"
 #undef private
@@ -19,8 +21,8 @@
 
 int main(int argc, char** argv)
 {
-    if (argc < 4) {
-        fprintf(stderr, "usage: %s words <file> <digits> | pi <digits> <threads>\n", argv[0]);
+    if (argc < 5) {
+        fprintf(stderr, "usage: %s words <file> <digits> <out> | pi <digits> <threads> <out>\n", argv[0]);
         return 2;
     }
     const std::string mode = argv[1];
@@ -47,6 +49,8 @@ int main(int argc, char** argv)
         const size_t p = (hex_digits + 9) / 9;
         const size_t p_dec = (digits + 9) / 9;
         const size_t terms = (size_t)(p_dec * 0.6346230241342037371474889163921741077188431452678) + 1;
+        fft_ensure_table(26);  // PI.h:145-146: the tables are built before the threads start
+        ntt_ensure_table(29);
         steps = terms - 1;
         time_init = wall_clock();
         BigFloat Q, R;
@@ -61,6 +65,9 @@ int main(int argc, char** argv)
         return 2;
     }
     const std::string s = P.to_string_dec(digits);
-    fwrite(s.data(), 1, s.size(), stdout);
-    return 0;
+    FILE* out = fopen(argv[4], "wb");
+    if (!out) return 6;
+    const bool ok = fwrite(s.data(), 1, s.size(), out) == s.size();
+    fclose(out);
+    return ok ? 0 : 7;
 }

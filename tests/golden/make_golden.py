@@ -150,9 +150,16 @@ def ref_dec_words(sign: bool, exp: int, words: np.ndarray, digits: int) -> bytes
         f.write(np.ascontiguousarray(words, dtype="<u4").tobytes())
         path = f.name
     try:
-        return subprocess.run([REF_DEC, "words", path, str(digits)], capture_output=True, check=True).stdout
+        return _ref_dec_run(["words", path, str(digits)])
     finally:
         os.unlink(path)
+
+
+def _ref_dec_run(args) -> bytes:
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "dec.txt")
+        subprocess.run([REF_DEC, *args, out], capture_output=True, check=True)
+        return open(out, "rb").read()
 
 
 def gen_dec() -> dict:
@@ -180,8 +187,7 @@ def gen_dec() -> dict:
     pi = {}
     for d in (10_000, 100_000, 1_000_000):
         t0 = time.time()
-        text = subprocess.run([REF_DEC, "pi", str(d), str(os.cpu_count() or 1)], capture_output=True,
-                              check=True).stdout
+        text = _ref_dec_run(["pi", str(d), str(os.cpu_count() or 1)])
         pi[str(d)] = {"md5": md5(text), "len": len(text), "head": text[:80].decode(), "tail": text[-80:].decode(),
                       "ref_seconds": round(time.time() - t0, 2)}
         print(f"pi dec {d}: {pi[str(d)]['md5']} ({pi[str(d)]['ref_seconds']} s)", flush=True)
