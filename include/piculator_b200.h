@@ -235,6 +235,7 @@ typedef struct {
     uint64_t products;     /* number of big products formed */
     double fft_max_err;    /* largest FFT rounding distance seen */
     uint64_t fft_recomputes;
+    uint64_t transform_reuses; /* Newton products that reused the iterate's forward transform */
 } pic_pi_stats;
 
 /* Computes pi to decimal_digits and writes the text the reference dumps into

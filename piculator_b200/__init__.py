@@ -51,7 +51,8 @@ class PiStats(C.Structure):
                 ("seconds_invsqrt", C.c_double), ("seconds_final_mul", C.c_double),
                 ("seconds_hex", C.c_double), ("seconds_total", C.c_double),
                 ("kernel_launches", C.c_uint64), ("products", C.c_uint64),
-                ("fft_max_err", C.c_double), ("fft_recomputes", C.c_uint64)]
+                ("fft_max_err", C.c_double), ("fft_recomputes", C.c_uint64),
+                ("transform_reuses", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}

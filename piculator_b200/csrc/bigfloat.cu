@@ -279,7 +279,10 @@ BigFloat BigFloat::rcp(size_t p, int threads) const
     if (p == 1) s = 0;
     if (p == 2) s = 1;
     BigFloat R = rcp(s, threads);
-    // r1 = r0 - (r0 * x - 1) * r0 -- BigFloat.cpp:510
+    // r1 = r0 - (r0 * x - 1) * r0 -- BigFloat.cpp:510.  Both products take
+    // r0 whole (it is shorter than p + 2 words) at the same main transform
+    // length, so its forward transform is made once.
+    OperandHold hold(R.T, R.L);
     return R.sub(this->mul(R, p, threads).sub(BigFloat(1), p).mul(R, p, threads), p);
 }
 
@@ -308,6 +311,7 @@ BigFloat invsqrt(uint32_t x, size_t p, int threads)
     if (p == 1) s = 0;
     if (p == 2) s = 1;
     BigFloat T = invsqrt(x, s, threads);
+    OperandHold hold(T.T, T.L);                  // r0 is transformed once for r0^2 and (...) * r0
     BigFloat temp = T.mul(T, p, threads);        // r0^2
     // r0^2 * x: the reference forms it as temp.mul(BigFloat(x), 0), an exact
     // product with a one-word operand (BigFloat.cpp:562).  mul(uint32) gives

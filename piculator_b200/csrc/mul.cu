@@ -3,6 +3,7 @@
 #include <string.h>
 
 #include <atomic>
+#include <utility>
 
 #include "carry.cuh"
 #include "common.cuh"
@@ -541,6 +542,66 @@ static NttBatch ntt3_batch_stride(uint64_t* data, size_t stride)
     return bat;
 }
 
+// ---- a held forward transform (transform reuse in the Newton steps) ----------
+// While an OperandHold for (src, n) is alive on this thread, three-prime
+// products that take that operand reuse its forward transform at main length
+// 2^k instead of transforming it again: the first such product computes it
+// (split + forward, stride 2^k) and keeps it, later ones read it.  The plain
+// product at 2^k and the main part of a wrapped product at Nm = 2^k split the
+// operand the same way (pieces 0 .. 2^k - 1, zero above), so one transform
+// serves both.  Only the operand's words, length and k decide a match.
+namespace {
+struct HeldOperand {
+    const uint32_t* src = nullptr;
+    size_t n = 0;
+    int k = -1;
+    DevBuf<uint64_t> T;  // 3 x 2^k residues, transforms 2^k apart, bit-reversed order
+};
+thread_local HeldOperand* t_held = nullptr;
+std::atomic<uint64_t> g_held_reuses{0};
+}  // namespace
+
+OperandHold::OperandHold(const uint32_t* src, size_t n) : prev_(t_held)
+{
+    auto* h = new HeldOperand;
+    h->src = src;
+    h->n = n;
+    held_ = h;
+    t_held = h;
+}
+
+OperandHold::~OperandHold()
+{
+    t_held = static_cast<HeldOperand*>(prev_);
+    delete static_cast<HeldOperand*>(held_);
+}
+
+uint64_t held_transform_reuses() { return g_held_reuses.load(); }
+
+static bool is_held(const uint32_t* x, size_t n) { return t_held && t_held->src == x && t_held->n == n; }
+
+// The held operand's forward transform at length 2^k (stride 2^k), computed
+// on first use at that length.
+static const uint64_t* held_transform(int k, cudaStream_t s)
+{
+    HeldOperand* h = t_held;
+    if (h->k != k) {
+        h->T = DevBuf<uint64_t>(3 * ((size_t)1 << k), s);
+        ntt3_forward_operand(h->T.get(), k, h->src, h->n, s);
+        h->k = k;
+    } else {
+        g_held_reuses.fetch_add(1);
+    }
+    return h->T.get();
+}
+
+// Copies three transforms of 2^k residues from stride `from` to stride `to`.
+static void copy_transforms(uint64_t* dst, size_t to, const uint64_t* src, size_t from, int k, cudaStream_t s)
+{
+    PIC_CUDA(cudaMemcpy2DAsync(dst, to * sizeof(uint64_t), src, from * sizeof(uint64_t),
+                               sizeof(uint64_t) << k, 3, cudaMemcpyDeviceToDevice, s));
+}
+
 // The wrapped form of mul_ntt3 (see wrap_fix_kernel): main transforms of
 // length Nm = 2^km, tails of length 2^kt over the top W pieces.
 static void mul_ntt3_wrapped(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int km,
@@ -553,27 +614,33 @@ static void mul_ntt3_wrapped(uint32_t* z, const uint32_t* a, size_t na, const ui
     const size_t ST = Nm + ((W + 15) & ~(size_t)15);
     const bool square = (a == b && na == nb);
     const uint64_t P0 = kProductPrimes[0], P1 = kProductPrimes[1], P2 = kProductPrimes[2];
-    DevBuf<uint64_t> A(3 * ST, s), B(square ? 0 : 3 * ST, s), tA(3 * T, s), tB(square ? 0 : 3 * T, s);
+    // a held b (or a held square) brings its main transform with it
+    const uint64_t* held = is_held(b, nb) ? held_transform(km, s) : nullptr;
+    DevBuf<uint64_t> A(3 * ST, s), B(square || held ? 0 : 3 * ST, s), tA(3 * T, s), tB(square ? 0 : 3 * T, s);
     {
         ProfScope ps(KC_SPLIT, 4.0 * (double)(na + nb) + 24.0 * (double)(2 * (Nm + T)), s);
-        split3_off_kernel<<<grid_for(Nm, 256), 256, 0, s>>>(A.get(), ST, a, na, 0, Nm, P0, P1, P2);
+        if (!(held && square))
+            split3_off_kernel<<<grid_for(Nm, 256), 256, 0, s>>>(A.get(), ST, a, na, 0, Nm, P0, P1, P2);
         split3_off_kernel<<<grid_for(T, 256), 256, 0, s>>>(tA.get(), T, a, na, Nm - pb + 1, T, P0, P1, P2);
         if (!square) {
-            split3_off_kernel<<<grid_for(Nm, 256), 256, 0, s>>>(B.get(), ST, b, nb, 0, Nm, P0, P1, P2);
+            if (!held)
+                split3_off_kernel<<<grid_for(Nm, 256), 256, 0, s>>>(B.get(), ST, b, nb, 0, Nm, P0, P1, P2);
             split3_off_kernel<<<grid_for(T, 256), 256, 0, s>>>(tB.get(), T, b, nb, Nm - pa + 1, T, P0, P1, P2);
         }
         PIC_CHECK_LAUNCH();
-        count_launch(square ? 2 : 4);
+        count_launch((held && square ? 0 : 1) + 1 + (square ? 0 : (held ? 1 : 2)));
     }
     const NttBatch mA = ntt3_batch_stride(A.get(), ST), mB = ntt3_batch_stride(B.get(), ST);
     const NttBatch xA = ntt3_batch_stride(tA.get(), T), xB = ntt3_batch_stride(tB.get(), T);
-    ntt_forward_dif(mA, km, s);
+    if (held && square) copy_transforms(A.get(), ST, held, Nm, km, s);
+    else ntt_forward_dif(mA, km, s);
     ntt_forward_dif(xA, kt, s);
     if (!square) {
-        ntt_forward_dif(mB, km, s);
+        if (!held) ntt_forward_dif(mB, km, s);
         ntt_forward_dif(xB, kt, s);
     }
-    ntt_pointwise_mont(mA, square ? A.get() : B.get(), km, s);
+    if (held) ntt_pointwise_mont(mA, held, km, s, Nm);
+    else ntt_pointwise_mont(mA, square ? A.get() : B.get(), km, s);
     ntt_pointwise_mont(xA, square ? tA.get() : tB.get(), kt, s);
     ntt_inverse_dit(mA, km, s);
     ntt_inverse_dit(xA, kt, s);
@@ -597,6 +664,10 @@ static void mul_ntt3_wrapped(uint32_t* z, const uint32_t* a, size_t na, const ui
 
 void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s)
 {
+    if (is_held(a, na) && !(a == b && na == nb)) {  // the held operand goes second
+        std::swap(a, b);
+        std::swap(na, nb);
+    }
     const size_t zw = na + nb;
     const size_t pa = (na + 1) / 2, pb = (nb + 1) / 2;
     const size_t ncoef = pa + pb - 1;
@@ -618,11 +689,13 @@ void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size
         }
     }
     const bool square = (a == b && na == nb);
+    const uint64_t* held = is_held(b, nb) ? held_transform(k, s) : nullptr;
     DevBuf<uint64_t> A(3 * N, s);
-    DevBuf<uint64_t> B(square ? 0 : 3 * N, s);
-    ntt3_forward_operand(A.get(), k, a, na, s);
-    if (!square) ntt3_forward_operand(B.get(), k, b, nb, s);
-    ntt3_pointwise(A.get(), square ? A.get() : B.get(), k, s);
+    DevBuf<uint64_t> B(square || held ? 0 : 3 * N, s);
+    if (held && square) copy_transforms(A.get(), N, held, N, k, s);
+    else ntt3_forward_operand(A.get(), k, a, na, s);
+    if (!square && !held) ntt3_forward_operand(B.get(), k, b, nb, s);
+    ntt3_pointwise(A.get(), held ? held : (square ? A.get() : B.get()), k, s);
     ntt3_inverse_to_words(A.get(), k, ncoef, 1, z, zw, s);
 }
 

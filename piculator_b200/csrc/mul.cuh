@@ -11,6 +11,24 @@ namespace pic {
 
 // Three-prime NTT: 64-bit pieces, primes kProductPrimes, Garner CRT.
 void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s);
+
+// While alive, three-prime products on this thread that take the operand
+// (src, n) transform it once per transform length and reuse that forward
+// transform (the Newton steps multiply by their iterate twice,
+// BigFloat.cpp:510, 561-567).  Scopes nest.
+class OperandHold {
+public:
+    OperandHold(const uint32_t* src, size_t n);
+    ~OperandHold();
+    OperandHold(const OperandHold&) = delete;
+    OperandHold& operator=(const OperandHold&) = delete;
+
+private:
+    void* prev_;
+    void* held_;
+};
+// Products that found the held transform ready (since the process started).
+uint64_t held_transform_reuses();
 // The reference's own layout: 16-bit points in u64, one prime (the
 // reference's prime for k), length 2^k >= 4 (na + nb) (BigFloat.cpp:380-385).
 void mul_ntt_ref(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s);

@@ -1296,7 +1296,7 @@ void ntt_bitreverse(const NttBatch& b, int k, cudaStream_t s)
     count_launch();
 }
 
-__global__ void pointwise_mont_kernel(NttBatch B, const uint64_t* __restrict__ other, int k)
+__global__ void pointwise_mont_kernel(NttBatch B, const uint64_t* __restrict__ other, size_t ostride, int k)
 {
     const size_t n = (size_t)1 << k;
     const size_t total = (size_t)B.count * n;
@@ -1305,16 +1305,16 @@ __global__ void pointwise_mont_kernel(NttBatch B, const uint64_t* __restrict__ o
         const size_t tr = g >> k, i = g & (n - 1);
         const PrimeDev P = pick_prime(B, (int)tr);
         uint64_t* d = B.data + tr * B.stride + i;
-        *d = P.lazy ? mont_mul_c(*d, other[tr * B.stride + i], P.p, (uint32_t)(P.p >> 32))
-                    : mont_mul(*d, other[tr * B.stride + i], P.p, P.pinv_neg);
+        *d = P.lazy ? mont_mul_c(*d, other[tr * ostride + i], P.p, (uint32_t)(P.p >> 32))
+                    : mont_mul(*d, other[tr * ostride + i], P.p, P.pinv_neg);
     }
 }
 
-void ntt_pointwise_mont(const NttBatch& a, const uint64_t* b, int k, cudaStream_t s)
+void ntt_pointwise_mont(const NttBatch& a, const uint64_t* b, int k, cudaStream_t s, size_t b_stride)
 {
     const size_t total = (size_t)a.count << k;
     ProfScope ps(KC_NTT_POINTWISE, 24.0 * (double)total, s);
-    pointwise_mont_kernel<<<grid_for(total, 256), 256, 0, s>>>(a, b, k);
+    pointwise_mont_kernel<<<grid_for(total, 256), 256, 0, s>>>(a, b, b_stride ? b_stride : a.stride, k);
     PIC_CHECK_LAUNCH();
     count_launch();
 }

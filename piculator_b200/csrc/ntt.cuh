@@ -106,8 +106,9 @@ void ntt_inverse_dit(const NttBatch& b, int k, cudaStream_t s);
 void ntt_bitreverse(const NttBatch& b, int k, cudaStream_t s);
 
 // out[i] = a[i] * b[i] * 2^-64 mod p over every transform of the batch
-// (b may equal a for squaring).
-void ntt_pointwise_mont(const NttBatch& a, const uint64_t* b, int k, cudaStream_t s);
+// (b may equal a for squaring); b's transforms are b_stride apart (0: a's
+// stride).
+void ntt_pointwise_mont(const NttBatch& a, const uint64_t* b, int k, cudaStream_t s, size_t b_stride = 0);
 
 // T[i] = T[i] * A[i] mod p exactly (reference ntt_pointwise semantics).
 void ntt_pointwise_plain(uint64_t* T, const uint64_t* A, int k, const PrimeDev& P, cudaStream_t s);

@@ -101,6 +101,7 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
     const uint64_t launches0 = ctx().launches.load();
     const uint64_t products0 = ctx().products.load();
     const uint64_t recompute0 = ctx().fft_recomputes.load();
+    const uint64_t reuse0 = held_transform_reuses();
     fft_reset_max_err();
     const int saved_mode = get_mul_mode();
     set_mul_mode(mode == PIC_PI_PLAIN ? PIC_MUL_NTT3 : PIC_MUL_AUTO);
@@ -159,6 +160,7 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
         st->products = ctx().products.load() - products0;
         st->fft_max_err = fft_max_err_seen();
         st->fft_recomputes = ctx().fft_recomputes.load() - recompute0;
+        st->transform_reuses = held_transform_reuses() - reuse0;
     }
     return P;
 }

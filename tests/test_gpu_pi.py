@@ -93,3 +93,13 @@ def test_pi_1e9_two_forms_cross_checked(pic, golden):
     assert hashlib.md5(t1).hexdigest() == g
     assert t1 == t2
     assert s1["fft_max_err"] == 0.0 and 0.0 < s2["fft_max_err"] < 0.25
+
+
+@pytest.mark.parametrize("digits", [1_000_000, 10_000_000])
+def test_newton_reuses_the_iterate_transform(pic, golden, digits):
+    """The division's and the inverse square root's Newton steps multiply by
+    their iterate twice (BigFloat.cpp:510, 561-567); the iterate's forward
+    transform is made once per step and reused, and the text is unchanged."""
+    text, st = pic.pi_hex(digits, pic.PI_CHOSEN)
+    assert hashlib.md5(text).hexdigest() == golden["pi"][str(digits)]["md5"]
+    assert st["transform_reuses"] > 0
