@@ -285,9 +285,11 @@ enum {
     PIC_TUNE_BSR_SMALL_MERGE = 5, /* short schoolbook levels: 0 CTA, 1 + warp, 2 + thread per parent (default) */
     PIC_TUNE_MUL_WRAP = 6,        /* 1: three-prime products use the wrapped form when it is shorter (default) */
     PIC_TUNE_BSR_COMBINE = 7,     /* 1: binary-splitting NTT merges form P in the transform domain (default) */
-    PIC_TUNE_FFT_ACCEPT_PPM = 8   /* FFT products whose max rounding distance exceeds value * 1e-6 are
+    PIC_TUNE_FFT_ACCEPT_PPM = 8,  /* FFT products whose max rounding distance exceeds value * 1e-6 are
                                      recomputed with NTT3 (default 250000 = 0.25; lower it to test the
                                      recompute path) */
+    PIC_TUNE_BSR_KARATSUBA = 9    /* CTA schoolbook merges take one Karatsuba level for operands of at
+                                     least this many words (0 = never) */
 };
 pic_status pic_set_tuning(int knob, int64_t value);
 int64_t pic_get_tuning(int knob);

@@ -199,6 +199,8 @@ def apply_tuning(path: str = TUNING_FILE) -> bool:
         check(L.pic_set_tuning(TUNE_MUL_FFT_MAX, int(prod["fft_max_words"])))
     if "bsr_school_max_words" in t.get("bsr", {}):
         check(L.pic_set_tuning(TUNE_BSR_SCHOOL_MAX, int(t["bsr"]["bsr_school_max_words"])))
+    if "bsr_karatsuba_min_words" in t.get("bsr", {}):
+        check(L.pic_set_tuning(TUNE_BSR_KARATSUBA, int(t["bsr"]["bsr_karatsuba_min_words"])))
     return True
 
 
@@ -358,7 +360,7 @@ class Transform:
 
 
 (TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS, TUNE_BSR_WRAP,
- TUNE_BSR_SMALL_MERGE, TUNE_MUL_WRAP, TUNE_BSR_COMBINE, TUNE_FFT_ACCEPT_PPM) = range(9)
+ TUNE_BSR_SMALL_MERGE, TUNE_MUL_WRAP, TUNE_BSR_COMBINE, TUNE_FFT_ACCEPT_PPM, TUNE_BSR_KARATSUBA) = range(10)
 
 
 def butterfly_rate() -> float:

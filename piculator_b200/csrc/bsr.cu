@@ -375,6 +375,81 @@ __device__ uint32_t cta_top(const uint32_t* x, uint32_t n)
     return (uint32_t)block_max_u64(mine);
 }
 
+// z[0..zn) += x[0..xn) (sub: -=), in place, words of x past zn ignored; the
+// caller guarantees the exact result fits zn words and is nonnegative.
+__device__ void cta_add_into(uint32_t* z, uint32_t zn, const uint32_t* x, uint32_t xn, bool sub)
+{
+    const uint32_t per = (zn + blockDim.x - 1) / blockDim.x;
+    const uint32_t w0 = threadIdx.x * per, w1 = min(w0 + per, zn);
+    auto X = [&](uint32_t i) -> uint32_t { return i < xn ? x[i] : 0u; };
+    uint32_t gp = kGPIdentity;
+    for (uint32_t i = w0; i < w1; i++) {
+        const uint32_t a = z[i], b = X(i);
+        uint32_t d, g, p;
+        if (!sub) {
+            const uint64_t t = (uint64_t)a + b;
+            d = (uint32_t)t;
+            g = (uint32_t)(t >> 32);
+            p = d == 0xffffffffu;
+        } else {
+            d = a - b;
+            g = a < b;
+            p = d == 0u;
+        }
+        gp = gp_combine(gp, g | (p << 1));
+    }
+    uint32_t total;
+    uint32_t cin = block_gp_scan(gp, &total) & 1u;
+    for (uint32_t i = w0; i < w1; i++) {
+        const uint32_t a = z[i], b = X(i);
+        if (!sub) {
+            const uint64_t t = (uint64_t)a + b;
+            const uint32_t d = (uint32_t)t;
+            z[i] = d + cin;
+            cin = (uint32_t)(t >> 32) | ((uint32_t)(d == 0xffffffffu) & cin);
+        } else {
+            const uint32_t d = a - b;
+            z[i] = d - cin;
+            cin = (uint32_t)(a < b) | ((uint32_t)(d == 0u) & cin);
+        }
+    }
+    __syncthreads();
+}
+
+// z[0..na+nb) = a * b with one Karatsuba level when both operands are long
+// enough: with h = min(na, nb) / 2, a = a1 B^h + a0, b = b1 B^h + b0,
+//   z0 = a0 b0 and z2 = a1 b1 straight into z (disjoint halves),
+//   m = (a0 + a1)(b0 + b1) - z0 - z2 = a0 b1 + a1 b0 (>= 0),
+//   z += m B^h;
+// three schoolbook products of about half the length instead of one: 3/4
+// of the multiply-adds.  ws holds 3 (na + nb) + 8 words.  The words are those
+// of the schoolbook product.
+__device__ uint32_t cta_mul_k(const uint32_t* a, uint32_t na, const uint32_t* b, uint32_t nb, uint32_t* z,
+                              uint32_t* col, uint32_t* ws, uint32_t kara_min)
+{
+    const uint32_t mn = min(na, nb);
+    if (kara_min == 0 || mn < kara_min) return cta_mul(a, na, b, nb, z, col);
+    const uint32_t zw = na + nb, h = mn / 2;
+    const uint32_t la = na - h + 1, lb = nb - h + 1;  // sum lengths (carry word included)
+    uint32_t* sa = ws;
+    uint32_t* sb = sa + la;
+    uint32_t* m = sb + lb;  // la + lb words
+    // sa = a0 + a1, sb = b0 + b1 (na - h >= h words in a1, b1)
+    for (uint32_t i = threadIdx.x; i < la; i += blockDim.x) sa[i] = i + h < na ? a[i + h] : 0u;
+    for (uint32_t i = threadIdx.x; i < lb; i += blockDim.x) sb[i] = i + h < nb ? b[i + h] : 0u;
+    __syncthreads();
+    cta_add_into(sa, la, a, h, false);
+    cta_add_into(sb, lb, b, h, false);
+    // z0, z2 into z; m = sa sb
+    cta_mul(a, h, b, h, z, col);
+    cta_mul(a + h, na - h, b + h, nb - h, z + 2 * h, col);
+    cta_mul(sa, la, sb, lb, m, col);
+    cta_add_into(m, la + lb, z, 2 * h, true);
+    cta_add_into(m, la + lb, z + 2 * h, zw - 2 * h, true);
+    cta_add_into(z + h, zw - h, m, la + lb, false);
+    return z[zw - 1] == 0 ? zw - 1 : zw;
+}
+
 // Signed sum of magnitudes (sa, a[0..na)) + (sb, b[0..nb)) into z (capacity
 // max(na, nb) + 1).  Returns the length; *sz the sign.  Exact arithmetic
 // with the reference's sign dispatch (BigFloat.cpp:288-305).
@@ -462,6 +537,7 @@ struct MergeArgs {
     uint8_t* pS;
     uint32_t pcP, pcQ, pcR;
     size_t count;  // parents
+    uint32_t kara_min;  // Karatsuba level for products whose operands both have this many words (0: never)
 };
 
 __global__ void __launch_bounds__(256) merge_school_kernel(MergeArgs m)
@@ -481,6 +557,7 @@ __global__ void __launch_bounds__(256) merge_school_kernel(MergeArgs m)
     uint32_t* t1 = RR + m.ccR;         // ccP + ccQ
     uint32_t* t2 = t1 + m.ccP + m.ccQ; // ccP + ccR
     uint32_t* col = t2 + m.ccP + m.ccR;  // 3 (ccP + ccQ) (the largest product)
+    uint32_t* ws = col + 3 * (m.ccP + m.ccQ);  // Karatsuba sums and middle product
     for (uint32_t k = threadIdx.x; k < nPL; k += blockDim.x) PL[k] = m.cPw[L * m.ccP + k];
     for (uint32_t k = threadIdx.x; k < nQL; k += blockDim.x) QL[k] = m.cQw[L * m.ccQ + k];
     for (uint32_t k = threadIdx.x; k < nRL; k += blockDim.x) RL[k] = m.cRw[L * m.ccR + k];
@@ -489,14 +566,14 @@ __global__ void __launch_bounds__(256) merge_school_kernel(MergeArgs m)
     for (uint32_t k = threadIdx.x; k < nRR; k += blockDim.x) RR[k] = m.cRw[R * m.ccR + k];
     __syncthreads();
     // Q = QL QR, R = RL RR written straight to the parent slots via t1 staging
-    uint32_t nQ = cta_mul(QL, nQL, QR, nQR, t1, col);
+    uint32_t nQ = cta_mul_k(QL, nQL, QR, nQR, t1, col, ws, m.kara_min);
     for (uint32_t k = threadIdx.x; k < nQ; k += blockDim.x) m.pQw[i * m.pcQ + k] = t1[k];
-    uint32_t nR = cta_mul(RL, nRL, RR, nRR, t1, col);
+    uint32_t nR = cta_mul_k(RL, nRL, RR, nRR, t1, col, ws, m.kara_min);
     for (uint32_t k = threadIdx.x; k < nR; k += blockDim.x) m.pRw[i * m.pcR + k] = t1[k];
     __syncthreads();
     // P = PL QR + PR RL (PI.h:110)
-    const uint32_t n1 = cta_mul(PL, nPL, QR, nQR, t1, col);
-    const uint32_t n2 = cta_mul(PR, nPR, RL, nRL, t2, col);
+    const uint32_t n1 = cta_mul_k(PL, nPL, QR, nQR, t1, col, ws, m.kara_min);
+    const uint32_t n2 = cta_mul_k(PR, nPR, RL, nRL, t2, col, ws, m.kara_min);
     bool sP;
     uint32_t* pz = col;  // reuse: max(n1, n2) + 1 <= 3 (ccP + ccQ)
     const uint32_t nP = cta_signed_add(sL, t1, n1, sR, t2, n2, pz, &sP);
@@ -1174,6 +1251,7 @@ static inline int ceil_log2_sz(size_t n)
 static Mod64 prime_mod(int q) { return make_mod(kProductPrimes[q]); }
 
 static bool g_wrap = true;
+static uint32_t g_kara_min = 0;  // CTA schoolbook merges: Karatsuba level from this many words (0: off)
 static int g_small_merge = 2;  // 0: CTA schoolbook, 1: + warp per parent, 2: + thread per parent
 static bool g_top_batched = true;
 static bool g_wide_add = true;
@@ -1563,8 +1641,9 @@ static void merge_school(Level& ch, Level& par, cudaStream_t s)
     m.pcQ = par.Q.cap;
     m.pcR = par.R.cap;
     m.count = par.count;
+    m.kara_min = g_kara_min;
     const size_t words = 2 * ((size_t)m.ccP + m.ccQ + m.ccR) + (m.ccP + m.ccQ) + (m.ccP + m.ccR) +
-                         3 * ((size_t)m.ccP + m.ccQ);
+                         3 * ((size_t)m.ccP + m.ccQ) + (g_kara_min ? 3 * ((size_t)m.ccP + m.ccQ) + 8 : 0);
     const size_t smem = words * sizeof(uint32_t);
     PIC_REQUIRE(smem <= 200 * 1024, PIC_ERR_INVALID, "schoolbook merge tile too large");
     if (smem > 48 * 1024)
@@ -1599,6 +1678,8 @@ static uint32_t g_school_max = 600;
 
 void bsr_set_school_threshold(uint32_t words) { g_school_max = words; }
 void bsr_set_wrap(bool on) { g_wrap = on; }
+void bsr_set_karatsuba(uint32_t min_words) { g_kara_min = min_words; }
+uint32_t bsr_karatsuba() { return g_kara_min; }
 void bsr_set_combine(bool on) { g_combine = on; }
 bool bsr_combine() { return g_combine; }
 void bsr_set_small_merge(int mode) { g_small_merge = mode; }

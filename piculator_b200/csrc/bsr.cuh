@@ -16,6 +16,10 @@ uint32_t bsr_school_threshold();
 // Wrapped products in the NTT merges (main transform at the smaller power of
 // two plus a short tail product); on by default.
 void bsr_set_wrap(bool on);
+// CTA schoolbook merges take one Karatsuba level for products whose operands
+// both have at least this many words (0: plain schoolbook).
+void bsr_set_karatsuba(uint32_t min_words);
+uint32_t bsr_karatsuba();
 bool bsr_wrap();
 // Kernels for the short schoolbook levels: 0 one CTA per parent, 1 also one
 // warp per parent (nodes <= 64 words), 2 also one thread per parent (nodes

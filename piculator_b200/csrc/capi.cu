@@ -633,6 +633,11 @@ pic_status pic_set_tuning(int knob, int64_t value)
             PIC_REQUIRE(value <= 2, PIC_ERR_INVALID, "small-merge mode is 0, 1 or 2");
             bsr_set_small_merge((int)value);
             break;
+        case PIC_TUNE_BSR_KARATSUBA:
+            PIC_REQUIRE(value == 0 || (value >= 4 && value <= 4096), PIC_ERR_INVALID,
+                        "Karatsuba threshold is 0 or 4..4096 words");
+            bsr_set_karatsuba((uint32_t)value);
+            break;
         case PIC_TUNE_FFT_ACCEPT_PPM:
             PIC_REQUIRE(value <= 500000, PIC_ERR_INVALID, "FFT acceptance is at most 500000 ppm (0.5)");
             mul_set_fft_accept((double)value * 1e-6);
@@ -669,6 +674,7 @@ int64_t pic_get_tuning(int knob)
     case PIC_TUNE_MUL_WRAP: return mul_wrap() ? 1 : 0;
     case PIC_TUNE_BSR_COMBINE: return bsr_combine() ? 1 : 0;
     case PIC_TUNE_FFT_ACCEPT_PPM: return (int64_t)llround(mul_fft_accept() * 1e6);
+    case PIC_TUNE_BSR_KARATSUBA: return bsr_karatsuba();
     }
     return -1;
 }

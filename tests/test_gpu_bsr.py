@@ -46,3 +46,24 @@ def test_bsr_plain_form_vs_oracle(pic, oracle):
     P, Q, R = pic.bsr(0, 300, 1000, pic.PI_PLAIN)
     wP, wQ, wR = oracle.bsr(0, 300, 1000)
     assert _same(P, wP) and _same(Q, wQ) and _same(R, wR)
+
+
+# CTA schoolbook merges with one Karatsuba level (threshold 4, 16, 64 words;
+# school_max 600 keeps every level up to 600-word children on the CTA
+# kernel), the thread / warp kernels off so the CTA kernel sees short nodes too.
+@pytest.mark.parametrize("a,b,p", [(0, 706, 923), (0, 3000, 200), (0, 2000, 100_000), (0, 8000, 300_000)])
+@pytest.mark.parametrize("kara", [4, 16, 64])
+def test_bsr_karatsuba_vs_oracle(pic, oracle, a, b, p, kara):
+    knobs = {pic.TUNE_BSR_SCHOOL_MAX: 600, pic.TUNE_BSR_SMALL_MERGE: 0, pic.TUNE_BSR_KARATSUBA: kara}
+    saved = {k: pic.get_tuning(k) for k in knobs}
+    for k, v in knobs.items():
+        pic.set_tuning(k, v)
+    try:
+        P, Q, R = pic.bsr(a, b, p, pic.PI_CHOSEN)
+    finally:
+        for k, v in saved.items():
+            pic.set_tuning(k, v)
+    wP, wQ, wR = oracle.bsr(a, b, p)
+    assert _same(Q, wQ), "Q"
+    assert _same(R, wR), "R"
+    assert _same(P, wP), "P"
