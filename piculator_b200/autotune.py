@@ -12,7 +12,9 @@ Size classes and what is chosen for each:
     FFT, or the one-prime reference layout) -- i.e. the prime count and
     transform family -- as crossover thresholds;
   * binary splitting: the child length below which a level merges with the
-    CTA schoolbook instead of batched NTTs, timed on whole 1e9-digit pi runs.
+    CTA schoolbook instead of batched NTTs, and the operand length from which
+    that schoolbook takes a Karatsuba level, timed on whole 1e9-digit pi runs
+    (--only-bsr reruns just this stage over an existing table).
 
     python -m piculator_b200.autotune [--quick] [--batched] [--out PATH]
 
@@ -123,7 +125,8 @@ def tune_ntt_batched(digits: int, ks=range(14, 28), radices=(3, 4)) -> dict:
     is timed, and each length takes the candidate whose merge levels of that
     length were fastest (a level's wrapped tail product, usually two lengths
     shorter, runs under the same candidate).  Radix 16 (radix_log2 4) applies
-    to the row passes of 2^11 .. 2^13 points; column passes stay radix 8."""
+    to row passes of 2^11 .. 2^13 points and column passes of 2^8 .. 2^11
+    rows; other passes stay radix 8."""
     import subprocess
     import sys
     import tempfile
@@ -181,22 +184,29 @@ def tune_products(timer: Timer) -> dict:
 
 
 def tune_bsr(quick: bool) -> dict:
-    """Schoolbook threshold of the binary-splitting merges, timed on whole pi
-    runs at the headline size (the best threshold moves with the size)."""
+    """Schoolbook threshold of the binary-splitting merges and the Karatsuba
+    level of the CTA schoolbook kernel, timed on whole pi runs at the headline
+    size (the best threshold moves with the size).  Every candidate computes
+    the same words."""
     digits = 10_000_000 if quick else 1_000_000_000
     res = {}
     P.pi_hex(digits, P.PI_CHOSEN, want_text=False)
-    for thr in (192, 300, 450, 600, 900):
+    cands = [(thr, kara) for thr in (300, 450, 600, 900, 1400) for kara in (0, 48, 96, 192)]
+    for thr, kara in cands:
         P.set_tuning(P.TUNE_BSR_SCHOOL_MAX, thr)
+        P.set_tuning(P.TUNE_BSR_KARATSUBA, kara)
         best = None
         for _ in range(2):
             _, st = P.pi_hex(digits, P.PI_CHOSEN, want_text=False)
             best = st["seconds_bsr"] if best is None else min(best, st["seconds_bsr"])
-        res[thr] = best
-        print(f"bsr school threshold {thr}: {res[thr]:.4f} s", flush=True)
-    best = min(res, key=res.get)
-    P.set_tuning(P.TUNE_BSR_SCHOOL_MAX, best)
-    return {"bsr_school_max_words": best, "digits": digits, "seconds": res}
+        res[f"{thr}/{kara}"] = best
+        print(f"bsr school threshold {thr}, Karatsuba from {kara}: {best:.4f} s", flush=True)
+    key = min(res, key=res.get)
+    thr, kara = (int(x) for x in key.split("/"))
+    P.set_tuning(P.TUNE_BSR_SCHOOL_MAX, thr)
+    P.set_tuning(P.TUNE_BSR_KARATSUBA, kara)
+    return {"bsr_school_max_words": thr, "bsr_karatsuba_min_words": kara, "digits": digits,
+            "seconds": res}
 
 
 def main():
@@ -207,7 +217,18 @@ def main():
                     help="time the geometry of k >= 14 on the merges of whole pi runs")
     ap.add_argument("--only-batched", action="store_true",
                     help="rerun only the batched geometry stage over the table in --out")
+    ap.add_argument("--only-bsr", action="store_true",
+                    help="rerun only the binary-splitting thresholds over the table in --out")
     args = ap.parse_args()
+    if args.only_bsr:
+        P.init(0, tuned=True)
+        result = json.load(open(args.out))
+        P.apply_tuning(args.out)
+        result["bsr"] = tune_bsr(False)
+        with open(args.out, "w") as f:
+            json.dump(result, f, indent=1)
+        print("wrote", args.out)
+        return
     if args.only_batched:
         P.init(0, tuned=True)
         result = json.load(open(args.out))
