@@ -61,12 +61,12 @@ def test_pi_decimal_matches_reference(pic, golden, digits):
 
 
 def test_exact_against_python_integers(pic):
-    """N = floor(M 10^D / 2^B) for a 2^21-word fraction, D = 2,000,007."""
+    """N = floor(M 10^D / 2^B) for a 2^18-word fraction, D = 1,500,003."""
     sys.set_int_max_str_digits(0)
-    L = (1 << 21) + 1
+    L = (1 << 18) + 1
     w = random_words(99, L)
     w[-1] = 3
-    digits = 2_000_007
+    digits = 1_500_003
     text = pic.DeviceBigFloat.from_words(True, 0, w).to_dec(digits)
     M = int.from_bytes(w[:-1].astype("<u4").tobytes(), "little")
     D = 9 * ((digits + 8) // 9)
