@@ -224,17 +224,23 @@ def test_fft_recompute_past_threshold(pic, n):
 
 @pytest.mark.parametrize("row_bits", [11, 12, 13])
 def test_radix16_row_passes(pic, row_bits):
-    """Row passes with radix-16 register rounds (geometry radix_log2 4) give
-    the same words as Python integers, for lengths 2^14 .. 2^24."""
+    """Passes with radix-16 register rounds (geometry radix_log2 4: rows of
+    2^11 .. 2^13 points, columns of 2^8 .. 2^11 rows) give the same words as
+    radix-8 rounds, for lengths 2^14 .. 2^23, and Python integers where they
+    are quick (2^14, 2^17)."""
     saved = {k: pic.get_ntt_geometry(k) for k in range(14, 25)}
     try:
-        for k in range(14, 25):
-            _, lw, _ = saved[k]
-            pic.set_ntt_geometry(k, row_bits, lw, 4)
         for lg in (14, 17, 20, 23):
             n = 1 << lg  # n words -> about n pieces -> length 2^lg
             a, b = random_words(lg + row_bits, n), random_words(lg + 2 * row_bits, n - 5)
-            assert _int(pic.mul_host(a, b, "ntt3")) == _int(a) * _int(b), lg
+            got = {}
+            for rb in (3, 4):
+                for k in range(14, 25):
+                    pic.set_ntt_geometry(k, row_bits, saved[k][1], rb)
+                got[rb] = pic.mul_host(a, b, "ntt3")
+            assert np.array_equal(got[3], got[4]), lg
+            if lg <= 17:
+                assert _int(got[4]) == _int(a) * _int(b), lg
     finally:
         for k, (r, lw, rb) in saved.items():
             pic.set_ntt_geometry(k, r, lw, rb)
