@@ -132,7 +132,8 @@ enum {
     PIC_MUL_NTT3 = 2,     /* three 62-bit primes, 64-bit points, CRT */
     PIC_MUL_FFT = 3,      /* FP64 FFT, limb split from the rounding bound,
                              NTT recompute when max distance > 0.25 */
-    PIC_MUL_SCHOOL = 4    /* batched schoolbook (short operands) */
+    PIC_MUL_SCHOOL = 4,   /* batched schoolbook (short operands) */
+    PIC_MUL_NTT3D = 5     /* three primes below 2^47, 56-bit points, FP64 butterflies, CRT */
 };
 pic_status pic_mul(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b,
                    size_t nb, int mode, pic_stream s);
@@ -288,8 +289,12 @@ enum {
     PIC_TUNE_FFT_ACCEPT_PPM = 8,  /* FFT products whose max rounding distance exceeds value * 1e-6 are
                                      recomputed with NTT3 (default 250000 = 0.25; lower it to test the
                                      recompute path) */
-    PIC_TUNE_BSR_KARATSUBA = 9    /* CTA schoolbook merges take one Karatsuba level for operands of at
+    PIC_TUNE_BSR_KARATSUBA = 9,   /* CTA schoolbook merges take one Karatsuba level for operands of at
                                      least this many words (0 = never) */
+    PIC_TUNE_NTT_FORM = 10,       /* three-prime form of AUTO products and binary-splitting merges:
+                                     0 integer (PIC_MUL_NTT3), 1 FP64 (PIC_MUL_NTT3D) */
+    PIC_TUNE_DBL_PASS_TABLES = 11 /* 1: FP64 column passes stream per-point twiddle tables; 0 (default):
+                                     they form the twiddles from the two-level tables */
 };
 pic_status pic_set_tuning(int knob, int64_t value);
 int64_t pic_get_tuning(int knob);
@@ -299,6 +304,10 @@ int64_t pic_get_tuning(int knob);
  * and bits per register round (2..4, i.e. radix 4, 8 or 16). */
 pic_status pic_set_ntt_geometry(int k, int row_bits, int col_width_log2, int radix_log2);
 pic_status pic_get_ntt_geometry(int k, int* row_bits, int* col_width_log2, int* radix_log2);
+/* The same per product form (0 integer, 1 FP64; the FP64 form takes row bits
+ * 11..13 and radix bits 3..4, its passes having no general fallback). */
+pic_status pic_set_ntt_geometry_form(int form, int k, int row_bits, int col_width_log2, int radix_log2);
+pic_status pic_get_ntt_geometry_form(int form, int k, int* row_bits, int* col_width_log2, int* radix_log2);
 
 /* Sizes Pi() derives from the digit count (PI.h:141-144). */
 pic_status pic_pi_sizes(uint64_t decimal_digits, uint64_t* hex_digits,

@@ -28,9 +28,11 @@ OK, ERR_INVALID, ERR_LENGTH, ERR_DIVIDE_BY_ZERO, ERR_LIMIT, ERR_CUDA, ERR_NO_MEM
 # checkpoint flags (pic_pi_set_checkpoint)
 CKPT_WRITE, CKPT_RESUME = 1, 2
 # product modes
-MUL_AUTO, MUL_NTT_REF, MUL_NTT3, MUL_FFT, MUL_SCHOOL = range(5)
+MUL_AUTO, MUL_NTT_REF, MUL_NTT3, MUL_FFT, MUL_SCHOOL, MUL_NTT3D = range(6)
 MUL_MODES = {"auto": MUL_AUTO, "ntt_ref": MUL_NTT_REF, "ntt3": MUL_NTT3, "fft": MUL_FFT,
-             "school": MUL_SCHOOL}
+             "school": MUL_SCHOOL, "ntt3d": MUL_NTT3D}
+# three-prime product forms (PIC_TUNE_NTT_FORM)
+FORM_INT, FORM_DBL = 0, 1
 # pi forms
 PI_CHOSEN, PI_PLAIN = 0, 1
 
@@ -141,6 +143,9 @@ _SIGS = {
     "pic_get_tuning": ([C.c_int], C.c_int64),
     "pic_set_ntt_geometry": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
     "pic_get_ntt_geometry": ([C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "pic_set_ntt_geometry_form": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+    "pic_get_ntt_geometry_form": ([C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int)], C.c_int),
     "pic_pi_sizes": ([C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                       C.POINTER(C.c_uint64)], C.c_int),
 }
@@ -192,6 +197,8 @@ def apply_tuning(path: str = TUNING_FILE) -> bool:
     L = lib()
     for k, g in t.get("ntt", {}).items():
         check(L.pic_set_ntt_geometry(int(k), g["row_bits"], g["col_width_log2"], g["radix_log2"]))
+    for k, g in t.get("ntt_fp64", {}).items():
+        check(L.pic_set_ntt_geometry_form(FORM_DBL, int(k), g["row_bits"], g["col_width_log2"], g["radix_log2"]))
     prod = t.get("products", {})
     if "school_max_words" in prod:
         check(L.pic_set_tuning(TUNE_MUL_SCHOOL_MAX, int(prod["school_max_words"])))
@@ -201,6 +208,8 @@ def apply_tuning(path: str = TUNING_FILE) -> bool:
         check(L.pic_set_tuning(TUNE_BSR_SCHOOL_MAX, int(t["bsr"]["bsr_school_max_words"])))
     if "bsr_karatsuba_min_words" in t.get("bsr", {}):
         check(L.pic_set_tuning(TUNE_BSR_KARATSUBA, int(t["bsr"]["bsr_karatsuba_min_words"])))
+    if "ntt_form" in prod:
+        check(L.pic_set_tuning(TUNE_NTT_FORM, int(prod["ntt_form"])))
     return True
 
 
@@ -360,7 +369,8 @@ class Transform:
 
 
 (TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS, TUNE_BSR_WRAP,
- TUNE_BSR_SMALL_MERGE, TUNE_MUL_WRAP, TUNE_BSR_COMBINE, TUNE_FFT_ACCEPT_PPM, TUNE_BSR_KARATSUBA) = range(10)
+ TUNE_BSR_SMALL_MERGE, TUNE_MUL_WRAP, TUNE_BSR_COMBINE, TUNE_FFT_ACCEPT_PPM, TUNE_BSR_KARATSUBA,
+ TUNE_NTT_FORM, TUNE_DBL_PASS_TABLES) = range(12)
 
 
 def butterfly_rate() -> float:
@@ -379,13 +389,13 @@ def get_tuning(knob: int) -> int:
     return int(lib().pic_get_tuning(knob))
 
 
-def set_ntt_geometry(k: int, row_bits: int, col_width_log2: int, radix_log2: int) -> None:
-    check(lib().pic_set_ntt_geometry(k, row_bits, col_width_log2, radix_log2))
+def set_ntt_geometry(k: int, row_bits: int, col_width_log2: int, radix_log2: int, form: int = FORM_INT) -> None:
+    check(lib().pic_set_ntt_geometry_form(form, k, row_bits, col_width_log2, radix_log2))
 
 
-def get_ntt_geometry(k: int) -> tuple[int, int, int]:
+def get_ntt_geometry(k: int, form: int = FORM_INT) -> tuple[int, int, int]:
     r, c, x = C.c_int(), C.c_int(), C.c_int()
-    check(lib().pic_get_ntt_geometry(k, C.byref(r), C.byref(c), C.byref(x)))
+    check(lib().pic_get_ntt_geometry_form(form, k, C.byref(r), C.byref(c), C.byref(x)))
     return r.value, c.value, x.value
 
 

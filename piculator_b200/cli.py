@@ -120,7 +120,7 @@ def main() -> None:
                    help="split the binary splitting over the torchrun ranks (one GPU each)")
     m = sub.add_parser("mul", help="time an isolated product of two splitmix64 operands")
     m.add_argument("--words", default="8388608")
-    m.add_argument("--mode", default="ntt3", choices=("auto", "school", "ntt3", "fft", "ntt_ref"))
+    m.add_argument("--mode", default="ntt3", choices=("auto", "school", "ntt3", "ntt3d", "fft", "ntt_ref"))
     m.add_argument("--repeat", type=int, default=3)
     args = ap.parse_args()
     import os

@@ -642,6 +642,11 @@ pic_status pic_set_tuning(int knob, int64_t value)
             PIC_REQUIRE(value <= 500000, PIC_ERR_INVALID, "FFT acceptance is at most 500000 ppm (0.5)");
             mul_set_fft_accept((double)value * 1e-6);
             break;
+        case PIC_TUNE_NTT_FORM:
+            PIC_REQUIRE(value <= 1, PIC_ERR_INVALID, "product form is 0 (integer) or 1 (FP64)");
+            mul_set_ntt_form((int)value);
+            break;
+        case PIC_TUNE_DBL_PASS_TABLES: ntt_set_dbl_pass_tables(value != 0); break;
         default: throw Error(PIC_ERR_INVALID, "unknown tuning knob");
         }
     });
@@ -662,6 +667,22 @@ pic_status pic_get_ntt_geometry(int k, int* row_bits, int* col_width_log2, int* 
     });
 }
 
+pic_status pic_set_ntt_geometry_form(int form, int k, int row_bits, int col_width_log2, int radix_log2)
+{
+    return guarded([&] { ntt_set_geometry(k, row_bits, col_width_log2, radix_log2, form); });
+}
+
+pic_status pic_get_ntt_geometry_form(int form, int k, int* row_bits, int* col_width_log2, int* radix_log2)
+{
+    return guarded([&] {
+        PIC_REQ_PTR(row_bits);
+        PIC_REQ_PTR(col_width_log2);
+        PIC_REQ_PTR(radix_log2);
+        PIC_REQUIRE(form == 0 || form == 1, PIC_ERR_INVALID, "unknown product form");
+        ntt_get_geometry(k, row_bits, col_width_log2, radix_log2, form);
+    });
+}
+
 int64_t pic_get_tuning(int knob)
 {
     switch (knob) {
@@ -675,6 +696,8 @@ int64_t pic_get_tuning(int knob)
     case PIC_TUNE_BSR_COMBINE: return bsr_combine() ? 1 : 0;
     case PIC_TUNE_FFT_ACCEPT_PPM: return (int64_t)llround(mul_fft_accept() * 1e6);
     case PIC_TUNE_BSR_KARATSUBA: return bsr_karatsuba();
+    case PIC_TUNE_NTT_FORM: return mul_ntt_form();
+    case PIC_TUNE_DBL_PASS_TABLES: return ntt_dbl_pass_tables() ? 1 : 0;
     }
     return -1;
 }

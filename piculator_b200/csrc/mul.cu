@@ -7,6 +7,7 @@
 
 #include "carry.cuh"
 #include "common.cuh"
+#include "fp64mod.cuh"
 #include "mul.cuh"
 
 namespace pic {
@@ -555,6 +556,7 @@ struct HeldOperand {
     const uint32_t* src = nullptr;
     size_t n = 0;
     int k = -1;
+    int form = kFormInt;
     DevBuf<uint64_t> T;  // 3 x 2^k residues, transforms 2^k apart, bit-reversed order
 };
 thread_local HeldOperand* t_held = nullptr;
@@ -580,15 +582,19 @@ uint64_t held_transform_reuses() { return g_held_reuses.load(); }
 
 static bool is_held(const uint32_t* x, size_t n) { return t_held && t_held->src == x && t_held->n == n; }
 
-// The held operand's forward transform at length 2^k (stride 2^k), computed
-// on first use at that length.
-static const uint64_t* held_transform(int k, cudaStream_t s)
+void ntt3d_forward_operand(uint64_t* out, int k, const uint32_t* a, size_t na, cudaStream_t s);
+
+// The held operand's forward transform at length 2^k (stride 2^k) in the
+// given product form, computed on first use at that length and form.
+static const uint64_t* held_transform(int k, int form, cudaStream_t s)
 {
     HeldOperand* h = t_held;
-    if (h->k != k) {
+    if (h->k != k || h->form != form) {
         h->T = DevBuf<uint64_t>(3 * ((size_t)1 << k), s);
-        ntt3_forward_operand(h->T.get(), k, h->src, h->n, s);
+        if (form == kFormDbl) ntt3d_forward_operand(h->T.get(), k, h->src, h->n, s);
+        else ntt3_forward_operand(h->T.get(), k, h->src, h->n, s);
         h->k = k;
+        h->form = form;
     } else {
         g_held_reuses.fetch_add(1);
     }
@@ -615,7 +621,7 @@ static void mul_ntt3_wrapped(uint32_t* z, const uint32_t* a, size_t na, const ui
     const bool square = (a == b && na == nb);
     const uint64_t P0 = kProductPrimes[0], P1 = kProductPrimes[1], P2 = kProductPrimes[2];
     // a held b (or a held square) brings its main transform with it
-    const uint64_t* held = is_held(b, nb) ? held_transform(km, s) : nullptr;
+    const uint64_t* held = is_held(b, nb) ? held_transform(km, kFormInt, s) : nullptr;
     DevBuf<uint64_t> A(3 * ST, s), B(square || held ? 0 : 3 * ST, s), tA(3 * T, s), tB(square ? 0 : 3 * T, s);
     {
         ProfScope ps(KC_SPLIT, 4.0 * (double)(na + nb) + 24.0 * (double)(2 * (Nm + T)), s);
@@ -689,7 +695,7 @@ void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size
         }
     }
     const bool square = (a == b && na == nb);
-    const uint64_t* held = is_held(b, nb) ? held_transform(k, s) : nullptr;
+    const uint64_t* held = is_held(b, nb) ? held_transform(k, kFormInt, s) : nullptr;
     DevBuf<uint64_t> A(3 * N, s);
     DevBuf<uint64_t> B(square || held ? 0 : 3 * N, s);
     if (held && square) copy_transforms(A.get(), N, held, N, k, s);
@@ -697,6 +703,382 @@ void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size
     if (!square && !held) ntt3_forward_operand(B.get(), k, b, nb, s);
     ntt3_pointwise(A.get(), held ? held : (square ? A.get() : B.get()), k, s);
     ntt3_inverse_to_words(A.get(), k, ncoef, 1, z, zw, s);
+}
+
+// ---- the FP64 three-prime form ---------------------------------------------
+// Operands in 56-bit pieces (piece j = bits 56 j .. 56 j + 55), residues
+// modulo kDblPrimes held as doubles (fp64mod.cuh), the same transform passes
+// with FP64 butterflies, pointwise products without a Montgomery factor, and a
+// CRT that places coefficient j (below p0 p1 p2 < 2^141) at bit 56 j.  Inverse
+// outputs arrive with |y| < 12 p (unscaled).
+
+size_t pieces56(size_t nwords) { return (32 * nwords + 55) / 56; }
+
+struct DblPrimes3 {
+    double p[3], pinv[3];
+};
+
+static DblPrimes3 dbl_primes3()
+{
+    DblPrimes3 d;
+    for (int q = 0; q < 3; q++) {
+        d.p[q] = (double)kDblPrimes[q];
+        d.pinv[q] = 1.0 / d.p[q];
+    }
+    return d;
+}
+
+static NttBatch ntt3d_batch_stride(uint64_t* data, size_t stride)
+{
+    NttBatch bat;
+    bat.data = data;
+    bat.stride = stride;
+    bat.count = 3;
+    bat.per_prime = 1;
+    for (int q = 0; q < 3; q++) bat.prime[q] = dbl_prime_tables(kDblPrimes[q]).dev;
+    return bat;
+}
+
+// out[q stride + j] = piece first + j of a mod p_q, j < N.
+__global__ void split3d_off_kernel(uint64_t* __restrict__ out, size_t stride, const uint32_t* __restrict__ a,
+                                   uint32_t na, size_t first, size_t N, DblPrimes3 P)
+{
+    for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < N; j += (size_t)gridDim.x * blockDim.x) {
+        const uint64_t v = src_piece56_raw(a, na, first + j);
+#pragma unroll
+        for (int q = 0; q < 3; q++) out[q * stride + j] = dstore(dpiece56(v, P.p[q], P.pinv[q]));
+    }
+}
+
+static void split3d(uint64_t* out, size_t stride, const uint32_t* a, size_t na, size_t first, size_t N,
+                    cudaStream_t s)
+{
+    PIC_REQUIRE(na < ((size_t)1 << 32), PIC_ERR_LENGTH, "operand too long for the FP64 form");
+    split3d_off_kernel<<<grid_for(N, 256), 256, 0, s>>>(out, stride, a, (uint32_t)na, first, N, dbl_primes3());
+    PIC_CHECK_LAUNCH();
+    count_launch();
+}
+
+void ntt3d_forward_operand(uint64_t* out, int k, const uint32_t* a, size_t na, cudaStream_t s)
+{
+    const size_t N = (size_t)1 << k;
+    {
+        ProfScope ps(KC_SPLIT, 4.0 * (double)na + 24.0 * (double)N, s);
+        split3d(out, N, a, na, 0, N, s);
+    }
+    ntt_forward_dif(ntt3d_batch_stride(out, N), k, s);
+}
+
+struct CrtDConsts {
+    double p[3], pinv[3];
+    double sw[3], swp[3];  // N^-1 mod p_q and its companion
+    double i01, i01p;      // p0^-1 mod p1
+    double i012, i012p;    // (p0 p1)^-1 mod p2
+    double q012, q012p;    // p1^-1 mod p2 = p0 (p0 p1)^-1 mod p2
+    double off[3];         // 2^140 mod p_q when every coefficient gets the offset 2^140, else 0
+    uint64_t p0, p01_lo, p01_hi;
+};
+
+static void dbl_pair(uint64_t w, uint64_t p, double& d, double& dp)
+{
+    d = (double)w;
+    dp = d / (double)p;
+}
+
+static CrtDConsts make_crtd(int k, bool offset)
+{
+    CrtDConsts C;
+    const uint64_t P0 = kDblPrimes[0], P1 = kDblPrimes[1], P2 = kDblPrimes[2];
+    for (int q = 0; q < 3; q++) {
+        const uint64_t p = kDblPrimes[q];
+        C.p[q] = (double)p;
+        C.pinv[q] = 1.0 / C.p[q];
+        dbl_pair(host_powmod(((uint64_t)1 << k) % p, p - 2, p), p, C.sw[q], C.swp[q]);
+        C.off[q] = offset ? (double)host_powmod(2, 140, p) : 0.0;
+    }
+    dbl_pair(host_powmod(P0 % P1, P1 - 2, P1), P1, C.i01, C.i01p);
+    dbl_pair(host_powmod(host_mulmod(P0 % P2, P1 % P2, P2), P2 - 2, P2), P2, C.i012, C.i012p);
+    dbl_pair(host_powmod(P1 % P2, P2 - 2, P2), P2, C.q012, C.q012p);
+    const unsigned __int128 p01 = (unsigned __int128)P0 * P1;
+    C.p0 = P0;
+    C.p01_lo = (uint64_t)p01;
+    C.p01_hi = (uint64_t)(p01 >> 64);
+    return C;
+}
+
+// x in (-p, 2p) -> [0, p)
+__device__ __forceinline__ double dcanon2(double x, double p)
+{
+    x = x < 0.0 ? __dadd_rn(x, p) : x;
+    return x >= p ? __dadd_rn(x, -p) : x;
+}
+
+// Garner's CRT on three FP64 residues (|y| < 2^51): x = r0 + p0 (v1 + p1 v2)
+// with r_q = y_q N^-1 (+ offset) mod p_q, as three 64-bit limbs (x < 2^141).
+__device__ __forceinline__ void crt3d(const CrtDConsts& C, double y0, double y1, double y2, uint64_t& l0,
+                                      uint64_t& l1, uint64_t& l2)
+{
+    const double r0 = dcanon2(__dadd_rn(dmul_tw(y0, C.sw[0], C.swp[0], C.p[0]), C.off[0]), C.p[0]);
+    const double r1 = dcanon2(__dadd_rn(dmul_tw(y1, C.sw[1], C.swp[1], C.p[1]), C.off[1]), C.p[1]);
+    const double r2 = dcanon2(__dadd_rn(dmul_tw(y2, C.sw[2], C.swp[2], C.p[2]), C.off[2]), C.p[2]);
+    const double v1 = dcanon(dmul_tw(__dadd_rn(r1, -r0), C.i01, C.i01p, C.p[1]), C.p[1]);
+    const double a = dmul_tw(__dadd_rn(r2, -r0), C.i012, C.i012p, C.p[2]);
+    const double b = dmul_tw(v1, C.q012, C.q012p, C.p[2]);
+    const double v2 = dcanon(dreduce(__dadd_rn(a, -b), C.p[2], C.pinv[2]), C.p[2]);
+    const uint64_t R0 = dto_u64(r0), V1 = dto_u64(v1), V2 = dto_u64(v2);
+    const unsigned __int128 lo = (unsigned __int128)R0 + (unsigned __int128)C.p0 * V1 +
+                                 (unsigned __int128)C.p01_lo * V2;  // < 2^95 + 2^111
+    const unsigned __int128 hi = (lo >> 64) + (unsigned __int128)C.p01_hi * V2;
+    l0 = (uint64_t)lo;
+    l1 = (uint64_t)hi;
+    l2 = (uint64_t)(hi >> 64);
+}
+
+// A CTA of 256 threads owns 448 output limbs (28672 bits = 512 coefficients of
+// 56 bits); limbs i0 - 1 .. i0 + 447 take coefficients 512 b - 3 .. 512 b + 511.
+constexpr size_t kCrtDLPC = 448;
+constexpr size_t kCrtDWPC = 2 * kCrtDLPC;
+constexpr int kCrtDSlots = 515;
+
+__device__ __forceinline__ int64_t floordiv56(int64_t a) { return a >= 0 ? a / 56 : -((-a + 55) / 56); }
+
+// The 64 bits of coefficient c (three limbs) shifted to bit s relative to a
+// limb (-141 < s < 64): bits -s .. -s + 63 of c.
+__device__ __forceinline__ uint64_t coef_window(const uint64_t* c, int s)
+{
+    if (s >= 0) return c[0] << s;
+    const int r = -s;
+    if (r < 64) return (c[0] >> r) | (c[1] << (64 - r));
+    if (r == 64) return c[1];
+    if (r < 128) return (c[1] >> (r - 64)) | (c[2] << (128 - r));
+    return c[2] >> (r - 128);
+}
+
+// Limb i of the sum of c_j 2^(56 j): the windows of the coefficients that
+// reach it (at most four), as a 66-bit (lo, hi).  xs holds coefficient j at
+// slot j - j0.
+__device__ __forceinline__ void limb_windows(const uint64_t* xs, int64_t j0, int64_t i, uint64_t& lo, uint64_t& hi)
+{
+    lo = 0;
+    hi = 0;
+    if (i < 0) return;
+    int64_t jlo = floordiv56(64 * i - 141) + 1;
+    if (jlo < 0) jlo = 0;
+    const int64_t jhi = (64 * i + 63) / 56;
+    for (int64_t j = jlo; j <= jhi; j++) add128(lo, hi, coef_window(xs + 3 * (j - j0), (int)(56 * j - 64 * i)));
+}
+
+__device__ __forceinline__ void crt3d_block(const uint64_t* __restrict__ Y, size_t pstride, size_t ncoef,
+                                            const CrtDConsts& C, uint32_t* __restrict__ z, size_t zw, int64_t cta,
+                                            uint32_t* agg_slot)
+{
+    __shared__ uint64_t xs[3 * kCrtDSlots];
+    const int64_t i0 = cta * (int64_t)kCrtDLPC, j0 = cta * 512 - 3;
+    const int64_t climit = (int64_t)((32 * zw + 55) / 56);  // coefficients below the last word
+    for (int t = threadIdx.x; t < kCrtDSlots; t += blockDim.x) {
+        const int64_t j = j0 + t;
+        uint64_t l0 = 0, l1 = 0, l2 = 0;
+        if (j >= 0 && (size_t)j < ncoef && j < climit)
+            crt3d(C, dbits(Y[j]), dbits(Y[pstride + j]), dbits(Y[2 * pstride + j]), l0, l1, l2);
+        xs[3 * t] = l0;
+        xs[3 * t + 1] = l1;
+        xs[3 * t + 2] = l2;
+    }
+    __syncthreads();
+    uint64_t dig[kCvtLPT];
+    uint32_t gen[kCvtLPT];
+#pragma unroll
+    for (int u = 0; u < kCvtLPT; u++) {
+        const int l = threadIdx.x * kCvtLPT + u;
+        dig[u] = 0;
+        gen[u] = 0;
+        if (l < (int)kCrtDLPC) {
+            uint64_t slo, shi, plo, phi;
+            limb_windows(xs, j0, i0 + l, slo, shi);
+            limb_windows(xs, j0, i0 + l - 1, plo, phi);
+            const uint64_t d = slo + phi;
+            dig[u] = d;
+            gen[u] = d < slo;
+        }
+    }
+    const size_t zend = 2 * ((size_t)i0 + kCrtDLPC);
+    limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw < zend ? zw : zend, agg_slot);
+}
+
+__global__ void __launch_bounds__(kCvtThreads) crt3d_k1(const uint64_t* __restrict__ Y, size_t pstride,
+                                                        size_t ncoef, CrtDConsts C, uint32_t* __restrict__ z,
+                                                        size_t zw, uint32_t* agg)
+{
+    crt3d_block(Y, pstride, ncoef, C, z, zw, (int64_t)blockIdx.x, agg + blockIdx.x);
+}
+
+__global__ void __launch_bounds__(kCvtThreads) crt3d_batch_k1(const uint64_t* __restrict__ Y, size_t istride,
+                                                              size_t pstride, size_t ncoef, CrtDConsts C,
+                                                              uint32_t* __restrict__ z, uint32_t zcap,
+                                                              const uint32_t* __restrict__ zlen, size_t cpp,
+                                                              uint32_t* agg)
+{
+    const size_t prod = blockIdx.x / cpp, lc = blockIdx.x % cpp;
+    crt3d_block(Y + prod * istride, pstride, ncoef, C, z + prod * (size_t)zcap, zlen[prod], (int64_t)lc,
+                agg + blockIdx.x);
+}
+
+static size_t crt3d_ctas(size_t zw) { return ((zw + 1) / 2 + kCrtDLPC - 1) / kCrtDLPC; }
+
+// Inverse-transformed residues (product length 2^k, prime q at y + q pstride)
+// -> zw words.
+static void crt3d_to_words(const uint64_t* y, size_t pstride, int k, size_t ncoef, uint32_t* z, size_t zw,
+                           cudaStream_t s)
+{
+    const CrtDConsts C = make_crtd(k, false);
+    const size_t nctas = crt3d_ctas(zw);
+    DevBuf<uint32_t> agg(nctas, s);
+    ProfScope ps(KC_CRT, 24.0 * (double)ncoef + 4.0 * (double)zw, s);
+    crt3d_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(y, pstride, ncoef, C, z, zw, agg.get());
+    PIC_CHECK_LAUNCH();
+    count_launch();
+    carry_scan_aggregates(agg.get(), nctas, nullptr, s);
+    carry_ripple(z, zw, kCrtDWPC, agg.get(), nctas, kCarryAdd, s);
+}
+
+void ntt3d_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
+                          uint32_t zcap, const uint32_t* zlen, cudaStream_t s, size_t ncoef, bool offset)
+{
+    if (count == 0) return;
+    if (ncoef == 0) ncoef = (size_t)1 << k;
+    const CrtDConsts C = make_crtd(k, offset);
+    const size_t cpp = crt3d_ctas(zcap);
+    const size_t nctas = count * cpp;
+    DevBuf<uint32_t> agg(nctas, s);
+    {
+        ProfScope ps(KC_CRT, (24.0 * (double)ncoef + 4.0 * zcap) * (double)count, s);
+        crt3d_batch_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(y, istride, pstride, ncoef, C, z, zcap, zlen, cpp,
+                                                               agg.get());
+        PIC_CHECK_LAUNCH();
+        count_launch();
+    }
+    carry_scan_segments(agg.get(), count, cpp, s);
+    carry_ripple_batch(z, zcap, zlen, kCrtDWPC, agg.get(), count, cpp, s);
+}
+
+// The wrapped form's fix-up (see wrap_fix_kernel) on FP64 residues:
+// y[j] -= h, y[Nm + j] = h with h = d_(W-1+j) Nm / T mod p.
+__global__ void wrap_fix_d_kernel(uint64_t* __restrict__ y, size_t ystride, const uint64_t* __restrict__ tail,
+                                  size_t T, size_t nitems, size_t item_mul, size_t nchild, size_t Nm, size_t W,
+                                  DblPrimes3 P, double cw, double cwp0, double cwp1, double cwp2)
+{
+    const size_t total = 3 * nitems * W;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
+        const size_t q = g / (nitems * W);
+        const size_t r = g - q * nitems * W;
+        const size_t it = r / W, j = r - it * W;
+        const double p = q == 0 ? P.p[0] : (q == 1 ? P.p[1] : P.p[2]);
+        const double wp = q == 0 ? cwp0 : (q == 1 ? cwp1 : cwp2);
+        const size_t child = q * nchild + it * item_mul;
+        const double h = dmul_tw(dbits(tail[child * T + W - 1 + j]), cw, wp, p);
+        uint64_t* yi = y + child * ystride;
+        yi[j] = dstore(__dadd_rn(dbits(yi[j]), -h));
+        yi[Nm + j] = dstore(h);
+    }
+}
+
+void launch_wrap_fix_d(uint64_t* y, size_t ystride, const uint64_t* tail, size_t T, size_t nitems,
+                       size_t item_mul, size_t nchild, size_t Nm, size_t W, cudaStream_t s)
+{
+    const double cw = (double)(Nm / T);  // below every prime
+    wrap_fix_d_kernel<<<grid_for(3 * nitems * W, 256), 256, 0, s>>>(
+        y, ystride, tail, T, nitems, item_mul, nchild, Nm, W, dbl_primes3(), cw, cw / (double)kDblPrimes[0],
+        cw / (double)kDblPrimes[1], cw / (double)kDblPrimes[2]);
+    PIC_CHECK_LAUNCH();
+}
+
+// Largest shorter operand (in pieces) the FP64 form multiplies exactly:
+// coefficients below 2^28 (2^56 - 1)^2 < p0 p1 p2.
+constexpr size_t kDblMaxPieces = (size_t)1 << 28;
+
+static void mul_ntt3d_wrapped(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int km,
+                              int kt, cudaStream_t s)
+{
+    const size_t zw = na + nb;
+    const size_t pa = pieces56(na), pb = pieces56(nb);
+    const size_t L = pa + pb - 1;
+    const size_t Nm = (size_t)1 << km, T = (size_t)1 << kt, W = L - Nm;
+    const size_t ST = Nm + ((W + 15) & ~(size_t)15);
+    const bool square = (a == b && na == nb);
+    const uint64_t* held = is_held(b, nb) ? held_transform(km, kFormDbl, s) : nullptr;
+    DevBuf<uint64_t> A(3 * ST, s), B(square || held ? 0 : 3 * ST, s), tA(3 * T, s), tB(square ? 0 : 3 * T, s);
+    {
+        ProfScope ps(KC_SPLIT, 4.0 * (double)(na + nb) + 24.0 * (double)(2 * (Nm + T)), s);
+        if (!(held && square)) split3d(A.get(), ST, a, na, 0, Nm, s);
+        split3d(tA.get(), T, a, na, Nm - pb + 1, T, s);
+        if (!square) {
+            if (!held) split3d(B.get(), ST, b, nb, 0, Nm, s);
+            split3d(tB.get(), T, b, nb, Nm - pa + 1, T, s);
+        }
+    }
+    const NttBatch mA = ntt3d_batch_stride(A.get(), ST), mB = ntt3d_batch_stride(B.get(), ST);
+    const NttBatch xA = ntt3d_batch_stride(tA.get(), T), xB = ntt3d_batch_stride(tB.get(), T);
+    if (held && square) copy_transforms(A.get(), ST, held, Nm, km, s);
+    else ntt_forward_dif(mA, km, s);
+    ntt_forward_dif(xA, kt, s);
+    if (!square) {
+        if (!held) ntt_forward_dif(mB, km, s);
+        ntt_forward_dif(xB, kt, s);
+    }
+    if (held) ntt_pointwise_mont(mA, held, km, s, Nm);
+    else ntt_pointwise_mont(mA, square ? A.get() : B.get(), km, s);
+    ntt_pointwise_mont(xA, square ? tA.get() : tB.get(), kt, s);
+    ntt_inverse_dit(mA, km, s);
+    ntt_inverse_dit(xA, kt, s);
+    {
+        ProfScope ps(KC_NTT_POINTWISE, 3.0 * (double)W * 24.0, s);
+        launch_wrap_fix_d(A.get(), ST, tA.get(), T, 1, 1, 1, Nm, W, s);
+        count_launch();
+    }
+    crt3d_to_words(A.get(), ST, km, L, z, zw, s);
+}
+
+// The FP64 form of mul_ntt3 (PIC_MUL_NTT3D): products whose shorter operand
+// has more than 2^28 pieces go to the integer form.
+void mul_ntt3d(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s)
+{
+    if (is_held(a, na) && !(a == b && na == nb)) {  // the held operand goes second
+        std::swap(a, b);
+        std::swap(na, nb);
+    }
+    const size_t zw = na + nb;
+    const size_t pa = pieces56(na), pb = pieces56(nb);
+    if ((pa < pb ? pa : pb) > kDblMaxPieces) {
+        mul_ntt3(z, a, na, b, nb, s);
+        return;
+    }
+    const size_t ncoef = pa + pb - 1;
+    int k = ceil_log2(ncoef);
+    if (k < 1) k = 1;
+    PIC_REQUIRE(k <= 30, PIC_ERR_LENGTH, "product too long for the FP64 three-prime NTT (2^30 points)");
+    const size_t N = (size_t)1 << k;
+    if (g_mul_wrap && k >= 4) {
+        const size_t Nm = N / 2;
+        if (std::max(pa, pb) <= Nm && ncoef > Nm) {
+            const size_t W = ncoef - Nm;
+            int kt = ceil_log2(2 * W - 1);
+            if (kt < 2) kt = 2;
+            if (((size_t)1 << kt) <= Nm / 2) {
+                mul_ntt3d_wrapped(z, a, na, b, nb, k - 1, kt, s);
+                return;
+            }
+        }
+    }
+    const bool square = (a == b && na == nb);
+    const uint64_t* held = is_held(b, nb) ? held_transform(k, kFormDbl, s) : nullptr;
+    DevBuf<uint64_t> A(3 * N, s);
+    DevBuf<uint64_t> B(square || held ? 0 : 3 * N, s);
+    if (held && square) copy_transforms(A.get(), N, held, N, k, s);
+    else ntt3d_forward_operand(A.get(), k, a, na, s);
+    if (!square && !held) ntt3d_forward_operand(B.get(), k, b, nb, s);
+    ntt_pointwise_mont(ntt3d_batch_stride(A.get(), N), held ? held : (square ? A.get() : B.get()), k, s);
+    ntt_inverse_dit(ntt3d_batch_stride(A.get(), N), k, s);
+    crt3d_to_words(A.get(), N, k, ncoef, z, zw, s);
 }
 
 void mul_ntt_ref(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s)
@@ -822,13 +1204,22 @@ void mul_set_thresholds(int64_t school_max, int64_t fft_max)
 int64_t mul_school_max() { return g_school_max_words; }
 int64_t mul_fft_max() { return g_fft_max_words; }
 
+// The three-prime form AUTO and the binary splitting use (kFormInt / kFormDbl).
+static int g_ntt_form = kFormInt;
+void mul_set_ntt_form(int form)
+{
+    PIC_REQUIRE(form == kFormInt || form == kFormDbl, PIC_ERR_INVALID, "unknown product form");
+    g_ntt_form = form;
+}
+int mul_ntt_form() { return g_ntt_form; }
+
 int mul_auto_mode(size_t na, size_t nb)
 {
     const size_t mn = na < nb ? na : nb;
     const size_t zw = na + nb;
     if (zw <= kSchoolMaxWords && (mn <= 48 || (int64_t)zw <= g_school_max_words)) return PIC_MUL_SCHOOL;
     if ((int64_t)zw <= g_fft_max_words) return PIC_MUL_FFT;
-    return PIC_MUL_NTT3;
+    return g_ntt_form == kFormDbl ? PIC_MUL_NTT3D : PIC_MUL_NTT3;
 }
 
 static std::atomic<uint64_t> g_fft_err_bits{0};
@@ -882,13 +1273,15 @@ void mul_dispatch(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, 
         return;
     case PIC_MUL_NTT_REF: mul_ntt_ref(z, a, na, b, nb, s); return;
     case PIC_MUL_NTT3: mul_ntt3(z, a, na, b, nb, s); return;
+    case PIC_MUL_NTT3D: mul_ntt3d(z, a, na, b, nb, s); return;
     case PIC_MUL_FFT: {
         double e = 0;
         if (!mul_fft(z, a, na, b, nb, s, &e) || e > g_fft_accept) {
             // the NTT is the oracle: a product whose rounding distance passed
             // the acceptance threshold is redone exactly
             ctx().fft_recomputes.fetch_add(1);
-            mul_ntt3(z, a, na, b, nb, s);
+            if (g_ntt_form == kFormDbl) mul_ntt3d(z, a, na, b, nb, s);
+            else mul_ntt3(z, a, na, b, nb, s);
         }
         return;
     }

@@ -11,6 +11,21 @@ namespace pic {
 
 // Three-prime NTT: 64-bit pieces, primes kProductPrimes, Garner CRT.
 void mul_ntt3(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s);
+// The same in FP64 arithmetic: 56-bit pieces, primes kDblPrimes (fp64mod.cuh).
+void mul_ntt3d(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, size_t nb, cudaStream_t s);
+// 56-bit pieces of an operand of n words.
+size_t pieces56(size_t nwords);
+// FP64-form building blocks: split + forward into out[3 * 2^k]; batched
+// inverse output like ntt3_batch_to_words (offset 2^140 per coefficient);
+// wrapped-product fix-up like launch_wrap_fix.
+void ntt3d_forward_operand(uint64_t* out, int k, const uint32_t* a, size_t na, cudaStream_t s);
+void ntt3d_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, size_t count, int k, uint32_t* z,
+                          uint32_t zcap, const uint32_t* zlen, cudaStream_t s, size_t ncoef, bool offset);
+void launch_wrap_fix_d(uint64_t* y, size_t ystride, const uint64_t* tail, size_t T, size_t nitems,
+                       size_t item_mul, size_t nchild, size_t Nm, size_t W, cudaStream_t s);
+// The three-prime form of AUTO products and binary-splitting merges.
+void mul_set_ntt_form(int form);
+int mul_ntt_form();
 
 // While alive, three-prime products on this thread that take the operand
 // (src, n) transform it once per transform length and reuse that forward

@@ -8,6 +8,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "fp64mod.cuh"
 #include "ntt.cuh"
 
 namespace pic {
@@ -21,6 +22,14 @@ namespace pic {
 // 9p and reaches [0, 4p) with two conditional subtractions.
 const uint64_t kProductPrimes[3] = {2305842979148922881ull, 2305842949084151809ull,
                                     2305842811645198337ull};
+
+// Three primes c * 2^32 + 1 just below 2^47 (2-adicity 35, 32, 32), the FP64
+// product form's: their product is ~2^140.99, so a convolution of 56-bit
+// pieces whose shorter operand has at most 2^28 pieces (coefficients below
+// 2^140) is recovered exactly, and with the offset 2^140 so is a signed sum
+// of two products of at most 2^27 pieces.  Below 2^47, forward values up to
+// 16 p stay under 2^51, the range of the FP64 quotient.
+const uint64_t kDblPrimes[3] = {140496970186753ull, 140458315481089ull, 140449725546497ull};
 
 // The reference's prime table, NTT.cpp:125-158.  The transform length picks
 // the prime, so natural-order outputs only match if the values match.
@@ -180,6 +189,86 @@ const PrimeTables& prime_tables(uint64_t p)
     return *t;
 }
 
+static void dbl_pairs(std::vector<uint64_t>& v, size_t i, uint64_t w, uint64_t p)
+{
+    const double wd = (double)w, wp = wd / (double)p;
+    memcpy(&v[2 * i], &wd, 8);
+    memcpy(&v[2 * i + 1], &wp, 8);
+}
+
+const PrimeTables& dbl_prime_tables(uint64_t p)
+{
+    PIC_REQUIRE(p < (1ull << 47) && p > (1ull << 40), PIC_ERR_INVALID, "FP64 primes lie in (2^40, 2^47)");
+    std::lock_guard<std::mutex> g(g_tab_lock);
+    auto it = g_tabs.find(p);
+    if (it != g_tabs.end()) return *it->second;
+    PrimeTables* t = new PrimeTables();
+    t->p = p;
+    t->g = smallest_generator(p);
+    int v = 0;
+    while (((p - 1) >> v & 1) == 0) v++;
+    t->adicity = v;
+    PIC_REQUIRE(v >= kInnerBits, PIC_ERR_INVALID, "FP64 prime without roots of order 2^13");
+    const int K = v < 32 ? v : 32;
+    const int S = (K + 1) / 2;
+    const int IB = kInnerBits;
+    const uint64_t wK = host_powmod(t->g, (p - 1) >> K, p);
+    const uint64_t wKi = host_powmod(wK, p - 2, p);
+    const uint64_t wI = host_powmod(wK, (uint64_t)1 << (K - IB), p);
+    const uint64_t wIi = host_powmod(wKi, (uint64_t)1 << (K - IB), p);
+    // per-level inner tables: the root of order 2^m is wI^(2^(IB - m)); pair
+    // 2^(m-1) - 1 + e holds its e-th power
+    std::vector<uint64_t> lf((size_t)2 << IB), li((size_t)2 << IB);
+    for (int lm = 1; lm <= IB; lm++) {
+        const uint64_t r = host_powmod(wI, (uint64_t)1 << (IB - lm), p);
+        const uint64_t ri = host_powmod(wIi, (uint64_t)1 << (IB - lm), p);
+        uint64_t a = 1, b = 1;
+        for (size_t e = 0; e < ((size_t)1 << (lm - 1)); e++) {
+            const size_t dst = ((size_t)1 << (lm - 1)) - 1 + e;
+            dbl_pairs(lf, dst, a, p);
+            dbl_pairs(li, dst, b, p);
+            a = host_mulmod(a, r, p);
+            b = host_mulmod(b, ri, p);
+        }
+    }
+    // two-level outer tables: root_(2^K)^i (i < 2^S) and root_(2^K)^(i 2^S)
+    std::vector<uint64_t> lof((size_t)2 << S), loi((size_t)2 << S);
+    std::vector<uint64_t> hif((size_t)2 << (K - S)), hii((size_t)2 << (K - S));
+    uint64_t a = 1, b = 1;
+    for (size_t i = 0; i < ((size_t)1 << S); i++) {
+        dbl_pairs(lof, i, a, p);
+        dbl_pairs(loi, i, b, p);
+        a = host_mulmod(a, wK, p);
+        b = host_mulmod(b, wKi, p);
+    }
+    const uint64_t wS = a, wSi = b;
+    a = 1, b = 1;
+    for (size_t i = 0; i < ((size_t)1 << (K - S)); i++) {
+        dbl_pairs(hif, i, a, p);
+        dbl_pairs(hii, i, b, p);
+        a = host_mulmod(a, wS, p);
+        b = host_mulmod(b, wSi, p);
+    }
+    PrimeDev& d = t->dev;
+    memset(&d, 0, sizeof d);
+    d.p = p;
+    d.K = K;
+    d.S = S;
+    d.IB = IB;
+    d.lazy = 0;
+    d.fp64 = 1;
+    d.pd = (double)p;
+    d.pinv = 1.0 / (double)p;
+    d.slo_fwd = upload(lof);
+    d.shi_fwd = upload(hif);
+    d.slo_inv = upload(loi);
+    d.shi_inv = upload(hii);
+    d.lvl_fwd = upload(lf);
+    d.lvl_inv = upload(li);
+    g_tabs[p] = t;
+    return *t;
+}
+
 // Per-length geometry (tunable; pic_set_ntt_geometry): row-pass bits, column
 // tile width (log2 columns per CTA, 0 = automatic) and bits per register round
 // (radix 2^rbits).
@@ -188,28 +277,34 @@ struct Geometry {
     int col_lw = 0;
     int rbits = 3;
 };
-static Geometry g_geom[33];
+static Geometry g_geom_forms[2][33];
 
-void ntt_set_geometry(int k, int row_bits, int col_lw, int rbits)
+static const Geometry& geom_of(const NttBatch& b, int k) { return g_geom_forms[b.prime[0].fp64 ? 1 : 0][k]; }
+
+void ntt_set_geometry(int k, int row_bits, int col_lw, int rbits, int form)
 {
+    PIC_REQUIRE(form == kFormInt || form == kFormDbl, PIC_ERR_INVALID, "unknown product form");
     PIC_REQUIRE(k >= 1 && k <= 32, PIC_ERR_INVALID, "k out of range");
-    PIC_REQUIRE(row_bits >= 8 && row_bits <= kInnerBits, PIC_ERR_INVALID, "row bits out of range (8..13)");
+    PIC_REQUIRE(row_bits >= (form == kFormDbl ? 11 : 8) && row_bits <= kInnerBits, PIC_ERR_INVALID,
+                "row bits out of range (8..13; FP64 form 11..13)");
     PIC_REQUIRE(col_lw >= 0 && col_lw <= 6, PIC_ERR_INVALID, "column width out of range (0..6)");
-    PIC_REQUIRE(rbits >= 2 && rbits <= 4, PIC_ERR_INVALID, "radix bits out of range (2..4)");
-    g_geom[k].row_bits = row_bits;
-    g_geom[k].col_lw = col_lw;
-    g_geom[k].rbits = rbits;
+    PIC_REQUIRE(rbits >= (form == kFormDbl ? 3 : 2) && rbits <= 4, PIC_ERR_INVALID,
+                "radix bits out of range (2..4; FP64 form 3..4)");
+    Geometry& g = g_geom_forms[form][k];
+    g.row_bits = row_bits;
+    g.col_lw = col_lw;
+    g.rbits = rbits;
 }
 
-void ntt_get_geometry(int k, int* row_bits, int* col_lw, int* rbits)
+void ntt_get_geometry(int k, int* row_bits, int* col_lw, int* rbits, int form)
 {
-    const Geometry& g = g_geom[k < 1 ? 1 : (k > 32 ? 32 : k)];
+    const Geometry& g = g_geom_forms[form == kFormDbl ? 1 : 0][k < 1 ? 1 : (k > 32 ? 32 : k)];
     *row_bits = g.row_bits;
     *col_lw = g.col_lw;
     *rbits = g.rbits;
 }
 
-std::vector<int> ntt_pass_bits(int k)
+std::vector<int> ntt_pass_bits(int k, int form)
 {
     // One in-CTA pass up to 2^13 points; then column passes of at most 11
     // bits (balanced) and the row pass.
@@ -218,7 +313,7 @@ std::vector<int> ntt_pass_bits(int k)
         bits.push_back(k);
         return bits;
     }
-    const int row = g_geom[k].row_bits, colmax = 11;
+    const int row = g_geom_forms[form == kFormDbl ? 1 : 0][k].row_bits, colmax = 11;
     int rest = k - row;
     const int ncol = (rest + colmax - 1) / colmax;
     for (int i = 0; i < ncol; i++) {
@@ -673,12 +768,88 @@ __device__ __forceinline__ void fbfly_unit_dit(uint64_t& a, uint64_t& b, const L
     b = x + L.p4 - y;
 }
 
+// Arithmetic of the fast passes.  ArithInt: lazy Shoup butterflies on 64-bit
+// residues (lazy primes).  ArithDbl: FP64 butterflies (FP64 primes, values
+// stored as the bits of doubles).  `LAST` marks the last level of a register
+// round: the FP64 forward butterflies reduce their sums there, so every
+// round starts and ends with |x| <= 0.75 p; inside a round of B levels the
+// values stay below 2^B 0.75 p (12 p for radix-16, under 2^51).  FP64
+// inverse butterflies add at most 0.75 p per level and never reduce: a pass
+// of L levels over inputs below X ends below 2 X + (L - 1) 0.75 p.
+struct ArithInt {
+    using T = uint64_t;
+    using Ctx = LazyPrime;
+    static __device__ __forceinline__ Ctx ctx(const PrimeDev& P) { return lazy_prime(P); }
+    static __device__ __forceinline__ T ld(uint64_t v) { return v; }
+    static __device__ __forceinline__ uint64_t st(T v) { return v; }
+    template <bool LAST>
+    static __device__ __forceinline__ void dif(T& a, T& b, const ulonglong2 t, const Ctx& L) { fbfly_dif(a, b, t, L); }
+    template <bool LAST>
+    static __device__ __forceinline__ void dif_unit(T& a, T& b, const Ctx& L) { fbfly_unit_dif(a, b, L); }
+    static __device__ __forceinline__ void dit(T& a, T& b, const ulonglong2 t, const Ctx& L) { fbfly_dit(a, b, t, L); }
+    static __device__ __forceinline__ void dit_unit(T& a, T& b, const Ctx& L) { fbfly_unit_dit(a, b, L); }
+    // v * w (pass twiddle) into [0, 4p) from any 64-bit v
+    static __device__ __forceinline__ T twiddle(T v, const ulonglong2 t, const Ctx& L)
+    {
+        return shoup_approx32(v, t.x, t.y, L.c);
+    }
+    // piece j of the item's child words, as a residue
+    static __device__ __forceinline__ T piece(const NttBatch& B, const SrcRow& r, size_t j, const Ctx& L)
+    {
+        return src_piece(B, r, j, L.p4);
+    }
+};
+
+struct ArithDbl {
+    using T = double;
+    struct Ctx {
+        double p, pinv;
+    };
+    static __device__ __forceinline__ Ctx ctx(const PrimeDev& P) { return Ctx{P.pd, P.pinv}; }
+    static __device__ __forceinline__ T ld(uint64_t v) { return dbits(v); }
+    static __device__ __forceinline__ uint64_t st(T v) { return dstore(v); }
+    template <bool LAST>
+    static __device__ __forceinline__ void dif(T& a, T& b, const ulonglong2 t, const Ctx& L)
+    {
+        const double s = __dadd_rn(a, b), d = __dadd_rn(a, -b);
+        b = dmul_tw(d, dbits(t.x), dbits(t.y), L.p);
+        a = LAST ? dreduce(s, L.p, L.pinv) : s;
+    }
+    template <bool LAST>
+    static __device__ __forceinline__ void dif_unit(T& a, T& b, const Ctx& L)
+    {
+        const double s = __dadd_rn(a, b), d = __dadd_rn(a, -b);
+        a = LAST ? dreduce(s, L.p, L.pinv) : s;
+        b = LAST ? dreduce(d, L.p, L.pinv) : d;
+    }
+    static __device__ __forceinline__ void dit(T& a, T& b, const ulonglong2 t, const Ctx& L)
+    {
+        const double u = dmul_tw(b, dbits(t.x), dbits(t.y), L.p);
+        b = __dadd_rn(a, -u);
+        a = __dadd_rn(a, u);
+    }
+    static __device__ __forceinline__ void dit_unit(T& a, T& b, const Ctx&)
+    {
+        const double s = __dadd_rn(a, b);
+        b = __dadd_rn(a, -b);
+        a = s;
+    }
+    static __device__ __forceinline__ T twiddle(T v, const ulonglong2 t, const Ctx& L)
+    {
+        return dmul_tw(v, dbits(t.x), dbits(t.y), L.p);
+    }
+    static __device__ __forceinline__ T piece(const NttBatch& B, const SrcRow& r, size_t j, const Ctx& L)
+    {
+        return dpiece56(src_piece56_raw(r.x, r.n, B.src.first + j), L.p, L.pinv);
+    }
+};
+
 // The B levels of one group (elements base + j + m 2^LST, m < 2^B) with the
 // per-level inner tables: the twiddle of butterfly u at group level l is
 // root_(2^(B-l+LST))^(j + u 2^LST), pair 2^(B-l+LST-1) - 1 + j + u 2^LST, so
 // lanes with consecutive j read consecutive pairs.
-template <int B, bool INV, int LST>
-__device__ __forceinline__ void group_fast(uint64_t (&x)[1 << B], int j, const LazyPrime& L,
+template <int B, bool INV, int LST, class A>
+__device__ __forceinline__ void group_fast(typename A::T (&x)[1 << B], int j, const typename A::Ctx& L,
                                            const ulonglong2* __restrict__ tw)
 {
     static_assert(B + LST <= 13, "sub-block larger than the inner table");
@@ -688,14 +859,16 @@ __device__ __forceinline__ void group_fast(uint64_t (&x)[1 << B], int j, const L
             const int hm = 1 << (B - 1 - l);
             if (l == B - 1 && LST == 0) {
 #pragma unroll
-                for (int m = 0; m < (1 << B); m += 2) fbfly_unit_dif(x[m], x[m + 1], L);
+                for (int m = 0; m < (1 << B); m += 2) A::template dif_unit<true>(x[m], x[m + 1], L);
                 continue;
             }
 #pragma unroll
             for (int m = 0; m < (1 << B); m++) {
                 if (m & hm) continue;
                 const int u = m & (hm - 1);
-                fbfly_dif(x[m], x[m + hm], __ldg(tw + ((1 << (B - l + LST - 1)) - 1) + j + (u << LST)), L);
+                const ulonglong2 t = __ldg(tw + ((1 << (B - l + LST - 1)) - 1) + j + (u << LST));
+                if (l == B - 1) A::template dif<true>(x[m], x[m + hm], t, L);
+                else A::template dif<false>(x[m], x[m + hm], t, L);
             }
         }
     } else {
@@ -704,14 +877,14 @@ __device__ __forceinline__ void group_fast(uint64_t (&x)[1 << B], int j, const L
             const int hm = 1 << (B - 1 - l);
             if (l == B - 1 && LST == 0) {
 #pragma unroll
-                for (int m = 0; m < (1 << B); m += 2) fbfly_unit_dit(x[m], x[m + 1], L);
+                for (int m = 0; m < (1 << B); m += 2) A::dit_unit(x[m], x[m + 1], L);
                 continue;
             }
 #pragma unroll
             for (int m = 0; m < (1 << B); m++) {
                 if (m & hm) continue;
                 const int u = m & (hm - 1);
-                fbfly_dit(x[m], x[m + hm], __ldg(tw + ((1 << (B - l + LST - 1)) - 1) + j + (u << LST)), L);
+                A::dit(x[m], x[m + hm], __ldg(tw + ((1 << (B - l + LST - 1)) - 1) + j + (u << LST)), L);
             }
         }
     }
@@ -734,14 +907,14 @@ struct RoundPlan {
 // Row layout: transform t of the CTA at s + (t << LR), element e at swz(e).
 // With several transforms per CTA (LRPC > 0, single-pass lengths), each
 // group takes the prime of its own transform: a CTA may straddle primes.
-template <bool INV, int LR, int LRPC, int NT, int RB, int R>
+template <bool INV, int LR, int LRPC, int NT, int RB, int R, class A>
 __device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const NttBatch& Bt, size_t row0,
-                                                const LazyPrime& L0, const ulonglong2* __restrict__ tw0)
+                                                const typename A::Ctx& L0, const ulonglong2* __restrict__ tw0)
 {
     using Plan = RoundPlan<LR, RB>;
     constexpr int RR = INV ? Plan::NR - 1 - R : R;
-    using A = typename Plan::template At<RR>;
-    constexpr int B = A::B, LB = A::LB, LST = A::LST;
+    using At = typename Plan::template At<RR>;
+    constexpr int B = At::B, LB = At::LB, LST = At::LST;
     constexpr int LG = LR - B;  // log2 groups per transform
     constexpr int G = 1 << (LRPC + LG);
     static_assert(G % NT == 0, "groups must split evenly over the threads");
@@ -752,22 +925,22 @@ __device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const 
         const int j = gi & ((1 << LST) - 1);
         const int base = ((gi >> LST) << LB) + j;
         uint64_t* ptr = s + (t << LR);
-        LazyPrime L = L0;
+        typename A::Ctx L = L0;
         const ulonglong2* tw = tw0;
         if (LRPC > 0 && row0 + t < (size_t)Bt.count) {  // rows past the batch keep the CTA's prime
             const PrimeDev Pt = pick_prime(Bt, (int)(row0 + t));
-            L = lazy_prime(Pt);
+            L = A::ctx(Pt);
             tw = reinterpret_cast<const ulonglong2*>(INV ? Pt.lvl_inv : Pt.lvl_fwd);
         }
-        uint64_t x[1 << B];
+        typename A::T x[1 << B];
 #pragma unroll
-        for (int m = 0; m < (1 << B); m++) x[m] = ptr[swz(base + (m << LST))];
-        group_fast<B, INV, LST>(x, j, L, tw);
+        for (int m = 0; m < (1 << B); m++) x[m] = A::ld(ptr[swz(base + (m << LST))]);
+        group_fast<B, INV, LST, A>(x, j, L, tw);
 #pragma unroll
-        for (int m = 0; m < (1 << B); m++) ptr[swz(base + (m << LST))] = x[m];
+        for (int m = 0; m < (1 << B); m++) ptr[swz(base + (m << LST))] = A::st(x[m]);
     }
     __syncthreads();
-    if constexpr (R + 1 < Plan::NR) rows_fast_round<INV, LR, LRPC, NT, RB, R + 1>(s, Bt, row0, L0, tw0);
+    if constexpr (R + 1 < Plan::NR) rows_fast_round<INV, LR, LRPC, NT, RB, R + 1, A>(s, Bt, row0, L0, tw0);
 }
 
 // One thread per group of a full round: 2^(LR + LRPC - RB) threads, at most
@@ -783,7 +956,7 @@ struct RowsFastShape {
 // Contiguous row pass: 2^LRPC rows of 2^LR points per CTA.  LRPC > 0 only
 // for single-pass lengths (k = LR, one row per transform); the last CTA may
 // hold fewer than 2^LRPC transforms.
-template <bool INV, int LR, int LRPC, int RB>
+template <bool INV, int LR, int LRPC, int RB, class A>
 __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape<LR, LRPC, RB>::MINB)
     ntt_rows_fast_kernel(NttBatch B, int k)
 {
@@ -795,7 +968,7 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape
     const size_t row0 = (size_t)blockIdx.x << LRPC;
     const size_t nrows = (size_t)B.count << lrow;
     const PrimeDev P = pick_prime(B, (int)(row0 >> lrow));
-    const LazyPrime L = lazy_prime(P);
+    const typename A::Ctx L = A::ctx(P);
     if (!INV && B.src.words != nullptr) {
         // first forward pass of a single-pass length (row == transform): the
         // input comes from the child slots
@@ -806,8 +979,7 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape
             uint64_t v = 0;
             if (LRPC == 0 || row < nrows) {
                 const int tr = (int)row;
-                const uint64_t p4 = 4 * pick_prime(B, tr).p;
-                v = src_piece(B, src_row(B, tr), idx & EMASK, p4);
+                v = A::st(A::piece(B, src_row(B, tr), idx & EMASK, A::ctx(pick_prime(B, tr))));
             }
             smem[(idx & ~EMASK) + swz(idx & EMASK)] = v;
         }
@@ -823,8 +995,8 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape
         }
     }
     __syncthreads();
-    rows_fast_round<INV, LR, LRPC, NT, RB, 0>(smem, B, row0, L,
-                                          reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
+    rows_fast_round<INV, LR, LRPC, NT, RB, 0, A>(smem, B, row0, L,
+                                             reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
 #pragma unroll
     for (int i = 0; i < TOT / NT; i++) {
         const int idx = threadIdx.x + i * NT;
@@ -837,14 +1009,14 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape
 
 // Column tile: 2^LC rows x 2^LW columns, element (m, w) at s[(m << LW) + w];
 // consecutive threads take consecutive columns.
-template <bool INV, int LC, int LW, int RB, int R>
-__device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const LazyPrime& L,
+template <bool INV, int LC, int LW, int RB, int R, class A>
+__device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const typename A::Ctx& L,
                                                 const ulonglong2* __restrict__ tw)
 {
     using Plan = RoundPlan<LC, RB>;
     constexpr int RR = INV ? Plan::NR - 1 - R : R;
-    using A = typename Plan::template At<RR>;
-    constexpr int B = A::B, LB = A::LB, LST = A::LST;
+    using At = typename Plan::template At<RR>;
+    constexpr int B = At::B, LB = At::LB, LST = At::LST;
     constexpr int LG = LC - B;  // log2 groups per column
     constexpr int G = 1 << (LW + LG);
     constexpr int WMASK = (1 << LW) - 1;
@@ -853,15 +1025,15 @@ __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const 
         const int w = g & WMASK, gi = g >> LW;
         const int j = gi & ((1 << LST) - 1);
         const int base = ((gi >> LST) << LB) + j;
-        uint64_t x[1 << B];
+        typename A::T x[1 << B];
 #pragma unroll
-        for (int m = 0; m < (1 << B); m++) x[m] = s[((base + (m << LST)) << LW) + w];
-        group_fast<B, INV, LST>(x, j, L, tw);
+        for (int m = 0; m < (1 << B); m++) x[m] = A::ld(s[((base + (m << LST)) << LW) + w]);
+        group_fast<B, INV, LST, A>(x, j, L, tw);
 #pragma unroll
-        for (int m = 0; m < (1 << B); m++) s[((base + (m << LST)) << LW) + w] = x[m];
+        for (int m = 0; m < (1 << B); m++) s[((base + (m << LST)) << LW) + w] = A::st(x[m]);
     }
     __syncthreads();
-    if constexpr (R + 1 < Plan::NR) cols_fast_round<INV, LC, LW, RB, R + 1>(s, L, tw);
+    if constexpr (R + 1 < Plan::NR) cols_fast_round<INV, LC, LW, RB, R + 1, A>(s, L, tw);
 }
 
 // floor(x 2^64 / p) for x < p: q' = floor(x mu / 2^64) with mu = floor(2^128 /
@@ -874,8 +1046,9 @@ __device__ __forceinline__ uint64_t shoup_companion_dev(uint64_t x, uint64_t p, 
 }
 
 // Pass twiddle tables: for a column pass over blocks of 2^lblock points split
-// 2^LC x M, entry m M + c = root_(2^lblock)^(+-c brev_LC(m)) as a Shoup pair,
-// laid out like the data so the pass streams it with the same coalescing.
+// 2^LC x M, entry m M + c = root_(2^lblock)^(+-c brev_LC(m)) as a Shoup pair
+// (FP64 primes: the pair (w, fl(w / p)) of doubles), laid out like the data
+// so the pass streams it with the same coalescing.
 struct PassTw {
     const ulonglong2* t[kMaxPrimesPerBatch];
 };
@@ -885,7 +1058,6 @@ __global__ void pass_table_kernel(ulonglong2* __restrict__ out, PrimeDev P, int 
     const size_t n = (size_t)1 << lblock;
     const int lM = lblock - lc;
     const int esh = P.K - lblock;
-    const LazyPrime L = lazy_prime(P);
     const ulonglong2* slo = reinterpret_cast<const ulonglong2*>(inv ? P.slo_inv : P.slo_fwd);
     const ulonglong2* shi = reinterpret_cast<const ulonglong2*>(inv ? P.shi_inv : P.shi_fwd);
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
@@ -893,6 +1065,12 @@ __global__ void pass_table_kernel(ulonglong2* __restrict__ out, PrimeDev P, int 
         const uint64_t k1 = __brev((unsigned)m) >> (32 - lc);
         const uint64_t E = (c * k1) << esh;
         const ulonglong2 h = __ldg(shi + (E >> P.S)), l = __ldg(slo + (E & (((uint64_t)1 << P.S) - 1)));
+        if (P.fp64) {
+            const double x = dcanon(dmul_tw(dbits(h.x), dbits(l.x), dbits(l.y), P.pd), P.pd);
+            out[g] = make_ulonglong2(dstore(x), dstore(__ddiv_rn(x, P.pd)));
+            continue;
+        }
+        const LazyPrime L = lazy_prime(P);
         uint64_t x = shoup_lazy32(h.x, l.x, l.y, L.c);
         x = x >= L.p ? x - L.p : x;
         out[g] = make_ulonglong2(x, shoup_companion_dev(x, L.p, P.mu_hi, P.mu_lo));
@@ -900,11 +1078,11 @@ __global__ void pass_table_kernel(ulonglong2* __restrict__ out, PrimeDev P, int 
 }
 
 // Strided column pass (same tiling as ntt_cols_kernel).  The inter-pass
-// twiddle root_(2^lblock)^((c0 + w) k1) is applied as two Shoup products
-// with the two-level outer tables: forward after the column DIF, inverse
-// before the column DIT.
+// twiddle root_(2^lblock)^((c0 + w) k1) is applied as one product with the
+// pass table, or as two with the two-level outer tables: forward after the
+// column DIF, inverse before the column DIT.
 // RB 4: radix-16 rounds, 16 residues per thread, two CTAs per SM.
-template <bool INV, int LC, int LW, int RB>
+template <bool INV, int LC, int LW, int RB, class A>
 __global__ void __launch_bounds__(256, RB == 4 ? 2 : (INV ? 3 : 4))
     ntt_cols_fast_kernel(NttBatch B, int k, int lpre, PassTw pt)
 {
@@ -918,7 +1096,7 @@ __global__ void __launch_bounds__(256, RB == 4 ? 2 : (INV ? 3 : 4))
     const size_t ob = rem >> ltiles;
     const uint32_t c0 = (uint32_t)((rem & (((size_t)1 << ltiles) - 1)) << LW);
     const PrimeDev P = pick_prime(B, tr);
-    const LazyPrime L = lazy_prime(P);
+    const typename A::Ctx L = A::ctx(P);
     uint64_t* base = B.data + (size_t)tr * B.stride + (ob << (k - lpre)) + c0;
     const int esh = P.K - (k - lpre);  // exponents of a root of order 2^(k - lpre), scaled to order 2^K
     const int S = P.S;
@@ -926,15 +1104,13 @@ __global__ void __launch_bounds__(256, RB == 4 ? 2 : (INV ? 3 : 4))
     const ulonglong2* __restrict__ slo = reinterpret_cast<const ulonglong2*>(INV ? P.slo_inv : P.slo_fwd);
     const ulonglong2* __restrict__ shi = reinterpret_cast<const ulonglong2*>(INV ? P.shi_inv : P.shi_fwd);
     const ulonglong2* __restrict__ T = tr < B.per_prime ? pt.t[0] : (tr < 2 * B.per_prime ? pt.t[1] : pt.t[2]);
-    auto twiddle = [&](uint64_t v, int m, int w) {
-        if (T != nullptr) {  // the pass table: one Shoup product, streamed like the data
-            const ulonglong2 t = __ldg(T + ((size_t)m << lM) + c0 + w);
-            return shoup_approx32(v, t.x, t.y, L.c);
-        }
+    auto twiddle = [&](typename A::T v, int m, int w) {
+        if (T != nullptr)  // the pass table: one product, streamed like the data
+            return A::twiddle(v, __ldg(T + ((size_t)m << lM) + c0 + w), L);
         const uint64_t k1 = __brev((unsigned)m) >> (32 - LC);
         const uint64_t E = ((uint64_t)(c0 + w) * k1) << esh;
         const ulonglong2 h = __ldg(shi + (E >> S)), l = __ldg(slo + (E & smask));
-        return shoup_approx32(shoup_approx32(v, h.x, h.y, L.c), l.x, l.y, L.c);
+        return A::twiddle(A::twiddle(v, h, L), l, L);
     };
     if (!INV && B.src.words != nullptr) {
         // first forward column pass (lpre == 0): the input comes from the
@@ -943,24 +1119,25 @@ __global__ void __launch_bounds__(256, RB == 4 ? 2 : (INV ? 3 : 4))
 #pragma unroll 8
         for (int idx = threadIdx.x; idx < TOT; idx += 256) {
             const int m = idx >> LW, w = idx & WMASK;
-            smem[idx] = src_piece(B, sr, ((size_t)m << lM) + c0 + w, L.p4);
+            smem[idx] = A::st(A::piece(B, sr, ((size_t)m << lM) + c0 + w, L));
         }
     } else {
 #pragma unroll 8
         for (int idx = threadIdx.x; idx < TOT; idx += 256) {
             const int m = idx >> LW, w = idx & WMASK;
             uint64_t v = base[((size_t)m << lM) + w];
-            if (INV) v = twiddle(v, m, w);
+            if (INV) v = A::st(twiddle(A::ld(v), m, w));
             smem[idx] = v;
         }
     }
     __syncthreads();
-    cols_fast_round<INV, LC, LW, RB, 0>(smem, L, reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
+    cols_fast_round<INV, LC, LW, RB, 0, A>(smem, L,
+                                           reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
 #pragma unroll 8
     for (int idx = threadIdx.x; idx < TOT; idx += 256) {
         const int m = idx >> LW, w = idx & WMASK;
         uint64_t v = smem[idx];
-        if (!INV) v = twiddle(v, m, w);
+        if (!INV) v = A::st(twiddle(A::ld(v), m, w));
         base[((size_t)m << lM) + w] = v;
     }
 }
@@ -974,7 +1151,12 @@ __global__ void src_split_kernel(NttBatch B, int k)
         const int tr = (int)(g >> k);
         const size_t j = g & (N - 1);
         const PrimeDev P = pick_prime(B, tr);
-        const uint64_t v = src_piece_raw(B, src_row(B, tr), j);
+        const SrcRow r = src_row(B, tr);
+        if (P.fp64) {
+            B.data[(size_t)tr * B.stride + j] = dstore(dpiece56(src_piece56_raw(r.x, r.n, B.src.first + j), P.pd, P.pinv));
+            continue;
+        }
+        const uint64_t v = src_piece_raw(B, r, j);
         B.data[(size_t)tr * B.stride + j] = P.lazy ? piece_to_strict(v, P.p) : v % P.p;
     }
 }
@@ -999,9 +1181,11 @@ static void set_smem(K kern, size_t smem)
 // of 2^11 .. 2^13 points and columns of 2^8 .. 2^11 rows.
 static bool fast_ok(const NttBatch& b, int k)
 {
-    if (!PIC_NTT_FAST || (g_geom[k].rbits != 3 && g_geom[k].rbits != 4)) return false;
+    const int rb = geom_of(b, k).rbits;
+    if (!(PIC_NTT_FAST || b.prime[0].fp64) || (rb != 3 && rb != 4)) return false;
     for (int q = 0; q * b.per_prime < b.count; q++)
-        if (!b.prime[q].lazy || b.prime[q].IB != 13 || b.prime[q].lvl_fwd == nullptr ||
+        if (!(b.prime[q].lazy || b.prime[q].fp64) || b.prime[q].fp64 != b.prime[0].fp64 || b.prime[q].IB != 13 ||
+            b.prime[q].lvl_fwd == nullptr ||
             (q > 0 && (b.prime[q].slo_fwd == nullptr) != (b.prime[0].slo_fwd == nullptr)))
             return false;
     return true;
@@ -1009,7 +1193,7 @@ static bool fast_ok(const NttBatch& b, int k)
 
 constexpr int fast_lrpc(int lr) { return lr < 11 ? 11 - lr : 0; }
 
-template <bool INV, int LR, int RB = 3>
+template <bool INV, int LR, int RB, class A>
 static void launch_rows_fast_t(const NttBatch& b, int k, cudaStream_t s)
 {
     constexpr int LRPC = fast_lrpc(LR);
@@ -1017,36 +1201,36 @@ static void launch_rows_fast_t(const NttBatch& b, int k, cudaStream_t s)
     const size_t rows = (size_t)b.count << (k - LR);
     const size_t grid = (rows + ((size_t)1 << LRPC) - 1) >> LRPC;
     const size_t smem = sizeof(uint64_t) * Sh::TOT;
-    set_smem(ntt_rows_fast_kernel<INV, LR, LRPC, RB>, smem);
-    ntt_rows_fast_kernel<INV, LR, LRPC, RB><<<(unsigned)grid, Sh::NT, smem, s>>>(b, k);
+    set_smem(ntt_rows_fast_kernel<INV, LR, LRPC, RB, A>, smem);
+    ntt_rows_fast_kernel<INV, LR, LRPC, RB, A><<<(unsigned)grid, Sh::NT, smem, s>>>(b, k);
 }
 
-template <bool INV>
+template <bool INV, class A>
 static bool launch_rows_fast(const NttBatch& b, int k, int lr, cudaStream_t s)
 {
     if (!(lr == k || lr >= 11)) return false;
-    if (g_geom[k].rbits == 4) {
+    if (geom_of(b, k).rbits == 4) {
         switch (lr) {
-        case 11: launch_rows_fast_t<INV, 11, 4>(b, k, s); return true;
-        case 12: launch_rows_fast_t<INV, 12, 4>(b, k, s); return true;
-        case 13: launch_rows_fast_t<INV, 13, 4>(b, k, s); return true;
+        case 11: launch_rows_fast_t<INV, 11, 4, A>(b, k, s); return true;
+        case 12: launch_rows_fast_t<INV, 12, 4, A>(b, k, s); return true;
+        case 13: launch_rows_fast_t<INV, 13, 4, A>(b, k, s); return true;
         default: break;  // shorter rows keep radix-8 rounds
         }
     }
     switch (lr) {
-    case 1: launch_rows_fast_t<INV, 1>(b, k, s); break;
-    case 2: launch_rows_fast_t<INV, 2>(b, k, s); break;
-    case 3: launch_rows_fast_t<INV, 3>(b, k, s); break;
-    case 4: launch_rows_fast_t<INV, 4>(b, k, s); break;
-    case 5: launch_rows_fast_t<INV, 5>(b, k, s); break;
-    case 6: launch_rows_fast_t<INV, 6>(b, k, s); break;
-    case 7: launch_rows_fast_t<INV, 7>(b, k, s); break;
-    case 8: launch_rows_fast_t<INV, 8>(b, k, s); break;
-    case 9: launch_rows_fast_t<INV, 9>(b, k, s); break;
-    case 10: launch_rows_fast_t<INV, 10>(b, k, s); break;
-    case 11: launch_rows_fast_t<INV, 11>(b, k, s); break;
-    case 12: launch_rows_fast_t<INV, 12>(b, k, s); break;
-    case 13: launch_rows_fast_t<INV, 13>(b, k, s); break;
+    case 1: launch_rows_fast_t<INV, 1, 3, A>(b, k, s); break;
+    case 2: launch_rows_fast_t<INV, 2, 3, A>(b, k, s); break;
+    case 3: launch_rows_fast_t<INV, 3, 3, A>(b, k, s); break;
+    case 4: launch_rows_fast_t<INV, 4, 3, A>(b, k, s); break;
+    case 5: launch_rows_fast_t<INV, 5, 3, A>(b, k, s); break;
+    case 6: launch_rows_fast_t<INV, 6, 3, A>(b, k, s); break;
+    case 7: launch_rows_fast_t<INV, 7, 3, A>(b, k, s); break;
+    case 8: launch_rows_fast_t<INV, 8, 3, A>(b, k, s); break;
+    case 9: launch_rows_fast_t<INV, 9, 3, A>(b, k, s); break;
+    case 10: launch_rows_fast_t<INV, 10, 3, A>(b, k, s); break;
+    case 11: launch_rows_fast_t<INV, 11, 3, A>(b, k, s); break;
+    case 12: launch_rows_fast_t<INV, 12, 3, A>(b, k, s); break;
+    case 13: launch_rows_fast_t<INV, 13, 3, A>(b, k, s); break;
     default: return false;
     }
     return true;
@@ -1064,9 +1248,16 @@ constexpr int kPassTableMaxBits = 24;
 static std::mutex g_pass_lock;
 static std::map<std::tuple<int, uint64_t, int, int, int>, ulonglong2*> g_pass_tables;
 
+// FP64 column passes stream the per-point table only when this is set: their
+// FP64 pipe has room to form each twiddle from the two-level tables (two
+// products), which saves 16 bytes of DRAM traffic per point.
+static bool g_dbl_pass_tables = false;
+void ntt_set_dbl_pass_tables(bool on) { g_dbl_pass_tables = on; }
+bool ntt_dbl_pass_tables() { return g_dbl_pass_tables; }
+
 static const ulonglong2* pass_table(const PrimeDev& P, bool inv, int lblock, int lc, cudaStream_t s)
 {
-    if (lblock > kPassTableMaxBits) return nullptr;
+    if (lblock > kPassTableMaxBits || (P.fp64 && !g_dbl_pass_tables)) return nullptr;
     int dev = 0;
     PIC_CUDA(cudaGetDevice(&dev));
     const auto key = std::make_tuple(dev, P.p, inv ? 1 : 0, lblock, lc);
@@ -1088,7 +1279,7 @@ static const ulonglong2* pass_table(const PrimeDev& P, bool inv, int lblock, int
     return d;
 }
 
-template <bool INV, int LC, int LW, int RB>
+template <bool INV, int LC, int LW, int RB, class A>
 static void launch_cols_fast_t(const NttBatch& b, int k, int lpre, size_t grid, cudaStream_t s)
 {
     constexpr size_t smem = sizeof(uint64_t) << (LC + LW);
@@ -1099,62 +1290,76 @@ static void launch_cols_fast_t(const NttBatch& b, int k, int lpre, size_t grid, 
         all = all && pt.t[q] != nullptr;
     }
     if (!all) pt = PassTw{};  // one form for every prime of the launch
-    set_smem(ntt_cols_fast_kernel<INV, LC, LW, RB>, smem);
-    ntt_cols_fast_kernel<INV, LC, LW, RB><<<(unsigned)grid, 256, smem, s>>>(b, k, lpre, pt);
+    set_smem(ntt_cols_fast_kernel<INV, LC, LW, RB, A>, smem);
+    ntt_cols_fast_kernel<INV, LC, LW, RB, A><<<(unsigned)grid, 256, smem, s>>>(b, k, lpre, pt);
 }
 
-template <bool INV, int LC, int RB = 3>
+template <bool INV, int LC, int RB, class A>
 static bool launch_cols_fast_lc(const NttBatch& b, int k, int lpre, int lw, size_t grid, cudaStream_t s)
 {
     switch (lw) {
-    case 2: if constexpr (LC + 2 <= 13) { launch_cols_fast_t<INV, LC, 2, RB>(b, k, lpre, grid, s); return true; } break;
-    case 3: if constexpr (LC + 3 <= 13) { launch_cols_fast_t<INV, LC, 3, RB>(b, k, lpre, grid, s); return true; } break;
-    case 4: if constexpr (LC + 4 <= 13) { launch_cols_fast_t<INV, LC, 4, RB>(b, k, lpre, grid, s); return true; } break;
-    case 5: if constexpr (LC + 5 <= 13) { launch_cols_fast_t<INV, LC, 5, RB>(b, k, lpre, grid, s); return true; } break;
-    case 6: if constexpr (LC + 6 <= 13) { launch_cols_fast_t<INV, LC, 6, RB>(b, k, lpre, grid, s); return true; } break;
+    case 2: if constexpr (LC + 2 <= 13) { launch_cols_fast_t<INV, LC, 2, RB, A>(b, k, lpre, grid, s); return true; } break;
+    case 3: if constexpr (LC + 3 <= 13) { launch_cols_fast_t<INV, LC, 3, RB, A>(b, k, lpre, grid, s); return true; } break;
+    case 4: if constexpr (LC + 4 <= 13) { launch_cols_fast_t<INV, LC, 4, RB, A>(b, k, lpre, grid, s); return true; } break;
+    case 5: if constexpr (LC + 5 <= 13) { launch_cols_fast_t<INV, LC, 5, RB, A>(b, k, lpre, grid, s); return true; } break;
+    case 6: if constexpr (LC + 6 <= 13) { launch_cols_fast_t<INV, LC, 6, RB, A>(b, k, lpre, grid, s); return true; } break;
     default: break;
     }
     return false;
 }
 
-template <bool INV>
+template <bool INV, class A>
 static bool launch_cols_fast(const NttBatch& b, int k, int lpre, int lc, int lw, size_t grid, cudaStream_t s)
 {
-    if (g_geom[k].rbits == 4) {  // radix-16 rounds for the tall columns of long transforms
+    if (geom_of(b, k).rbits == 4) {  // radix-16 rounds for the tall columns of long transforms
         switch (lc) {
-        case 8: return launch_cols_fast_lc<INV, 8, 4>(b, k, lpre, lw, grid, s);
-        case 9: return launch_cols_fast_lc<INV, 9, 4>(b, k, lpre, lw, grid, s);
-        case 10: return launch_cols_fast_lc<INV, 10, 4>(b, k, lpre, lw, grid, s);
-        case 11: return launch_cols_fast_lc<INV, 11, 4>(b, k, lpre, lw, grid, s);
+        case 8: return launch_cols_fast_lc<INV, 8, 4, A>(b, k, lpre, lw, grid, s);
+        case 9: return launch_cols_fast_lc<INV, 9, 4, A>(b, k, lpre, lw, grid, s);
+        case 10: return launch_cols_fast_lc<INV, 10, 4, A>(b, k, lpre, lw, grid, s);
+        case 11: return launch_cols_fast_lc<INV, 11, 4, A>(b, k, lpre, lw, grid, s);
         default: break;
         }
     }
     switch (lc) {
-    case 1: return launch_cols_fast_lc<INV, 1>(b, k, lpre, lw, grid, s);
-    case 2: return launch_cols_fast_lc<INV, 2>(b, k, lpre, lw, grid, s);
-    case 3: return launch_cols_fast_lc<INV, 3>(b, k, lpre, lw, grid, s);
-    case 4: return launch_cols_fast_lc<INV, 4>(b, k, lpre, lw, grid, s);
-    case 5: return launch_cols_fast_lc<INV, 5>(b, k, lpre, lw, grid, s);
-    case 6: return launch_cols_fast_lc<INV, 6>(b, k, lpre, lw, grid, s);
-    case 7: return launch_cols_fast_lc<INV, 7>(b, k, lpre, lw, grid, s);
-    case 8: return launch_cols_fast_lc<INV, 8>(b, k, lpre, lw, grid, s);
-    case 9: return launch_cols_fast_lc<INV, 9>(b, k, lpre, lw, grid, s);
-    case 10: return launch_cols_fast_lc<INV, 10>(b, k, lpre, lw, grid, s);
-    case 11: return launch_cols_fast_lc<INV, 11>(b, k, lpre, lw, grid, s);
+    case 1: return launch_cols_fast_lc<INV, 1, 3, A>(b, k, lpre, lw, grid, s);
+    case 2: return launch_cols_fast_lc<INV, 2, 3, A>(b, k, lpre, lw, grid, s);
+    case 3: return launch_cols_fast_lc<INV, 3, 3, A>(b, k, lpre, lw, grid, s);
+    case 4: return launch_cols_fast_lc<INV, 4, 3, A>(b, k, lpre, lw, grid, s);
+    case 5: return launch_cols_fast_lc<INV, 5, 3, A>(b, k, lpre, lw, grid, s);
+    case 6: return launch_cols_fast_lc<INV, 6, 3, A>(b, k, lpre, lw, grid, s);
+    case 7: return launch_cols_fast_lc<INV, 7, 3, A>(b, k, lpre, lw, grid, s);
+    case 8: return launch_cols_fast_lc<INV, 8, 3, A>(b, k, lpre, lw, grid, s);
+    case 9: return launch_cols_fast_lc<INV, 9, 3, A>(b, k, lpre, lw, grid, s);
+    case 10: return launch_cols_fast_lc<INV, 10, 3, A>(b, k, lpre, lw, grid, s);
+    case 11: return launch_cols_fast_lc<INV, 11, 3, A>(b, k, lpre, lw, grid, s);
     default: return false;
     }
+}
+
+template <bool INV>
+static bool launch_rows_fast_any(const NttBatch& b, int k, int lr, cudaStream_t s)
+{
+    return b.prime[0].fp64 ? launch_rows_fast<INV, ArithDbl>(b, k, lr, s) : launch_rows_fast<INV, ArithInt>(b, k, lr, s);
+}
+
+template <bool INV>
+static bool launch_cols_fast_any(const NttBatch& b, int k, int lpre, int lc, int lw, size_t grid, cudaStream_t s)
+{
+    return b.prime[0].fp64 ? launch_cols_fast<INV, ArithDbl>(b, k, lpre, lc, lw, grid, s)
+                           : launch_cols_fast<INV, ArithInt>(b, k, lpre, lc, lw, grid, s);
 }
 
 static void launch_rows(bool inv, const NttBatch& b, int k, int lr, cudaStream_t s)
 {
     if (fast_ok(b, k)) {
         ProfScope ps(KC_NTT_ROWS, 16.0 * (double)b.count * (double)((size_t)1 << k), s);
-        if (inv ? launch_rows_fast<true>(b, k, lr, s) : launch_rows_fast<false>(b, k, lr, s)) {
+        if (inv ? launch_rows_fast_any<true>(b, k, lr, s) : launch_rows_fast_any<false>(b, k, lr, s)) {
             PIC_CHECK_LAUNCH();
             count_launch();
             return;
         }
     }
+    PIC_REQUIRE(!b.prime[0].fp64, PIC_ERR_INVALID, "FP64 NTT row pass outside the fast kernels' shapes");
     if (!inv && b.src.words != nullptr) materialize_src(b, k, s);  // the general kernels read `data`
     int lrpc = 0;
     if (lr == k) {
@@ -1167,7 +1372,7 @@ static void launch_rows(bool inv, const NttBatch& b, int k, int lr, cudaStream_t
     const size_t grid = rows >> lrpc;
     ProfScope ps(KC_NTT_ROWS, 16.0 * (double)b.count * (double)((size_t)1 << k), s);
     const size_t smem = sizeof(uint64_t) << (lrpc + lr);
-    const int rb = g_geom[k].rbits;
+    const int rb = geom_of(b, k).rbits;
     int threads = 1 << (lrpc + lr - rb);
     if (threads < 32) threads = 32;
     if (threads > 512) threads = 512;
@@ -1194,8 +1399,9 @@ static void launch_rows(bool inv, const NttBatch& b, int k, int lr, cudaStream_t
 
 static void launch_cols(bool inv, const NttBatch& b, int k, int lpre, int lc, cudaStream_t s)
 {
-    int lw = g_geom[k].col_lw ? g_geom[k].col_lw : col_width_log2(lc);
-    const int rb = g_geom[k].rbits;
+    const Geometry& gm = geom_of(b, k);
+    int lw = gm.col_lw ? gm.col_lw : col_width_log2(lc);
+    const int rb = gm.rbits;
     const int lM = k - lpre - lc;
     if (lc + lw > kInnerBits) lw = kInnerBits - lc;  // tile <= 2^13 points (64 KB)
     if (lw < 2) lw = 2;
@@ -1204,11 +1410,13 @@ static void launch_cols(bool inv, const NttBatch& b, int k, int lpre, int lc, cu
     const size_t smem = sizeof(uint64_t) << (lc + lw);
     ProfScope ps(KC_NTT_COLS, 16.0 * (double)b.count * (double)((size_t)1 << k), s);
     if (fast_ok(b, k) && b.prime[0].slo_fwd != nullptr &&
-        (inv ? launch_cols_fast<true>(b, k, lpre, lc, lw, grid, s) : launch_cols_fast<false>(b, k, lpre, lc, lw, grid, s))) {
+        (inv ? launch_cols_fast_any<true>(b, k, lpre, lc, lw, grid, s)
+             : launch_cols_fast_any<false>(b, k, lpre, lc, lw, grid, s))) {
         PIC_CHECK_LAUNCH();
         count_launch();
         return;
     }
+    PIC_REQUIRE(!b.prime[0].fp64, PIC_ERR_INVALID, "FP64 NTT column pass outside the fast kernels' shapes");
     if (!inv && b.src.words != nullptr) materialize_src(b, k, s);  // the general kernels read `data`
     const bool lazy = b.prime[0].lazy != 0;
 #define PIC_COLS(I, Z, R)                                                                          \
@@ -1239,14 +1447,15 @@ static void check_batch(const NttBatch& b, int k)
     PIC_REQUIRE(b.stride >= ((size_t)1 << k), PIC_ERR_INVALID, "NTT batch stride too small");
     for (int q = 0; q * b.per_prime < b.count; q++) {
         PIC_REQUIRE(b.prime[q].K >= k, PIC_ERR_INVALID, "prime has no root of unity of this order");
-        PIC_REQUIRE(b.prime[q].lazy == b.prime[0].lazy, PIC_ERR_INVALID, "mixed lazy/strict primes in one batch");
+        PIC_REQUIRE(b.prime[q].lazy == b.prime[0].lazy && b.prime[q].fp64 == b.prime[0].fp64, PIC_ERR_INVALID,
+                    "mixed prime kinds in one batch");
     }
 }
 
 void ntt_forward_dif(const NttBatch& b, int k, cudaStream_t s)
 {
     check_batch(b, k);
-    std::vector<int> bits = ntt_pass_bits(k);
+    std::vector<int> bits = ntt_pass_bits(k, b.prime[0].fp64 ? kFormDbl : kFormInt);
     NttBatch rest = b;
     rest.src = SplitSrc{};  // only the first pass reads the child slots
     int lpre = 0;
@@ -1262,7 +1471,7 @@ void ntt_inverse_dit(const NttBatch& b_in, int k, cudaStream_t s)
     NttBatch b = b_in;
     b.src = SplitSrc{};
     check_batch(b, k);
-    std::vector<int> bits = ntt_pass_bits(k);
+    std::vector<int> bits = ntt_pass_bits(k, b.prime[0].fp64 ? kFormDbl : kFormInt);
     launch_rows(true, b, k, bits.back(), s);
     int lpre = k - bits.back();
     for (int i = (int)bits.size() - 2; i >= 0; i--) {
@@ -1305,6 +1514,10 @@ __global__ void pointwise_mont_kernel(NttBatch B, const uint64_t* __restrict__ o
         const size_t tr = g >> k, i = g & (n - 1);
         const PrimeDev P = pick_prime(B, (int)tr);
         uint64_t* d = B.data + tr * B.stride + i;
+        if (P.fp64) {  // forward outputs |x| <= 0.75 p: the product is below 0.57 p^2
+            *d = dstore(dmul_mod(dbits(*d), dbits(other[tr * ostride + i]), P.pd, P.pinv));
+            continue;
+        }
         *d = P.lazy ? mont_mul_c(*d, other[tr * ostride + i], P.p, (uint32_t)(P.p >> 32))
                     : mont_mul(*d, other[tr * ostride + i], P.p, P.pinv_neg);
     }

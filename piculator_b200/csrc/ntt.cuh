@@ -58,6 +58,11 @@ struct PrimeDev {
     const uint64_t* lvl_inv;
     // floor(2^128 / p) = mu_hi 2^64 + mu_lo: Shoup companions on the device
     uint64_t mu_hi, mu_lo;
+    // FP64 primes (below 2^47, the FP64 product form): residues are doubles
+    // holding signed integers, and every table pair is (w, fl(w / p)) as the
+    // bits of two doubles.  Only the fast passes serve them.
+    int fp64;
+    double pd, pinv;  // p and fl(1 / p)
 };
 
 // Host-owned tables for one prime (built once, cached for the process).
@@ -76,6 +81,15 @@ uint64_t smallest_generator(uint64_t p);
 
 // The three 62-bit primes of the multi-prime product (c * 2^32 + 1).
 extern const uint64_t kProductPrimes[3];
+// The three primes of the FP64 product form (c * 2^32 + 1 below 2^47).
+extern const uint64_t kDblPrimes[3];
+// Tables of an FP64 prime (p < 2^47, 2-adicity >= 13), cached like prime_tables.
+const PrimeTables& dbl_prime_tables(uint64_t p);
+
+// Product forms: the integer three-prime NTT (64-bit pieces, primes below
+// 2^61, lazy Shoup butterflies) and the FP64 one (56-bit pieces, primes below
+// 2^47, butterflies on the FP64 pipe).
+enum NttForm { kFormInt = 0, kFormDbl = 1 };
 
 // A batch of transforms of length 2^k laid out at data + i * stride
 // (i < count); transform i uses prime[i / per_prime].
@@ -107,7 +121,7 @@ void ntt_bitreverse(const NttBatch& b, int k, cudaStream_t s);
 
 // out[i] = a[i] * b[i] * 2^-64 mod p over every transform of the batch
 // (b may equal a for squaring); b's transforms are b_stride apart (0: a's
-// stride).
+// stride).  FP64 primes: out[i] = a[i] * b[i] mod p (no Montgomery factor).
 void ntt_pointwise_mont(const NttBatch& a, const uint64_t* b, int k, cudaStream_t s, size_t b_stride = 0);
 
 // T[i] = T[i] * A[i] mod p exactly (reference ntt_pointwise semantics).
@@ -119,10 +133,14 @@ void ntt_scale_ninv(uint64_t* T, int k, const PrimeDev& P, cudaStream_t s);
 double butterfly_ceiling(cudaStream_t s);
 
 // Pass split used for length 2^k (for reporting / tests).
-std::vector<int> ntt_pass_bits(int k);
-// Tunable geometry per length (row-pass bits 8..13, column tile log2 width
-// 0..6 with 0 = automatic, bits per register round 2..4).
-void ntt_set_geometry(int k, int row_bits, int col_lw, int rbits);
-void ntt_get_geometry(int k, int* row_bits, int* col_lw, int* rbits);
+std::vector<int> ntt_pass_bits(int k, int form = kFormInt);
+// Tunable geometry per length and form (row-pass bits 8..13, column tile
+// log2 width 0..6 with 0 = automatic, bits per register round 2..4; the FP64
+// form runs only the fast passes: row bits 11..13, rounds of 3 or 4 bits).
+void ntt_set_geometry(int k, int row_bits, int col_lw, int rbits, int form = kFormInt);
+// FP64 column passes: per-point twiddle tables (on) or two-level tables (off, default).
+void ntt_set_dbl_pass_tables(bool on);
+bool ntt_dbl_pass_tables();
+void ntt_get_geometry(int k, int* row_bits, int* col_lw, int* rbits, int form = kFormInt);
 
 }  // namespace pic

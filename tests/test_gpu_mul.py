@@ -11,7 +11,7 @@ from oracle.ffi import random_words
 
 pytestmark = pytest.mark.gpu
 
-MODES = ["school", "ntt_ref", "ntt3", "fft", "auto"]
+MODES = ["school", "ntt_ref", "ntt3", "ntt3d", "fft", "auto"]
 
 
 def _md5(w):
@@ -59,7 +59,7 @@ def test_edge_products_golden(pic, golden, mode):
 
 
 @pytest.mark.parametrize("lg", [12, 16, 20])
-@pytest.mark.parametrize("mode", ["ntt_ref", "ntt3", "fft", "auto"])
+@pytest.mark.parametrize("mode", ["ntt_ref", "ntt3", "ntt3d", "fft", "auto"])
 def test_isolated_products_golden(pic, golden, lg, mode):
     rec = [r for r in golden["products"]["isolated"] if r["log2n"] == lg][0]
     n = 1 << lg
@@ -86,7 +86,7 @@ def big_operands():
 # (BigFloat.cpp:380-441).  The fixture holds the md5 of the reference's own
 # product words.  The FP64 FFT has no proven piece width at these lengths.
 @pytest.mark.parametrize("lg", [24, 27])
-@pytest.mark.parametrize("mode", ["ntt3", "ntt_ref", "auto"])
+@pytest.mark.parametrize("mode", ["ntt3", "ntt3d", "ntt_ref", "auto"])
 def test_isolated_products_golden_large(pic, golden, big_operands, lg, mode):
     rec = [r for r in golden["products"]["isolated"] if r["log2n"] == lg][0]
     a, b = big_operands(lg)

@@ -1,0 +1,96 @@
+"""The FP64 three-prime product form (PIC_MUL_NTT3D): 56-bit pieces, three
+primes below 2^47, butterflies and CRT in FP64 arithmetic.  Every product must
+equal the oracle's, Python integers' and the integer form's words exactly."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle.ffi import random_words
+
+pytestmark = pytest.mark.gpu
+
+
+def _int(w):
+    return int.from_bytes(np.ascontiguousarray(w, dtype="<u4").tobytes(), "little")
+
+
+@pytest.mark.parametrize("na,nb", [(1, 1), (1, 2), (2, 3), (7, 7), (31, 33), (64, 64), (100, 1), (1, 257),
+                                   (255, 256), (1000, 1000), (1023, 2000), (2047, 2049), (4097, 3),
+                                   (7, 7777)])
+def test_products_vs_oracle(pic, oracle, na, nb):
+    a = random_words(na * 7 + nb, na)
+    b = random_words(nb * 13 + na, nb)
+    assert np.array_equal(pic.mul_host(a, b, "ntt3d"), oracle.mul_words(a, b))
+
+
+@pytest.mark.parametrize("n", [5000, 1 << 14, 40000, 1 << 17, 300001])
+def test_products_vs_python_int(pic, n):
+    a = random_words(n, n)
+    b = random_words(n + 1, n - 3)
+    assert _int(pic.mul_host(a, b, "ntt3d")) == _int(a) * _int(b)
+
+
+def test_all_ones_max_carry_chain(pic):
+    # (B^n - 1)^2: every coefficient at its largest, the longest carry chains
+    for n in (3, 4097, 1 << 16, (1 << 18) + 5, 1 << 21):
+        ones = np.full(n, 0xFFFFFFFF, dtype=np.uint32)
+        z = pic.mul_host(ones, ones, "ntt3d")
+        assert z[0] == 1 and np.all(z[1:n] == 0)
+        assert z[n] == 0xFFFFFFFE and np.all(z[n + 1:] == 0xFFFFFFFF)
+
+
+@pytest.mark.parametrize("na,nb", [(2200, 2200), (2201, 2199), (3000, 1300), (60000, 10000), (92000, 46000),
+                                   (150000, 150000)])
+def test_wrapped_and_plain_forms(pic, na, nb):
+    a = random_words(na + 5, na)
+    b = random_words(nb + 9, nb)
+    want = _int(a) * _int(b)
+    saved = pic.get_tuning(pic.TUNE_MUL_WRAP)
+    try:
+        for wrap in (1, 0):
+            pic.set_tuning(pic.TUNE_MUL_WRAP, wrap)
+            assert _int(pic.mul_host(a, b, "ntt3d")) == want, f"wrap={wrap}"
+    finally:
+        pic.set_tuning(pic.TUNE_MUL_WRAP, saved)
+
+
+def test_squaring_same_pointer(pic, torch_cuda, oracle):
+    torch = torch_cuda
+    for n in (3000, 2200):
+        a = random_words(77 + n, n)
+        ta = torch.from_numpy(a.view(np.int32)).cuda()
+        z = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+        pic.mul_dev(z.data_ptr(), ta.data_ptr(), n, ta.data_ptr(), n, "ntt3d", torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert np.array_equal(z.cpu().numpy().view(np.uint32), oracle.mul_words(a, a))
+
+
+@pytest.mark.parametrize("row_bits", [11, 12, 13])
+def test_geometries_match_integer_form(pic, row_bits):
+    """Every FP64 pass geometry (rows of 2^11 .. 2^13 points, radix-8 and
+    radix-16 rounds) gives the integer form's words, for transform lengths
+    2^14 .. 2^24, and Python integers where they are quick."""
+    saved = {k: pic.get_ntt_geometry(k, pic.FORM_DBL) for k in range(14, 26)}
+    try:
+        for lg in (13, 16, 19, 22):
+            n = 1 << lg
+            a, b = random_words(lg + row_bits, n), random_words(lg + 2 * row_bits, n - 5)
+            want = pic.mul_host(a, b, "ntt3")
+            for rb in (3, 4):
+                for k in range(14, 26):
+                    pic.set_ntt_geometry(k, row_bits, saved[k][1], rb, pic.FORM_DBL)
+                got = pic.mul_host(a, b, "ntt3d")
+                assert np.array_equal(got, want), (lg, rb)
+            if lg <= 16:
+                assert _int(want) == _int(a) * _int(b)
+    finally:
+        for k, (r, lw, rb) in saved.items():
+            pic.set_ntt_geometry(k, r, lw, rb, pic.FORM_DBL)
+
+
+@pytest.mark.parametrize("lg", [22, 24])
+def test_large_products_agree_with_integer_form(pic, lg):
+    n = 1 << lg
+    a, b = random_words(42, n), random_words(43, n)
+    assert np.array_equal(pic.mul_host(a, b, "ntt3d"), pic.mul_host(a, b, "ntt3"))
