@@ -293,8 +293,9 @@ enum {
                                      least this many words (0 = never) */
     PIC_TUNE_NTT_FORM = 10,       /* three-prime form of AUTO products and binary-splitting merges:
                                      0 integer (PIC_MUL_NTT3), 1 FP64 (PIC_MUL_NTT3D) */
-    PIC_TUNE_DBL_PASS_TABLES = 11 /* 1: FP64 column passes stream per-point twiddle tables; 0 (default):
-                                     they form the twiddles from the two-level tables */
+    PIC_TUNE_DBL_PASS_TABLES = 11 /* FP64 column passes over blocks of at most 2^value points (0..24,
+                                     default 20) stream per-point twiddle tables; longer blocks form the
+                                     twiddles from the two-level tables */
 };
 pic_status pic_set_tuning(int knob, int64_t value);
 int64_t pic_get_tuning(int knob);

@@ -210,6 +210,8 @@ def apply_tuning(path: str = TUNING_FILE) -> bool:
         check(L.pic_set_tuning(TUNE_BSR_KARATSUBA, int(t["bsr"]["bsr_karatsuba_min_words"])))
     if "ntt_form" in prod:
         check(L.pic_set_tuning(TUNE_NTT_FORM, int(prod["ntt_form"])))
+    if "dbl_pass_bits" in prod:
+        check(L.pic_set_tuning(TUNE_DBL_PASS_TABLES, int(prod["dbl_pass_bits"])))
     return True
 
 

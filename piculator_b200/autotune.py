@@ -119,22 +119,35 @@ def _timeline_ms_by_k(stderr: str) -> dict:
     return out
 
 
-def tune_ntt_batched(digits: int, ks=range(14, 28), radices=(3, 4)) -> dict:
+def tune_ntt_batched(digits: int, ks=range(14, 28), radices=(3, 4), form: int = P.FORM_INT,
+                     rows=(11, 12, 13), pass_bits=(None,)) -> dict:
     """NTT geometry per length, timed on the batched merges of whole pi runs:
     each candidate is applied to every length at once, the second of two runs
     is timed, and each length takes the candidate whose merge levels of that
     length were fastest (a level's wrapped tail product, usually two lengths
     shorter, runs under the same candidate).  Radix 16 (radix_log2 4) applies
     to row passes of 2^11 .. 2^13 points and column passes of 2^8 .. 2^11
-    rows; other passes stay radix 8."""
+    rows; other passes stay radix 8.  With form FORM_DBL the runs use the
+    FP64 product form and the geometry is that form's; pass_bits then lists
+    the candidate FP64 pass-table limits (PIC_TUNE_DBL_PASS_TABLES), and the
+    one with the fastest whole binary splitting is kept (returned under the
+    key "dbl_pass_bits")."""
     import subprocess
     import sys
     import tempfile
-    cands = [(row, lw, rb) for row in (11, 12, 13) for lw in (0, 3, 5) for rb in radices]
+    cands = [(row, lw, rb, pb) for row in rows for lw in (0, 3, 5) for rb in radices for pb in pass_bits]
     ms: dict = {}
+    total: dict = {}
     env = dict(os.environ, PIC_TIMELINE="1")
-    for row, lw, rb in cands:
-        tab = {"ntt": {str(k): {"row_bits": row, "col_width_log2": lw, "radix_log2": rb} for k in ks}}
+    key = "ntt_fp64" if form == P.FORM_DBL else "ntt"
+    for row, lw, rb, pb in cands:
+        geo = {str(k): {"row_bits": row if k > 13 or form == P.FORM_INT else 12, "col_width_log2": lw,
+                        "radix_log2": rb} for k in ks}
+        tab = {key: geo}
+        if form == P.FORM_DBL:
+            tab["products"] = {"ntt_form": 1}
+            if pb is not None:
+                tab["products"]["dbl_pass_bits"] = pb
         with tempfile.NamedTemporaryFile("w", suffix=".json", delete=False) as f:
             json.dump(tab, f)
             path = f.name
@@ -144,17 +157,25 @@ def tune_ntt_batched(digits: int, ks=range(14, 28), radices=(3, 4)) -> dict:
                                check=True)
         finally:
             os.unlink(path)
-        for k, v in _timeline_ms_by_k(r.stderr).items():
-            ms.setdefault(k, {})[(row, lw, rb)] = v
-        print(f"ntt batched {row}/{lw}/{rb}: { {k: round(v[(row, lw, rb)], 2) for k, v in sorted(ms.items())} }",
+        by_k = _timeline_ms_by_k(r.stderr)
+        for k, v in by_k.items():
+            ms.setdefault(pb, {}).setdefault(k, {})[(row, lw, rb)] = v
+        total.setdefault(pb, {})[(row, lw, rb)] = sum(by_k.values())
+        print(f"ntt batched {key} {row}/{lw}/{rb}/{pb}: { {k: round(v, 2) for k, v in sorted(by_k.items())} }",
               flush=True)
+    # the pass-table limit whose best per-length choices sum lowest
+    def best_sum(pb):
+        return sum(min(by.values()) for k, by in ms[pb].items() if k in ks)
+    pb = min(ms, key=best_sum)
     out = {}
-    for k, by in sorted(ms.items()):
+    for k, by in sorted(ms[pb].items()):
         if k not in ks:
             continue
         (row, lw, rb), best = min(by.items(), key=lambda kv: kv[1])
         out[str(k)] = {"row_bits": row, "col_width_log2": lw, "radix_log2": rb, "ms_batched": best}
-        P.set_ntt_geometry(k, row, lw, rb)
+        P.set_ntt_geometry(k, row, lw, rb, form)
+    if form == P.FORM_DBL and pb is not None:
+        out["dbl_pass_bits"] = pb
     return out
 
 
@@ -219,7 +240,20 @@ def main():
                     help="rerun only the batched geometry stage over the table in --out")
     ap.add_argument("--only-bsr", action="store_true",
                     help="rerun only the binary-splitting thresholds over the table in --out")
+    ap.add_argument("--only-fp64", action="store_true",
+                    help="rerun only the FP64 form's batched geometry and pass-table limit over the table in --out")
     args = ap.parse_args()
+    if args.only_fp64:
+        P.init(0, tuned=True)
+        result = json.load(open(args.out))
+        got = tune_ntt_batched(1_000_000_000, ks=range(10, 28), form=P.FORM_DBL, rows=(11, 12),
+                               pass_bits=(20, 24))
+        result.setdefault("products", {})["dbl_pass_bits"] = got.pop("dbl_pass_bits", 20)
+        result["ntt_fp64"] = got
+        with open(args.out, "w") as f:
+            json.dump(result, f, indent=1)
+        print("wrote", args.out)
+        return
     if args.only_bsr:
         P.init(0, tuned=True)
         result = json.load(open(args.out))

@@ -27,6 +27,7 @@
 #include "bsr.cuh"
 #include "carry.cuh"
 #include "common.cuh"
+#include "fp64mod.cuh"
 #include "mul.cuh"
 #include "ntt.cuh"
 #include "pi.cuh"
@@ -915,6 +916,58 @@ __global__ void __launch_bounds__(256) merge_pointwise_kernel(uint64_t* __restri
     *reinterpret_cast<ulonglong2*>(R + L) = make_ulonglong2(mont_mul_c(rl.x, rr.x, M.p, c), mont_mul_c(rl.y, rr.y, M.p, c));
 }
 
+// The same on FP64-form residues (signed doubles, fp64mod.cuh): forward
+// outputs |x| <= 0.75 p give products |y| <= 0.75 p, and T1 +- T2 stays below
+// 1.5 p, inside what the FP64 inverse accepts.
+struct DblMod3 {
+    double p[3], pinv[3];
+};
+
+__global__ void __launch_bounds__(256) merge_pointwise_d_kernel(uint64_t* __restrict__ P, uint64_t* __restrict__ Q,
+                                                                uint64_t* __restrict__ R, uint32_t npar, int k,
+                                                                size_t stride, uint32_t jbpr, DblMod3 M,
+                                                                const uint8_t* __restrict__ sgn)
+{
+    const uint32_t row = blockIdx.x / jbpr, jb = blockIdx.x - row * jbpr;
+    const uint32_t q = row / npar, i = row - q * npar;
+    const size_t j = ((size_t)jb * blockDim.x + threadIdx.x) * 2;
+    if (j >= ((size_t)1 << k)) return;
+    const double p = q == 0 ? M.p[0] : (q == 1 ? M.p[1] : M.p[2]);
+    const double pinv = q == 0 ? M.pinv[0] : (q == 1 ? M.pinv[1] : M.pinv[2]);
+    const size_t base = (size_t)q * 2 * npar;
+    const size_t L = (base + 2 * (size_t)i) * stride + j, Rr = L + stride;
+    const double2 pl = *reinterpret_cast<const double2*>(P + L), pr = *reinterpret_cast<const double2*>(P + Rr);
+    const double2 ql = *reinterpret_cast<const double2*>(Q + L), qr = *reinterpret_cast<const double2*>(Q + Rr);
+    const double2 rl = *reinterpret_cast<const double2*>(R + L), rr = *reinterpret_cast<const double2*>(R + Rr);
+    const double2 t1 = make_double2(dmul_mod(pl.x, qr.x, p, pinv), dmul_mod(pl.y, qr.y, p, pinv));
+    const double2 t2 = make_double2(dmul_mod(pr.x, rl.x, p, pinv), dmul_mod(pr.y, rl.y, p, pinv));
+    if (sgn != nullptr) {
+        const bool same = (sgn[2 * i] != 0) == (sgn[2 * i + 1] != 0);
+        *reinterpret_cast<double2*>(P + L) = same ? make_double2(__dadd_rn(t1.x, t2.x), __dadd_rn(t1.y, t2.y))
+                                                  : make_double2(__dadd_rn(t1.x, -t2.x), __dadd_rn(t1.y, -t2.y));
+    } else {
+        *reinterpret_cast<double2*>(P + L) = t1;
+        *reinterpret_cast<double2*>(P + Rr) = t2;
+    }
+    *reinterpret_cast<double2*>(Q + L) = make_double2(dmul_mod(ql.x, qr.x, p, pinv), dmul_mod(ql.y, qr.y, p, pinv));
+    *reinterpret_cast<double2*>(R + L) = make_double2(dmul_mod(rl.x, rr.x, p, pinv), dmul_mod(rl.y, rr.y, p, pinv));
+}
+
+static void launch_merge_pointwise_d(uint64_t* P, uint64_t* Q, uint64_t* R, size_t npar, int k, size_t stride,
+                                     const uint8_t* sgn, cudaStream_t s)
+{
+    PIC_REQUIRE(k >= 1 && stride % 2 == 0 && npar <= 0x7fffffffu / 3, PIC_ERR_INVALID, "pointwise merge shape");
+    const uint32_t jbpr = (uint32_t)((((size_t)1 << k) + 511) / 512);
+    const size_t blocks = 3 * npar * (size_t)jbpr;
+    PIC_REQUIRE(blocks <= 0x7fffffffu, PIC_ERR_INVALID, "pointwise merge grid too large");
+    DblMod3 M;
+    for (int q = 0; q < 3; q++) {
+        M.p[q] = (double)kDblPrimes[q];
+        M.pinv[q] = 1.0 / M.p[q];
+    }
+    merge_pointwise_d_kernel<<<(unsigned)blocks, 256, 0, s>>>(P, Q, R, (uint32_t)npar, k, stride, jbpr, M, sgn);
+}
+
 // Launch over 3 primes x npar parents x 2^k points (stride even, 2^k >= 2).
 static void launch_merge_pointwise(uint64_t* P, uint64_t* Q, uint64_t* R, size_t npar, int k, size_t stride,
                                    const Mod64& m0, const Mod64& m1, const Mod64& m2, const uint8_t* sgn,
@@ -1257,23 +1310,30 @@ static bool g_top_batched = true;
 static bool g_wide_add = true;
 
 // Parameters of one level's batched NTT merge.  Every operand has at most
-// smax = ceil(cmax / 2) 64-bit pieces, every product at most L = 2 smax - 1
+// smax pieces (ceil(cmax / 2) of 64 bits, or in the FP64 form
+// ceil(32 cmax / 56) of 56 bits), every product at most L = 2 smax - 1
 // coefficients.  Plain form: one transform of length 2^ceil_log2(L).  Wrapped
 // form (when L sits just above a power of two): main length Nm = 2^(k-1) plus
 // a tail product of length T >= 2W - 1 over the top W = L - Nm pieces.
 struct MergeShape {
-    int k = 0;          // main transform bits
-    size_t N = 0;       // main length
-    size_t stride = 0;  // item stride of the main arrays (>= N + W)
+    int form = kFormInt;  // three-prime form of the level
+    int k = 0;            // main transform bits
+    size_t N = 0;         // main length
+    size_t stride = 0;    // item stride of the main arrays (>= N + W)
     bool wrap = false;
-    int kt = 0;         // tail transform bits
+    int kt = 0;           // tail transform bits
     size_t T = 0, W = 0, t0 = 0;
 };
+
+// The FP64 form serves a level while 2 smax (2^56)^2 + 2^140 < p0 p1 p2:
+// smax <= 2^26 pieces (the signed combined P with its offset).
+constexpr size_t kDblMergeMaxPieces = (size_t)1 << 26;
 
 static MergeShape merge_shape(uint32_t cmax)
 {
     MergeShape m;
-    const size_t smax = ((size_t)cmax + 1) / 2;
+    m.form = (mul_ntt_form() == kFormDbl && pieces56(cmax) <= kDblMergeMaxPieces) ? kFormDbl : kFormInt;
+    const size_t smax = m.form == kFormDbl ? pieces56(cmax) : ((size_t)cmax + 1) / 2;
     const size_t L = smax ? 2 * smax - 1 : 1;
     int k = ceil_log2_sz(L);
     if (k < 2) k = 2;
@@ -1328,6 +1388,18 @@ struct ProductsOut {
 // wrapped top coefficients).
 static size_t products_ncoef(const MergeShape& sh) { return sh.wrap ? sh.N + sh.W : sh.N; }
 
+// Words of V + K in the combined form (every coefficient plus the offset:
+// below 2^160 at bit 64 j, or below 2^141 at bit 56 j in the FP64 form), and
+// of K alone.
+static uint32_t combined_words(const MergeShape& sh, size_t ncoef)
+{
+    return sh.form == kFormDbl ? (uint32_t)((56 * ncoef + 86 + 31) / 32 + 1) : (uint32_t)(2 * ncoef + 6);
+}
+static uint32_t offset_words(const MergeShape& sh, size_t ncoef)
+{
+    return sh.form == kFormDbl ? (uint32_t)(((140 + 56 * (ncoef - 1)) >> 5) + 1) : (uint32_t)(2 * ncoef + 3);
+}
+
 __global__ void fill_u32_kernel(uint32_t* p, size_t n, uint32_t v)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
@@ -1348,9 +1420,10 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
     const size_t N = sh.N, ST = sh.stride, T = sh.T;
     const Mod64 m0 = prime_mod(0), m1 = prime_mod(1), m2 = prime_mod(2);
     const bool needR = o.R != nullptr;
+    const bool dbl = sh.form == kFormDbl;
     // tail scale Nm / T in Montgomery form (mont_mul(x, c) = x Nm / T)
     uint64_t cT[3] = {0, 0, 0};
-    if (sh.wrap)
+    if (sh.wrap && !dbl)
         for (int q = 0; q < 3; q++) cT[q] = to_mont((uint64_t)(N / T), kProductPrimes[q]);
     const size_t ncoef = products_ncoef(sh);
     {
@@ -1380,7 +1453,8 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         fb.stride = ST;
         fb.count = (int)(3 * nc);
         fb.per_prime = (int)nc;
-        for (int q = 0; q < 3; q++) fb.prime[q] = prime_tables(kProductPrimes[q]).dev;
+        for (int q = 0; q < 3; q++)
+            fb.prime[q] = dbl ? dbl_prime_tables(kDblPrimes[q]).dev : prime_tables(kProductPrimes[q]).dev;
         NttBatch tb = fb;
         tb.stride = T;
         // the children's words are split into residues by each transform's
@@ -1409,8 +1483,13 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         tb.src = SplitSrc{};
         {
             ProfScope ps(KC_NTT_POINTWISE, 3.0 * 3 * np * (double)(N + T) * 80.0 / 8.0, s);
-            launch_merge_pointwise(PB, QB, RB, np, k, ST, m0, m1, m2, o.csign, s);
-            if (sh.wrap) launch_merge_pointwise(PT, QT, RT, np, sh.kt, T, m0, m1, m2, o.csign, s);
+            if (dbl) {
+                launch_merge_pointwise_d(PB, QB, RB, np, k, ST, o.csign, s);
+                if (sh.wrap) launch_merge_pointwise_d(PT, QT, RT, np, sh.kt, T, o.csign, s);
+            } else {
+                launch_merge_pointwise(PB, QB, RB, np, k, ST, m0, m1, m2, o.csign, s);
+                if (sh.wrap) launch_merge_pointwise(PT, QT, RT, np, sh.kt, T, m0, m1, m2, o.csign, s);
+            }
             PIC_CHECK_LAUNCH();
             count_launch(sh.wrap ? 2 : 1);
         }
@@ -1458,16 +1537,19 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
             }
             ProfScope ps(KC_NTT_POINTWISE, 3.0 * 4 * np * (double)sh.W * 24.0, s);
             const size_t W = sh.W;
-            if (comb) launch_wrap_fix(PB, ST, PT, T, np, 2, nc, N, W, cT, s);
-            else launch_wrap_fix(PB, ST, PT, T, nc, 1, nc, N, W, cT, s);
-            launch_wrap_fix(QB, ST, QT, T, np, 2, nc, N, W, cT, s);
-            if (needR)
-                launch_wrap_fix(RB, ST, RT, T, np, 2, nc, N, W, cT, s);
+            auto fix = [&](uint64_t* y, const uint64_t* tail, size_t nitems, size_t item_mul) {
+                if (dbl) launch_wrap_fix_d(y, ST, tail, T, nitems, item_mul, nc, N, W, s);
+                else launch_wrap_fix(y, ST, tail, T, nitems, item_mul, nc, N, W, cT, s);
+            };
+            if (comb) fix(PB, PT, np, 2);
+            else fix(PB, PT, nc, 1);
+            fix(QB, QT, np, 2);
+            if (needR) fix(RB, RT, np, 2);
             PIC_CHECK_LAUNCH();
             count_launch(needR ? 3 : 2);
         }
         if (comb) {
-            fill_u32_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.l1, np, (uint32_t)(2 * ncoef + 6));
+            fill_u32_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.l1, np, combined_words(sh, ncoef));
         } else {
             product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.Q.len.get(), p0, np, 0, 1, o.l1);
             product_len_kernel<<<grid_for(np, 256), 256, 0, s>>>(ch.P.len.get(), ch.R.len.get(), p0, np, 1, 0, o.l2);
@@ -1479,14 +1561,18 @@ static void ntt_products(const Level& ch, size_t p0, size_t np, const MergeShape
         count_launch(needR ? 4 : 3);
         // T1: residues at bP items 2i (stride 2 ST), T2 at items 2i+1
         const size_t pstride = nc * ST;  // [prime][child][ST]
+        auto to_words = [&](const uint64_t* y, uint32_t* z, uint32_t zcap, const uint32_t* zlen, bool offset) {
+            if (dbl) ntt3d_batch_to_words(y, 2 * ST, pstride, np, k, z, zcap, zlen, s, ncoef, offset);
+            else ntt3_batch_to_words(y, 2 * ST, pstride, np, k, z, zcap, zlen, s, ncoef, offset);
+        };
         if (comb) {
-            ntt3_batch_to_words(PB, 2 * ST, pstride, np, k, o.T1, o.c1, o.l1, s, ncoef, /*offset=*/true);
+            to_words(PB, o.T1, o.c1, o.l1, true);
         } else {
-            ntt3_batch_to_words(PB, 2 * ST, pstride, np, k, o.T1, o.c1, o.l1, s, ncoef);
-            ntt3_batch_to_words(PB + ST, 2 * ST, pstride, np, k, o.T2, o.c2, o.l2, s, ncoef);
+            to_words(PB, o.T1, o.c1, o.l1, false);
+            to_words(PB + ST, o.T2, o.c2, o.l2, false);
         }
-        ntt3_batch_to_words(QB, 2 * ST, pstride, np, k, o.Q, o.cQ, o.lQ, s, ncoef);
-        if (needR) ntt3_batch_to_words(RB, 2 * ST, pstride, np, k, o.R, o.cR, o.lR, s, ncoef);
+        to_words(QB, o.Q, o.cQ, o.lQ, false);
+        if (needR) to_words(RB, o.R, o.cR, o.lR, false);
         if (!comb) {
             fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.T1, o.c1, o.l1, np);
             fix_top_kernel<<<grid_for(np, 256), 256, 0, s>>>(o.T2, o.c2, o.l2, np);
@@ -1504,6 +1590,18 @@ __global__ void offset_words_kernel(uint32_t* K, size_t nwords)
 {
     for (size_t w = blockIdx.x * (size_t)blockDim.x + threadIdx.x; w < nwords; w += (size_t)gridDim.x * blockDim.x)
         K[w] = (w >= 4 && (w & 1) == 0) ? 0x80000000u : 0u;
+}
+
+// FP64 form: K = sum_(j < ncoef) 2^(140 + 56 j); the bits are 56 apart, so a
+// word holds at most one (nwords covers the last).
+__global__ void offset_words56_kernel(uint32_t* K, size_t nwords)
+{
+    for (size_t w = blockIdx.x * (size_t)blockDim.x + threadIdx.x; w < nwords; w += (size_t)gridDim.x * blockDim.x) {
+        const int64_t lo = 32 * (int64_t)w;  // bits lo .. lo + 31
+        const int64_t j = lo <= 140 ? 0 : (lo - 140 + 55) / 56;
+        const int64_t b = 140 + 56 * j;
+        K[w] = b < lo + 32 ? 1u << (b - lo) : 0u;
+    }
 }
 
 // Addend signs of P = sL (V + K) + (not sL) K: parent i at out[2i], out[2i + 1].
@@ -1570,9 +1668,10 @@ static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
     const size_t ncoef = products_ncoef(sh);
     count_products(4 * par.count);  // P0 Q1, P1 R0, Q0 Q1, R0 R1 per parent (PI.h:110-112)
     // combined form: P = sL (T1 +- T2) converted once as V + K (the CRT adds
-    // 2^159 to every coefficient so the signed ones stay exact), then
+    // 2^159, in the FP64 form 2^140, to every coefficient so the signed ones
+    // stay exact), then
     // P = sL (V + K) - sL K with the exact signed sum
-    const uint32_t cV = (uint32_t)(2 * ncoef + 8), cK = (uint32_t)(2 * ncoef + 3);
+    const uint32_t cV = combined_words(sh, ncoef) + 2, cK = offset_words(sh, ncoef);
     const uint32_t c1 = g_combine ? cV : ccP + ccQ, c2 = g_combine ? 0 : ccP + ccR;
     // bytes per parent: the transforms plus the word buffers for P
     const size_t per_parent = ntt_bytes_per_parent(sh) + 4 * (size_t)(c1 + c2 + ccQ + ccR);
@@ -1581,7 +1680,8 @@ static void merge_ntt(Level& ch, Level& par, cudaStream_t s, size_t mem_budget)
     if (chunk > par.count) chunk = par.count;
     DevBuf<uint32_t> K(g_combine ? cK : 0, s);
     if (g_combine) {
-        offset_words_kernel<<<grid_for(cK, 256), 256, 0, s>>>(K.get(), cK);
+        if (sh.form == kFormDbl) offset_words56_kernel<<<grid_for(cK, 256), 256, 0, s>>>(K.get(), cK);
+        else offset_words_kernel<<<grid_for(cK, 256), 256, 0, s>>>(K.get(), cK);
         PIC_CHECK_LAUNCH();
         count_launch();
     }

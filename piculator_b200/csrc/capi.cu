@@ -646,7 +646,10 @@ pic_status pic_set_tuning(int knob, int64_t value)
             PIC_REQUIRE(value <= 1, PIC_ERR_INVALID, "product form is 0 (integer) or 1 (FP64)");
             mul_set_ntt_form((int)value);
             break;
-        case PIC_TUNE_DBL_PASS_TABLES: ntt_set_dbl_pass_tables(value != 0); break;
+        case PIC_TUNE_DBL_PASS_TABLES:
+            PIC_REQUIRE(value <= 24, PIC_ERR_INVALID, "FP64 pass-table bits are 0..24");
+            ntt_set_dbl_pass_bits((int)value);
+            break;
         default: throw Error(PIC_ERR_INVALID, "unknown tuning knob");
         }
     });
@@ -697,7 +700,7 @@ int64_t pic_get_tuning(int knob)
     case PIC_TUNE_FFT_ACCEPT_PPM: return (int64_t)llround(mul_fft_accept() * 1e6);
     case PIC_TUNE_BSR_KARATSUBA: return bsr_karatsuba();
     case PIC_TUNE_NTT_FORM: return mul_ntt_form();
-    case PIC_TUNE_DBL_PASS_TABLES: return ntt_dbl_pass_tables() ? 1 : 0;
+    case PIC_TUNE_DBL_PASS_TABLES: return ntt_dbl_pass_bits();
     }
     return -1;
 }

@@ -140,12 +140,13 @@ __device__ __forceinline__ void crt3(const Crt3Consts& C, uint64_t y0, uint64_t 
 
 // Shared tail of both conversions: limb digits (T = D_i + C_(i-1)) -> words
 // with in-block carry resolution; writes the CTA's (G, P).
-__device__ __forceinline__ void limbs_to_words(const uint64_t (&dig)[kCvtLPT], const uint32_t (&gen)[kCvtLPT],
+template <int NL>
+__device__ __forceinline__ void limbs_to_words(const uint64_t (&dig)[NL], const uint32_t (&gen)[NL],
                                                size_t first_limb, uint32_t* z, size_t zw, uint32_t* agg_slot)
 {
     uint32_t gp = kGPIdentity;
 #pragma unroll
-    for (int u = 0; u < kCvtLPT; u++) {
+    for (int u = 0; u < NL; u++) {
         const size_t w = 2 * (first_limb + u);
         const uint32_t lo = (uint32_t)dig[u], hi = (uint32_t)(dig[u] >> 32);
         if (w < zw) gp = gp_combine(gp, (uint32_t)(lo == 0xffffffffu) << 1);
@@ -154,7 +155,7 @@ __device__ __forceinline__ void limbs_to_words(const uint64_t (&dig)[kCvtLPT], c
     uint32_t total;
     uint32_t cin = block_gp_scan(gp, &total) & 1u;
 #pragma unroll
-    for (int u = 0; u < kCvtLPT; u++) {
+    for (int u = 0; u < NL; u++) {
         const size_t w = 2 * (first_limb + u);
         const uint32_t lo = (uint32_t)dig[u], hi = (uint32_t)(dig[u] >> 32);
         if (w < zw) z[w] = lo + cin;
@@ -834,89 +835,115 @@ __device__ __forceinline__ void crt3d(const CrtDConsts& C, double y0, double y1,
     l2 = (uint64_t)(hi >> 64);
 }
 
-// A CTA of 256 threads owns 448 output limbs (28672 bits = 512 coefficients of
-// 56 bits); limbs i0 - 1 .. i0 + 447 take coefficients 512 b - 3 .. 512 b + 511.
-constexpr size_t kCrtDLPC = 448;
+// A thread takes 8 consecutive coefficients (group u: bits 448 u .. 448 u +
+// 447 of the product) and the 7 limbs they start; limb L of the group
+// collects the windows of the group's coefficients c = -3 .. 7 that reach it
+// (coefficient c at bit 56 c, limb L at bit 64 L; c < 0 come from the
+// previous thread through shared memory), so every shift is a compile-time
+// constant and the lanes of a warp never diverge.
+constexpr int kCrtDThreads = 128;
+constexpr size_t kCrtDLPC = 7 * (size_t)kCrtDThreads;  // limbs per CTA
 constexpr size_t kCrtDWPC = 2 * kCrtDLPC;
-constexpr int kCrtDSlots = 515;
 
-__device__ __forceinline__ int64_t floordiv56(int64_t a) { return a >= 0 ? a / 56 : -((-a + 55) / 56); }
-
-// The 64 bits of coefficient c (three limbs) shifted to bit s relative to a
-// limb (-141 < s < 64): bits -s .. -s + 63 of c.
-__device__ __forceinline__ uint64_t coef_window(const uint64_t* c, int s)
+// The 64 bits of coefficient x (three limbs, below 2^141) that fall in a limb
+// starting s = 56 C - 64 L bits below the coefficient's bit 0.
+template <int C, int L>
+__device__ __forceinline__ uint64_t coef_win(const uint64_t (&x)[3])
 {
-    if (s >= 0) return c[0] << s;
-    const int r = -s;
-    if (r < 64) return (c[0] >> r) | (c[1] << (64 - r));
-    if (r == 64) return c[1];
-    if (r < 128) return (c[1] >> (r - 64)) | (c[2] << (128 - r));
-    return c[2] >> (r - 128);
+    constexpr int s = 56 * C - 64 * L;
+    if constexpr (s >= 0) {
+        return x[0] << s;
+    } else {
+        constexpr int r = -s;
+        if constexpr (r < 64) return (x[0] >> r) | (x[1] << (64 - r));
+        else if constexpr (r == 64) return x[1];
+        else if constexpr (r < 128) return (x[1] >> (r - 64)) | (x[2] << (128 - r));
+        else if constexpr (r == 128) return x[2];
+        else return x[2] >> (r - 128);
+    }
 }
 
-// Limb i of the sum of c_j 2^(56 j): the windows of the coefficients that
-// reach it (at most four), as a 66-bit (lo, hi).  xs holds coefficient j at
-// slot j - j0.
-__device__ __forceinline__ void limb_windows(const uint64_t* xs, int64_t j0, int64_t i, uint64_t& lo, uint64_t& hi)
+template <int L, int C = -3>
+__device__ __forceinline__ void group_limb(const uint64_t (&c)[11][3], uint64_t& lo, uint64_t& hi)
 {
-    lo = 0;
-    hi = 0;
-    if (i < 0) return;
-    int64_t jlo = floordiv56(64 * i - 141) + 1;
-    if (jlo < 0) jlo = 0;
-    const int64_t jhi = (64 * i + 63) / 56;
-    for (int64_t j = jlo; j <= jhi; j++) add128(lo, hi, coef_window(xs + 3 * (j - j0), (int)(56 * j - 64 * i)));
+    if constexpr (C <= 7) {
+        constexpr int s = 56 * C - 64 * L;
+        if constexpr (s < 64 && s > -141) add128(lo, hi, coef_win<C, L>(c[C + 3]));
+        group_limb<L, C + 1>(c, lo, hi);
+    }
+}
+
+template <int L>
+__device__ __forceinline__ void group_limbs(const uint64_t (&c)[11][3], uint64_t (&lo)[8], uint64_t (&hi)[8])
+{
+    if constexpr (L <= 6) {
+        lo[L + 1] = 0;
+        hi[L + 1] = 0;
+        group_limb<L>(c, lo[L + 1], hi[L + 1]);
+        group_limbs<L + 1>(c, lo, hi);
+    }
 }
 
 __device__ __forceinline__ void crt3d_block(const uint64_t* __restrict__ Y, size_t pstride, size_t ncoef,
                                             const CrtDConsts& C, uint32_t* __restrict__ z, size_t zw, int64_t cta,
                                             uint32_t* agg_slot)
 {
-    __shared__ uint64_t xs[3 * kCrtDSlots];
-    const int64_t i0 = cta * (int64_t)kCrtDLPC, j0 = cta * 512 - 3;
+    __shared__ uint64_t prev[kCrtDThreads][9];
+    const int64_t u = cta * kCrtDThreads + threadIdx.x;
+    const int64_t j0 = 8 * u;
     const int64_t climit = (int64_t)((32 * zw + 55) / 56);  // coefficients below the last word
-    for (int t = threadIdx.x; t < kCrtDSlots; t += blockDim.x) {
-        const int64_t j = j0 + t;
-        uint64_t l0 = 0, l1 = 0, l2 = 0;
-        if (j >= 0 && (size_t)j < ncoef && j < climit)
-            crt3d(C, dbits(Y[j]), dbits(Y[pstride + j]), dbits(Y[2 * pstride + j]), l0, l1, l2);
-        xs[3 * t] = l0;
-        xs[3 * t + 1] = l1;
-        xs[3 * t + 2] = l2;
-    }
-    __syncthreads();
-    uint64_t dig[kCvtLPT];
-    uint32_t gen[kCvtLPT];
+    const int64_t jlim = climit < (int64_t)ncoef ? climit : (int64_t)ncoef;
+    auto coef = [&](int64_t j, uint64_t (&x)[3]) {
+        x[0] = x[1] = x[2] = 0;
+        if (j >= 0 && j < jlim)
+            crt3d(C, dbits(Y[j]), dbits(Y[pstride + j]), dbits(Y[2 * pstride + j]), x[0], x[1], x[2]);
+    };
+    uint64_t c[11][3];
 #pragma unroll
-    for (int u = 0; u < kCvtLPT; u++) {
-        const int l = threadIdx.x * kCvtLPT + u;
-        dig[u] = 0;
-        gen[u] = 0;
-        if (l < (int)kCrtDLPC) {
-            uint64_t slo, shi, plo, phi;
-            limb_windows(xs, j0, i0 + l, slo, shi);
-            limb_windows(xs, j0, i0 + l - 1, plo, phi);
-            const uint64_t d = slo + phi;
-            dig[u] = d;
-            gen[u] = d < slo;
-        }
+    for (int i = 0; i < 8; i++) coef(j0 + i, c[3 + i]);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int w = 0; w < 3; w++) prev[threadIdx.x][3 * i + w] = c[8 + i][w];
+    __syncthreads();
+    if (threadIdx.x > 0) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int w = 0; w < 3; w++) c[i][w] = prev[threadIdx.x - 1][3 * i + w];
+    } else {
+#pragma unroll
+        for (int i = 0; i < 3; i++) coef(j0 - 3 + i, c[i]);
     }
-    const size_t zend = 2 * ((size_t)i0 + kCrtDLPC);
-    limbs_to_words(dig, gen, (size_t)i0 + threadIdx.x * kCvtLPT, z, zw < zend ? zw : zend, agg_slot);
+    uint64_t lo[8], hi[8];  // limbs -1 .. 6 of the group
+    lo[0] = 0;
+    hi[0] = 0;
+    group_limb<-1>(c, lo[0], hi[0]);
+    group_limbs<0>(c, lo, hi);
+    uint64_t dig[7];
+    uint32_t gen[7];
+#pragma unroll
+    for (int L = 0; L < 7; L++) {
+        const uint64_t d = lo[L + 1] + hi[L];
+        dig[L] = d;
+        gen[L] = d < lo[L + 1];
+    }
+    const size_t zend = 2 * ((size_t)cta * kCrtDLPC + kCrtDLPC);
+    limbs_to_words<7>(dig, gen, 7 * (size_t)u, z, zw < zend ? zw : zend, agg_slot);
 }
 
-__global__ void __launch_bounds__(kCvtThreads) crt3d_k1(const uint64_t* __restrict__ Y, size_t pstride,
-                                                        size_t ncoef, CrtDConsts C, uint32_t* __restrict__ z,
-                                                        size_t zw, uint32_t* agg)
+__global__ void __launch_bounds__(kCrtDThreads) crt3d_k1(const uint64_t* __restrict__ Y, size_t pstride,
+                                                         size_t ncoef, CrtDConsts C, uint32_t* __restrict__ z,
+                                                         size_t zw, uint32_t* agg)
 {
     crt3d_block(Y, pstride, ncoef, C, z, zw, (int64_t)blockIdx.x, agg + blockIdx.x);
 }
 
-__global__ void __launch_bounds__(kCvtThreads) crt3d_batch_k1(const uint64_t* __restrict__ Y, size_t istride,
-                                                              size_t pstride, size_t ncoef, CrtDConsts C,
-                                                              uint32_t* __restrict__ z, uint32_t zcap,
-                                                              const uint32_t* __restrict__ zlen, size_t cpp,
-                                                              uint32_t* agg)
+__global__ void __launch_bounds__(kCrtDThreads) crt3d_batch_k1(const uint64_t* __restrict__ Y, size_t istride,
+                                                               size_t pstride, size_t ncoef, CrtDConsts C,
+                                                               uint32_t* __restrict__ z, uint32_t zcap,
+                                                               const uint32_t* __restrict__ zlen, size_t cpp,
+                                                               uint32_t* agg)
 {
     const size_t prod = blockIdx.x / cpp, lc = blockIdx.x % cpp;
     crt3d_block(Y + prod * istride, pstride, ncoef, C, z + prod * (size_t)zcap, zlen[prod], (int64_t)lc,
@@ -934,7 +961,7 @@ static void crt3d_to_words(const uint64_t* y, size_t pstride, int k, size_t ncoe
     const size_t nctas = crt3d_ctas(zw);
     DevBuf<uint32_t> agg(nctas, s);
     ProfScope ps(KC_CRT, 24.0 * (double)ncoef + 4.0 * (double)zw, s);
-    crt3d_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(y, pstride, ncoef, C, z, zw, agg.get());
+    crt3d_k1<<<(unsigned)nctas, kCrtDThreads, 0, s>>>(y, pstride, ncoef, C, z, zw, agg.get());
     PIC_CHECK_LAUNCH();
     count_launch();
     carry_scan_aggregates(agg.get(), nctas, nullptr, s);
@@ -952,7 +979,7 @@ void ntt3d_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, siz
     DevBuf<uint32_t> agg(nctas, s);
     {
         ProfScope ps(KC_CRT, (24.0 * (double)ncoef + 4.0 * zcap) * (double)count, s);
-        crt3d_batch_k1<<<(unsigned)nctas, kCvtThreads, 0, s>>>(y, istride, pstride, ncoef, C, z, zcap, zlen, cpp,
+        crt3d_batch_k1<<<(unsigned)nctas, kCrtDThreads, 0, s>>>(y, istride, pstride, ncoef, C, z, zcap, zlen, cpp,
                                                                agg.get());
         PIC_CHECK_LAUNCH();
         count_launch();

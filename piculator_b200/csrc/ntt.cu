@@ -907,9 +907,15 @@ struct RoundPlan {
 // Row layout: transform t of the CTA at s + (t << LR), element e at swz(e).
 // With several transforms per CTA (LRPC > 0, single-pass lengths), each
 // group takes the prime of its own transform: a CTA may straddle primes.
-template <bool INV, int LR, int LRPC, int NT, int RB, int R, class A>
+// The first round reads its groups straight from global memory through
+// in(t, e, ctx) (forward: the largest stride, consecutive lanes read
+// consecutive points; inverse: a run of 2^B points per lane, through L1);
+// with OUT_DIRECT the last round (inverse: the largest stride again) writes
+// through out(t, e, v).  The rounds between exchange through shared memory.
+template <bool INV, int LR, int LRPC, int NT, int RB, int R, bool OUT_DIRECT, class A, class In, class Out>
 __device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const NttBatch& Bt, size_t row0,
-                                                const typename A::Ctx& L0, const ulonglong2* __restrict__ tw0)
+                                                const typename A::Ctx& L0, const ulonglong2* __restrict__ tw0,
+                                                const In& in, const Out& out)
 {
     using Plan = RoundPlan<LR, RB>;
     constexpr int RR = INV ? Plan::NR - 1 - R : R;
@@ -917,6 +923,7 @@ __device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const 
     constexpr int B = At::B, LB = At::LB, LST = At::LST;
     constexpr int LG = LR - B;  // log2 groups per transform
     constexpr int G = 1 << (LRPC + LG);
+    constexpr bool LAST = R + 1 == Plan::NR;
     static_assert(G % NT == 0, "groups must split evenly over the threads");
 #pragma unroll
     for (int q = 0; q < G / NT; q++) {
@@ -934,13 +941,22 @@ __device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const 
         }
         typename A::T x[1 << B];
 #pragma unroll
-        for (int m = 0; m < (1 << B); m++) x[m] = A::ld(ptr[swz(base + (m << LST))]);
+        for (int m = 0; m < (1 << B); m++) {
+            const int e = base + (m << LST);
+            if constexpr (R == 0) x[m] = in(t, e, L);
+            else x[m] = A::ld(ptr[swz(e)]);
+        }
         group_fast<B, INV, LST, A>(x, j, L, tw);
 #pragma unroll
-        for (int m = 0; m < (1 << B); m++) ptr[swz(base + (m << LST))] = A::st(x[m]);
+        for (int m = 0; m < (1 << B); m++) {
+            const int e = base + (m << LST);
+            if constexpr (LAST && OUT_DIRECT) out(t, e, x[m]);
+            else ptr[swz(e)] = A::st(x[m]);
+        }
     }
-    __syncthreads();
-    if constexpr (R + 1 < Plan::NR) rows_fast_round<INV, LR, LRPC, NT, RB, R + 1, A>(s, Bt, row0, L0, tw0);
+    if constexpr (!(LAST && OUT_DIRECT)) __syncthreads();
+    if constexpr (!LAST)
+        rows_fast_round<INV, LR, LRPC, NT, RB, R + 1, OUT_DIRECT, A>(s, Bt, row0, L0, tw0, in, out);
 }
 
 // One thread per group of a full round: 2^(LR + LRPC - RB) threads, at most
@@ -955,7 +971,9 @@ struct RowsFastShape {
 
 // Contiguous row pass: 2^LRPC rows of 2^LR points per CTA.  LRPC > 0 only
 // for single-pass lengths (k = LR, one row per transform); the last CTA may
-// hold fewer than 2^LRPC transforms.
+// hold fewer than 2^LRPC transforms.  Forward passes stage their output
+// through shared memory (their last round has the smallest stride); inverse
+// passes write it directly.
 template <bool INV, int LR, int LRPC, int RB, class A>
 __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape<LR, LRPC, RB>::MINB)
     ntt_rows_fast_kernel(NttBatch B, int k)
@@ -969,49 +987,42 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape
     const size_t nrows = (size_t)B.count << lrow;
     const PrimeDev P = pick_prime(B, (int)(row0 >> lrow));
     const typename A::Ctx L = A::ctx(P);
-    if (!INV && B.src.words != nullptr) {
-        // first forward pass of a single-pass length (row == transform): the
-        // input comes from the child slots
+    const bool from_src = !INV && B.src.words != nullptr;  // single-pass length: row == transform
+    uint64_t* __restrict__ data = B.data;
+    auto at = [&](int t, int e) {
+        const size_t row = row0 + t;
+        return (row >> lrow) * B.stride + ((row & rmask) << LR) + e;
+    };
+    auto in = [&](int t, int e, const typename A::Ctx& Lt) -> typename A::T {
+        if (LRPC > 0 && row0 + t >= nrows) return A::ld(0);
+        if (from_src) return A::piece(B, src_row(B, (int)(row0 + t)), e, Lt);
+        return A::ld(data[at(t, e)]);
+    };
+    auto out = [&](int t, int e, typename A::T v) {
+        if (LRPC == 0 || row0 + t < nrows) data[at(t, e)] = A::st(v);
+    };
+    rows_fast_round<INV, LR, LRPC, NT, RB, 0, INV, A>(
+        smem, B, row0, L, reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd), in, out);
+    if constexpr (!INV) {
 #pragma unroll
         for (int i = 0; i < TOT / NT; i++) {
             const int idx = threadIdx.x + i * NT;
             const size_t row = row0 + (idx >> LR);
-            uint64_t v = 0;
-            if (LRPC == 0 || row < nrows) {
-                const int tr = (int)row;
-                v = A::st(A::piece(B, src_row(B, tr), idx & EMASK, A::ctx(pick_prime(B, tr))));
-            }
-            smem[(idx & ~EMASK) + swz(idx & EMASK)] = v;
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < TOT / NT; i++) {
-            const int idx = threadIdx.x + i * NT;
-            const size_t row = row0 + (idx >> LR);
-            uint64_t v = 0;
             if (LRPC == 0 || row < nrows)
-                v = B.data[(row >> lrow) * B.stride + ((row & rmask) << LR) + (idx & EMASK)];
-            smem[(idx & ~EMASK) + swz(idx & EMASK)] = v;
+                data[(row >> lrow) * B.stride + ((row & rmask) << LR) + (idx & EMASK)] =
+                    smem[(idx & ~EMASK) + swz(idx & EMASK)];
         }
-    }
-    __syncthreads();
-    rows_fast_round<INV, LR, LRPC, NT, RB, 0, A>(smem, B, row0, L,
-                                             reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
-#pragma unroll
-    for (int i = 0; i < TOT / NT; i++) {
-        const int idx = threadIdx.x + i * NT;
-        const size_t row = row0 + (idx >> LR);
-        if (LRPC == 0 || row < nrows)
-            B.data[(row >> lrow) * B.stride + ((row & rmask) << LR) + (idx & EMASK)] =
-                smem[(idx & ~EMASK) + swz(idx & EMASK)];
     }
 }
 
 // Column tile: 2^LC rows x 2^LW columns, element (m, w) at s[(m << LW) + w];
-// consecutive threads take consecutive columns.
-template <bool INV, int LC, int LW, int RB, int R, class A>
+// consecutive threads take consecutive columns.  The first round reads
+// global memory through in(m, w) and the last writes it through
+// out(m, w, v), both in runs of 2^LW consecutive points; the rounds between
+// exchange through shared memory.
+template <bool INV, int LC, int LW, int RB, int R, class A, class In, class Out>
 __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const typename A::Ctx& L,
-                                                const ulonglong2* __restrict__ tw)
+                                                const ulonglong2* __restrict__ tw, const In& in, const Out& out)
 {
     using Plan = RoundPlan<LC, RB>;
     constexpr int RR = INV ? Plan::NR - 1 - R : R;
@@ -1020,6 +1031,7 @@ __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const 
     constexpr int LG = LC - B;  // log2 groups per column
     constexpr int G = 1 << (LW + LG);
     constexpr int WMASK = (1 << LW) - 1;
+    constexpr bool LAST = R + 1 == Plan::NR;
 #pragma unroll
     for (int g = threadIdx.x; g < G; g += 256) {
         const int w = g & WMASK, gi = g >> LW;
@@ -1027,13 +1039,23 @@ __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const 
         const int base = ((gi >> LST) << LB) + j;
         typename A::T x[1 << B];
 #pragma unroll
-        for (int m = 0; m < (1 << B); m++) x[m] = A::ld(s[((base + (m << LST)) << LW) + w]);
+        for (int m = 0; m < (1 << B); m++) {
+            const int r = base + (m << LST);
+            if constexpr (R == 0) x[m] = in(r, w);
+            else x[m] = A::ld(s[(r << LW) + w]);
+        }
         group_fast<B, INV, LST, A>(x, j, L, tw);
 #pragma unroll
-        for (int m = 0; m < (1 << B); m++) s[((base + (m << LST)) << LW) + w] = A::st(x[m]);
+        for (int m = 0; m < (1 << B); m++) {
+            const int r = base + (m << LST);
+            if constexpr (LAST) out(r, w, x[m]);
+            else s[(r << LW) + w] = A::st(x[m]);
+        }
     }
-    __syncthreads();
-    if constexpr (R + 1 < Plan::NR) cols_fast_round<INV, LC, LW, RB, R + 1, A>(s, L, tw);
+    if constexpr (!LAST) {
+        __syncthreads();
+        cols_fast_round<INV, LC, LW, RB, R + 1, A>(s, L, tw, in, out);
+    }
 }
 
 // floor(x 2^64 / p) for x < p: q' = floor(x mu / 2^64) with mu = floor(2^128 /
@@ -1080,14 +1102,14 @@ __global__ void pass_table_kernel(ulonglong2* __restrict__ out, PrimeDev P, int 
 // Strided column pass (same tiling as ntt_cols_kernel).  The inter-pass
 // twiddle root_(2^lblock)^((c0 + w) k1) is applied as one product with the
 // pass table, or as two with the two-level outer tables: forward after the
-// column DIF, inverse before the column DIT.
+// column DIF, inverse before the column DIT.  The tile is read by the first
+// register round and written by the last, without staging.
 // RB 4: radix-16 rounds, 16 residues per thread, two CTAs per SM.
 template <bool INV, int LC, int LW, int RB, class A>
 __global__ void __launch_bounds__(256, RB == 4 ? 2 : (INV ? 3 : 4))
     ntt_cols_fast_kernel(NttBatch B, int k, int lpre, PassTw pt)
 {
     extern __shared__ uint64_t smem[];
-    constexpr int TOT = 1 << (LC + LW), WMASK = (1 << LW) - 1;
     const int lM = k - lpre - LC;
     const int ltiles = lM - LW;
     const size_t cta = blockIdx.x;
@@ -1112,34 +1134,20 @@ __global__ void __launch_bounds__(256, RB == 4 ? 2 : (INV ? 3 : 4))
         const ulonglong2 h = __ldg(shi + (E >> S)), l = __ldg(slo + (E & smask));
         return A::twiddle(A::twiddle(v, h, L), l, L);
     };
-    if (!INV && B.src.words != nullptr) {
-        // first forward column pass (lpre == 0): the input comes from the
-        // child slot, point m M + c0 + w
-        const SrcRow sr = src_row(B, tr);
-#pragma unroll 8
-        for (int idx = threadIdx.x; idx < TOT; idx += 256) {
-            const int m = idx >> LW, w = idx & WMASK;
-            smem[idx] = A::st(A::piece(B, sr, ((size_t)m << lM) + c0 + w, L));
-        }
-    } else {
-#pragma unroll 8
-        for (int idx = threadIdx.x; idx < TOT; idx += 256) {
-            const int m = idx >> LW, w = idx & WMASK;
-            uint64_t v = base[((size_t)m << lM) + w];
-            if (INV) v = A::st(twiddle(A::ld(v), m, w));
-            smem[idx] = v;
-        }
-    }
-    __syncthreads();
+    // first forward column pass (lpre == 0) with a split source: point
+    // m M + c0 + w comes from the child slot
+    const bool from_src = !INV && B.src.words != nullptr;
+    const SrcRow sr = from_src ? src_row(B, tr) : SrcRow{nullptr, 0};
+    auto in = [&](int m, int w) -> typename A::T {
+        if (from_src) return A::piece(B, sr, ((size_t)m << lM) + c0 + w, L);
+        const typename A::T v = A::ld(base[((size_t)m << lM) + w]);
+        return INV ? twiddle(v, m, w) : v;
+    };
+    auto out = [&](int m, int w, typename A::T v) {
+        base[((size_t)m << lM) + w] = A::st(INV ? v : twiddle(v, m, w));
+    };
     cols_fast_round<INV, LC, LW, RB, 0, A>(smem, L,
-                                           reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd));
-#pragma unroll 8
-    for (int idx = threadIdx.x; idx < TOT; idx += 256) {
-        const int m = idx >> LW, w = idx & WMASK;
-        uint64_t v = smem[idx];
-        if (!INV) v = A::st(twiddle(A::ld(v), m, w));
-        base[((size_t)m << lM) + w] = v;
-    }
+                                           reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd), in, out);
 }
 
 // The SplitSrc input written into `data` (for passes that read `data`).
@@ -1248,16 +1256,17 @@ constexpr int kPassTableMaxBits = 24;
 static std::mutex g_pass_lock;
 static std::map<std::tuple<int, uint64_t, int, int, int>, ulonglong2*> g_pass_tables;
 
-// FP64 column passes stream the per-point table only when this is set: their
-// FP64 pipe has room to form each twiddle from the two-level tables (two
-// products), which saves 16 bytes of DRAM traffic per point.
-static bool g_dbl_pass_tables = false;
-void ntt_set_dbl_pass_tables(bool on) { g_dbl_pass_tables = on; }
-bool ntt_dbl_pass_tables() { return g_dbl_pass_tables; }
+// FP64 column passes stream the per-point table only for blocks of at most
+// 2^g_dbl_pass_bits points (tables that stay in L2); longer ones form each
+// twiddle from the two-level tables (two products on the FP64 pipe, which
+// has room), saving 16 bytes of DRAM traffic per point.
+static int g_dbl_pass_bits = 20;
+void ntt_set_dbl_pass_bits(int bits) { g_dbl_pass_bits = bits; }
+int ntt_dbl_pass_bits() { return g_dbl_pass_bits; }
 
 static const ulonglong2* pass_table(const PrimeDev& P, bool inv, int lblock, int lc, cudaStream_t s)
 {
-    if (lblock > kPassTableMaxBits || (P.fp64 && !g_dbl_pass_tables)) return nullptr;
+    if (lblock > kPassTableMaxBits || (P.fp64 && lblock > g_dbl_pass_bits)) return nullptr;
     int dev = 0;
     PIC_CUDA(cudaGetDevice(&dev));
     const auto key = std::make_tuple(dev, P.p, inv ? 1 : 0, lblock, lc);

@@ -138,9 +138,10 @@ std::vector<int> ntt_pass_bits(int k, int form = kFormInt);
 // log2 width 0..6 with 0 = automatic, bits per register round 2..4; the FP64
 // form runs only the fast passes: row bits 11..13, rounds of 3 or 4 bits).
 void ntt_set_geometry(int k, int row_bits, int col_lw, int rbits, int form = kFormInt);
-// FP64 column passes: per-point twiddle tables (on) or two-level tables (off, default).
-void ntt_set_dbl_pass_tables(bool on);
-bool ntt_dbl_pass_tables();
+// FP64 column passes use per-point twiddle tables for blocks of at most
+// 2^bits points (0: never), else the two-level tables.
+void ntt_set_dbl_pass_bits(int bits);
+int ntt_dbl_pass_bits();
 void ntt_get_geometry(int k, int* row_bits, int* col_lw, int* rbits, int form = kFormInt);
 
 }  // namespace pic

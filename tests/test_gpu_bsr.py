@@ -25,9 +25,11 @@ def _same(dev, want) -> bool:
 # Combine: P formed in the transform domain (1) or from two separate products (0).
 @pytest.mark.parametrize("school_max,wrap,small,combine", [(192, 1, 2, 1), (192, 1, 0, 1), (8, 1, 2, 1),
                                                            (8, 0, 2, 1), (8, 1, 2, 0)])
-def test_bsr_vs_oracle(pic, oracle, a, b, p, school_max, wrap, small, combine):
+# Three-prime form of the NTT merges: integer (0) or FP64 (1).
+@pytest.mark.parametrize("form", [0, 1])
+def test_bsr_vs_oracle(pic, oracle, a, b, p, school_max, wrap, small, combine, form):
     knobs = {pic.TUNE_BSR_SCHOOL_MAX: school_max, pic.TUNE_BSR_WRAP: wrap, pic.TUNE_BSR_SMALL_MERGE: small,
-             pic.TUNE_BSR_COMBINE: combine}
+             pic.TUNE_BSR_COMBINE: combine, pic.TUNE_NTT_FORM: form}
     saved = {k: pic.get_tuning(k) for k in knobs}
     for k, v in knobs.items():
         pic.set_tuning(k, v)

@@ -94,3 +94,31 @@ def test_large_products_agree_with_integer_form(pic, lg):
     n = 1 << lg
     a, b = random_words(42, n), random_words(43, n)
     assert np.array_equal(pic.mul_host(a, b, "ntt3d"), pic.mul_host(a, b, "ntt3"))
+
+
+def _pi_in_form(pic, digits, form):
+    saved = pic.get_tuning(pic.TUNE_NTT_FORM)
+    pic.set_tuning(pic.TUNE_NTT_FORM, form)
+    try:
+        return pic.pi_hex(digits, pic.PI_CHOSEN)
+    finally:
+        pic.set_tuning(pic.TUNE_NTT_FORM, saved)
+
+
+@pytest.mark.parametrize("digits", [10_000, 100_000, 1_000_000, 3_141_593, 10_000_000, 27_182_818])
+def test_pi_in_fp64_form_matches_reference(pic, golden, digits):
+    """The whole computation (binary-splitting merges, Newton products) in the
+    FP64 form: every hex digit equal to the reference's pi.txt."""
+    import hashlib
+    text, _ = _pi_in_form(pic, digits, pic.FORM_DBL)
+    g = golden["pi"][str(digits)]
+    assert len(text) == g["bytes"]
+    assert hashlib.md5(text).hexdigest() == g["md5"]
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("digits", [100_000_000, 1_000_000_000])
+def test_pi_in_fp64_form_large(pic, golden, digits):
+    import hashlib
+    text, _ = _pi_in_form(pic, digits, pic.FORM_DBL)
+    assert hashlib.md5(text).hexdigest() == golden["pi"][str(digits)]["md5"]
