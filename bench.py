@@ -242,37 +242,44 @@ def replica_check(args):
         dist.destroy_process_group()
 
 
-def int_roof(P, torch, L, stream):
-    """Row-pass butterflies per second on a 2^23-word three-prime product
-    (3 row passes per product, each over 3 x 2^23 points and row_bits levels)
-    against the register-only butterfly ceiling."""
+def arith_roof(P, torch, L, stream):
+    """Row-pass butterflies per second on a three-prime product of two
+    0.8 * 2^23-word operands in the active form (a plain transform of length
+    2^23 in both forms; 3 row passes per product, each over 3 x 2^23 points
+    and row_bits levels) against the register-only butterfly ceiling of that
+    form's arithmetic."""
     import ctypes as C
 
-    k, n = 23, 1 << 23
-    row_bits = P.get_ntt_geometry(k)[0]
+    form = P.get_tuning(P.TUNE_NTT_FORM)
+    mode = "ntt3d" if form == P.FORM_DBL else "ntt3"
+    k = 23
+    n = int(0.8 * (1 << k))
+    row_bits = P.get_ntt_geometry(k, form)[0]
     a = torch.randint(-2**31, 2**31 - 1, (n,), dtype=torch.int32, device="cuda")
     b = torch.randint(-2**31, 2**31 - 1, (n,), dtype=torch.int32, device="cuda")
     z = torch.empty(2 * n, dtype=torch.int32, device="cuda")
     for _ in range(2):
-        P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, "ntt3")
+        P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, mode)
     torch.cuda.synchronize()
     P.check(L.pic_profile_begin())
     reps = 5
     for _ in range(reps):
-        P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, "ntt3")
+        P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, mode)
     stats = (P.KernelStat * 32)()
     cnt = C.c_int()
     P.check(L.pic_profile_end(stats, 32, C.byref(cnt)))
     rows = [s for s in stats[: cnt.value] if s.name.decode() == "ntt_rows"]
     if not rows or rows[0].seconds <= 0:
         return None
-    bfly = rows[0].launches * 3 * (n // 2) * row_bits
+    bfly = rows[0].launches * 3 * (1 << (k - 1)) * row_bits
     achieved = bfly / rows[0].seconds / 1e9
-    ceiling = P.butterfly_rate()
-    return {"kernel": "ntt_rows", "workload": "three-prime product of two 2^23-word operands",
+    ceiling = P.butterfly_rate(form)
+    basis = ("FP64 modular DIF butterflies (about nine FP64 instructions each)" if form == P.FORM_DBL
+             else "lazy Shoup DIF butterflies") + " with operands in registers, no memory traffic"
+    return {"kernel": "ntt_rows", "form": "fp64" if form == P.FORM_DBL else "integer",
+            "workload": f"three-prime product of two {n}-word operands (transform length 2^{k})",
             "row_bits": row_bits, "achieved": achieved, "ceiling": ceiling, "unit": "G butterflies/s",
-            "frac": achieved / ceiling,
-            "ceiling_basis": "lazy Shoup DIF butterflies with operands in registers, no memory traffic"}
+            "frac": achieved / ceiling, "ceiling_basis": basis}
 
 
 def batched_products(P, torch, L, stream, count: int = 8192, top: int = 8192, seed: int = 7):
@@ -318,10 +325,26 @@ def batched_products(P, torch, L, stream, count: int = 8192, top: int = 8192, se
             "speedup": single / batched}
 
 
+def transform_bits(coefs: int, per_max: int) -> list:
+    """Transform lengths (log2) of one three-prime product with `coefs`
+    coefficients and operands of at most per_max pieces: one of 2^k, or the
+    wrapped form's main 2^(k-1) and tail 2^kt (the rule of mul_ntt3 and
+    mul_ntt3d with wrapped products on)."""
+    k = max(1, (coefs - 1).bit_length())
+    if k >= 4:
+        nm = 1 << (k - 1)
+        if per_max <= nm < coefs:
+            kt = max(2, (2 * (coefs - nm) - 2).bit_length())
+            if (1 << kt) <= nm // 2:
+                return [k - 1, kt]
+    return [k]
+
+
 def isolated_products(P, torch, L, stream):
     """The isolated-multiply workload: two N-limb operands (splitmix64 seeds 42
-    and 43), N = 2^12 ... 2^27, exact three-prime NTT product through pic_mul
-    (inputs resident in HBM), its words checked against the reference's md5;
+    and 43), N = 2^12 ... 2^27, exact three-prime NTT product in both forms
+    (integer and FP64) through pic_mul (inputs resident in HBM), its words
+    checked against the reference's md5;
     where a proven FP64 piece width exists, the FFT product's time and its
     largest rounding distance.  B_mul = bytes of the transforms (two forward,
     one inverse; 16 B per point and pass, three primes) + 4 (na + nb + nz)."""
@@ -339,7 +362,7 @@ def isolated_products(P, torch, L, stream):
         b = torch.from_numpy(random_words(43, n).view(np.int32)).cuda()
         z = torch.empty(2 * n, dtype=torch.int32, device="cuda")
         rec = {"log2n": lg}
-        for mode in ("ntt3", "fft"):
+        for mode in ("ntt3", "ntt3d", "fft"):
             if mode == "fft" and lg > 20:
                 continue
             P.mul_dev(z.data_ptr(), a.data_ptr(), n, b.data_ptr(), n, mode)
@@ -356,13 +379,16 @@ def isolated_products(P, torch, L, stream):
             L_ = w.size - (1 if w[-1] == 0 else 0)
             ok = hashlib.md5(w[:L_].tobytes()).hexdigest() == gold[lg]["md5"] if lg in gold else None
             rec[mode] = {"ms": ms, "matches_reference": ok}
-            if mode == "ntt3":
-                pieces = 2 * (n // 2) - 1
-                k = max(1, (pieces - 1).bit_length())
-                # passes of the tuned geometry: one up to 2^13 points, else
-                # ceil((k - row bits) / 11) column passes and the row pass
-                passes = 1 if k <= 13 else 1 + -(-(k - P.get_ntt_geometry(k)[0]) // 11)
-                b_mul = 3 * 3 * passes * 16.0 * (1 << k) + 4.0 * 4 * n
+            if mode in ("ntt3", "ntt3d"):
+                # coefficients of the product: 64-bit pieces, or 56-bit in the FP64 form
+                per = n // 2 if mode == "ntt3" else -(-32 * n // 56)
+                form = P.FORM_DBL if mode == "ntt3d" else P.FORM_INT
+                b_mul = 4.0 * 4 * n
+                for k in transform_bits(2 * per - 1, per):
+                    # passes of the tuned geometry: one up to 2^13 points, else
+                    # ceil((k - row bits) / 11) column passes and the row pass
+                    passes = 1 if k <= 13 else 1 + -(-(k - P.get_ntt_geometry(k, form)[0]) // 11)
+                    b_mul += 3 * 3 * passes * 16.0 * (1 << k)
                 rec[mode]["B_mul_GB"] = b_mul / 1e9
                 rec[mode]["GBps"] = b_mul / (ms * 1e-3) / 1e9
             else:
@@ -473,29 +499,37 @@ def ours(args):
     top = max(kstats, key=lambda k: k["seconds"])
     achieved = top["bytes"] / top["seconds"] / 1e9 if top["seconds"] > 0 else 0.0
     total_k = sum(k["seconds"] for k in kstats) or 1.0
-    # DRAM bytes per algorithmic byte of the NTT passes, from one ncu capture of
-    # the 2^23-word three-prime product (dram__bytes_read.sum +
-    # dram__bytes_write.sum over 16 B per point): the row pass moves 14.9 B per
-    # point, the column pass 30.8 B (data plus its twiddle table); both are per
-    # point, so they scale to a launch of any size.
-    dram_per_alg = {"ntt_rows": 14.9 / 16.0, "ntt_cols": 30.8 / 16.0}
+    # DRAM bytes per algorithmic byte (16 B per point and pass) of the NTT
+    # passes: dram__bytes_read.sum + dram__bytes_write.sum of every launch of
+    # the kernel in one 1e9-digit computation (ncu, one pass per launch), over
+    # the kernel's algorithmic bytes in the same computation.  FP64 form: rows
+    # 1591.5 GB / 1739.5 GB, columns 1786.5 GB / 1763.6 GB (their per-point
+    # twiddle tables mostly hit L2).  Integer form, from the 2^23-word product:
+    # rows 14.9 B and columns 30.8 B per point.
+    if P.get_tuning(P.TUNE_NTT_FORM) == P.FORM_DBL:
+        dram_per_alg = {"ntt_rows": 1591.5 / 1739.5, "ntt_cols": 1786.5 / 1763.6}
+        traffic_basis = ("ncu DRAM bytes of every launch of the kernel in one 1e9-digit computation over its "
+                         "algorithmic bytes, times the kernel's average launch")
+    else:
+        dram_per_alg = {"ntt_rows": 14.9 / 16.0, "ntt_cols": 30.8 / 16.0}
+        traffic_basis = "ncu DRAM bytes per point of the 2^23-word product, scaled to the kernel's average launch"
     avg_bytes = top["bytes"] / max(top["launches"], 1)
     traffic = avg_bytes * dram_per_alg[top["name"]] if top["name"] in dram_per_alg else None
     roofline = {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "traffic_basis": "ncu DRAM bytes per point of the 2^23-word product, scaled "
-                                                     "to the kernel's average launch",
+                "traffic": traffic, "traffic_basis": traffic_basis,
                 "launches": top["launches"],
                 "avg_launch_ms": 1e3 * top["seconds"] / max(top["launches"], 1),
                 "share_of_kernel_time": top["seconds"] / total_k,
                 "measured": "CUDA events around every launch of the kernel, over K extra profiled steps"}
 
-    # The integer roofline of the same passes: butterflies per second of the
-    # row pass on the 2^23-word three-prime product against the register-only
-    # butterfly rate of this GPU (pic_measure_butterfly_rate).
-    int_roofline = None
+    # The arithmetic roofline of the same passes: butterflies per second of
+    # the row pass on a 2^23-point three-prime product in the active form
+    # against the register-only butterfly rate of that arithmetic
+    # (pic_measure_butterfly_rate_form).
+    arith_roofline = None
     if rank == 0:
-        int_roofline = int_roof(P, torch, L, stream)
+        arith_roofline = arith_roof(P, torch, L, stream)
 
     plain = None
     if not args.no_plain and rank == 0:
@@ -602,7 +636,7 @@ def ours(args):
             "digits_check": digits_check,
             "gpu_launches": int(launches),
             "roofline": roofline,
-            "int_roofline": int_roofline,
+            "arith_roofline": arith_roofline,
             "cpu_baseline": cpu,
             "measured_vs_reference": like,
             "pi_1e8_s": pi_1e8,

@@ -72,6 +72,9 @@ pic_status pic_profile_end(pic_kernel_stat* out, int cap, int* n);
  * butterflies per second (in G) with operands in registers and no memory
  * traffic.  No reference counterpart (a measurement aid). */
 pic_status pic_measure_butterfly_rate(double* gbfly_per_s);
+/* The same per product form: 0 the integer butterflies above, 1 the FP64
+ * form's (FP64 modular products, about nine FP64 instructions each). */
+pic_status pic_measure_butterfly_rate_form(int form, double* gbfly_per_s);
 
 /* Test hook: make the next n device allocations fail with PIC_ERR_NO_MEMORY
  * (host-side fault injection; no GPU fault is involved). */

@@ -91,6 +91,7 @@ _SIGS = {
     "pic_profile_begin": ([], C.c_int),
     "pic_profile_end": ([C.POINTER(KernelStat), C.c_int, C.POINTER(C.c_int)], C.c_int),
     "pic_measure_butterfly_rate": ([C.POINTER(C.c_double)], C.c_int),
+    "pic_measure_butterfly_rate_form": ([C.c_int, C.POINTER(C.c_double)], C.c_int),
     "pic_pi_compute": ([C.c_uint64, C.c_int, C.POINTER(C.c_void_p), C.POINTER(PiStats)], C.c_int),
     "pic_ntt_ensure_table": ([C.c_int], C.c_int),
     "pic_ntt_forward": ([_U64P, C.c_int, _P], C.c_int),
@@ -375,11 +376,11 @@ class Transform:
  TUNE_NTT_FORM, TUNE_DBL_PASS_TABLES) = range(12)
 
 
-def butterfly_rate() -> float:
-    """G lazy Shoup butterflies per second with everything in registers: the
-    integer ceiling the NTT passes are measured against."""
+def butterfly_rate(form: int = FORM_INT) -> float:
+    """G butterflies per second with everything in registers (integer lazy
+    Shoup, or the FP64 form's): the arithmetic ceiling of the NTT passes."""
     v = C.c_double(0.0)
-    check(lib().pic_measure_butterfly_rate(C.byref(v)))
+    check(lib().pic_measure_butterfly_rate_form(form, C.byref(v)))
     return v.value
 
 

@@ -145,6 +145,16 @@ pic_status pic_measure_butterfly_rate(double* gbfly_per_s)
     });
 }
 
+pic_status pic_measure_butterfly_rate_form(int form, double* gbfly_per_s)
+{
+    return guarded([&] {
+        require_init();
+        PIC_REQ_PTR(gbfly_per_s);
+        PIC_REQUIRE(form == 0 || form == 1, PIC_ERR_INVALID, "unknown product form");
+        *gbfly_per_s = form == 1 ? butterfly_ceiling_dbl(ctx().stream) : butterfly_ceiling(ctx().stream);
+    });
+}
+
 // ---- NTT.h ---------------------------------------------------------------------
 static PrimeDev ref_prime_dev(int k)
 {

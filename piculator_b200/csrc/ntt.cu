@@ -6,6 +6,7 @@
 #include <tuple>
 #include <vector>
 #include <mutex>
+#include <type_traits>
 
 #include "common.cuh"
 #include "fp64mod.cuh"
@@ -1105,8 +1106,19 @@ __global__ void pass_table_kernel(ulonglong2* __restrict__ out, PrimeDev P, int 
 // column DIF, inverse before the column DIT.  The tile is read by the first
 // register round and written by the last, without staging.
 // RB 4: radix-16 rounds, 16 residues per thread, two CTAs per SM.
+// Resident CTAs per SM the column kernels are compiled for (the register
+// budget): radix-16 two; radix-8 integer four forward, three inverse; FP64
+// PIC_DBL_COLS_MINB.
+#ifndef PIC_DBL_COLS_MINB
+#define PIC_DBL_COLS_MINB 4
+#endif
+template <class A, int RB, bool INV>
+struct ColsMinBlocks {
+    static constexpr int value = RB == 4 ? 2 : (std::is_same<A, ArithDbl>::value ? PIC_DBL_COLS_MINB : (INV ? 3 : 4));
+};
+
 template <bool INV, int LC, int LW, int RB, class A>
-__global__ void __launch_bounds__(256, RB == 4 ? 2 : (INV ? 3 : 4))
+__global__ void __launch_bounds__(256, ColsMinBlocks<A, RB, INV>::value)
     ntt_cols_fast_kernel(NttBatch B, int k, int lpre, PassTw pt)
 {
     extern __shared__ uint64_t smem[];

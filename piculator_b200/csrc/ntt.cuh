@@ -131,6 +131,8 @@ void ntt_scale_ninv(uint64_t* T, int k, const PrimeDev& P, cudaStream_t s);
 
 // G lazy Shoup butterflies per second with operands in registers (ceiling.cu).
 double butterfly_ceiling(cudaStream_t s);
+// The same for the FP64 form's butterflies (about nine FP64 instructions each).
+double butterfly_ceiling_dbl(cudaStream_t s);
 
 // Pass split used for length 2^k (for reporting / tests).
 std::vector<int> ntt_pass_bits(int k, int form = kFormInt);
