@@ -595,16 +595,18 @@ def ours(args):
         ratio = reference_ratio(args.digits, sample)
         if os.path.exists(REF_PI):
             threads = os.cpu_count() or 1
-            t_ref = run_reference_pi(sample, threads)
-            # the GPU's own time on the same sample, for a measured ratio
+            # the GPU's own time on the same sample, for a measured ratio,
+            # taken while the GPU is still busy from the runs above (after the
+            # seconds of CPU-only work below its first runs were 2-7x slower)
             gpu_runs = []
-            for _ in range(4):  # the first run at a new size builds its tables
+            for _ in range(6):  # the first run at a new size builds its tables
                 h = C.c_void_p()
                 st2 = P.PiStats()
                 P.check(L.pic_pi_compute(sample, P.PI_CHOSEN, C.byref(h), C.byref(st2)))
                 L.pic_bf_free(h)
                 gpu_runs.append(st2.seconds_total)
             gpu_s = min(gpu_runs[1:])
+            t_ref = run_reference_pi(sample, threads)
             like = {"digits": sample, "reference_s": t_ref, "reference_threads": threads,
                     "gpu_s": gpu_s, "gpu_runs_s": gpu_runs, "ratio": t_ref / gpu_s}
             if ratio is not None:
