@@ -1021,9 +1021,17 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape
 // global memory through in(m, w) and the last writes it through
 // out(m, w, v), both in runs of 2^LW consecutive points; the rounds between
 // exchange through shared memory.
-template <bool INV, int LC, int LW, int RB, int R, class A, class In, class Out>
+// PIC_COLS_TW_PREFETCH (default on): the last forward round loads its
+// pass-table twiddles before its butterflies, so their latency overlaps the
+// arithmetic (out(r, w, v, t) then applies them).
+#ifndef PIC_COLS_TW_PREFETCH
+#define PIC_COLS_TW_PREFETCH 1
+#endif
+
+template <bool INV, int LC, int LW, int RB, int R, class A, class In, class Out, class Pre>
 __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const typename A::Ctx& L,
-                                                const ulonglong2* __restrict__ tw, const In& in, const Out& out)
+                                                const ulonglong2* __restrict__ tw, const In& in, const Out& out,
+                                                const Pre& pre)
 {
     using Plan = RoundPlan<LC, RB>;
     constexpr int RR = INV ? Plan::NR - 1 - R : R;
@@ -1045,17 +1053,24 @@ __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const 
             if constexpr (R == 0) x[m] = in(r, w);
             else x[m] = A::ld(s[(r << LW) + w]);
         }
+        constexpr bool PRE = LAST && !INV && PIC_COLS_TW_PREFETCH;
+        ulonglong2 tp[PRE ? (1 << B) : 1];
+        if constexpr (PRE) {
+#pragma unroll
+            for (int m = 0; m < (1 << B); m++) tp[m] = pre(base + (m << LST), w);
+        }
         group_fast<B, INV, LST, A>(x, j, L, tw);
 #pragma unroll
         for (int m = 0; m < (1 << B); m++) {
             const int r = base + (m << LST);
-            if constexpr (LAST) out(r, w, x[m]);
+            if constexpr (PRE) out(r, w, x[m], &tp[m]);
+            else if constexpr (LAST) out(r, w, x[m], nullptr);
             else s[(r << LW) + w] = A::st(x[m]);
         }
     }
     if constexpr (!LAST) {
         __syncthreads();
-        cols_fast_round<INV, LC, LW, RB, R + 1, A>(s, L, tw, in, out);
+        cols_fast_round<INV, LC, LW, RB, R + 1, A>(s, L, tw, in, out, pre);
     }
 }
 
@@ -1155,11 +1170,18 @@ __global__ void __launch_bounds__(256, ColsMinBlocks<A, RB, INV>::value)
         const typename A::T v = A::ld(base[((size_t)m << lM) + w]);
         return INV ? twiddle(v, m, w) : v;
     };
-    auto out = [&](int m, int w, typename A::T v) {
-        base[((size_t)m << lM) + w] = A::st(INV ? v : twiddle(v, m, w));
+    // pre(m, w): the pass-table pair of point (m, w) (zero without a table);
+    // out applies a preloaded pair when it gets one
+    auto pre = [&](int m, int w) -> ulonglong2 {
+        return T != nullptr ? __ldg(T + ((size_t)m << lM) + c0 + w) : make_ulonglong2(0, 0);
+    };
+    auto out = [&](int m, int w, typename A::T v, const ulonglong2* t) {
+        if (!INV) v = (t != nullptr && T != nullptr) ? A::twiddle(v, *t, L) : twiddle(v, m, w);
+        base[((size_t)m << lM) + w] = A::st(v);
     };
     cols_fast_round<INV, LC, LW, RB, 0, A>(smem, L,
-                                           reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd), in, out);
+                                           reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd), in, out,
+                                           pre);
 }
 
 // The SplitSrc input written into `data` (for passes that read `data`).
