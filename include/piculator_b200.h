@@ -296,9 +296,13 @@ enum {
                                      least this many words (0 = never) */
     PIC_TUNE_NTT_FORM = 10,       /* three-prime form of AUTO products and binary-splitting merges:
                                      0 integer (PIC_MUL_NTT3), 1 FP64 (PIC_MUL_NTT3D) */
-    PIC_TUNE_DBL_PASS_TABLES = 11 /* FP64 column passes over blocks of at most 2^value points (0..24,
+    PIC_TUNE_DBL_PASS_TABLES = 11, /* FP64 column passes over blocks of at most 2^value points (0..24,
                                      default 20) stream per-point twiddle tables; longer blocks form the
                                      twiddles from the two-level tables */
+    PIC_TUNE_COLS_BULK = 12       /* 8..12: FP64 column passes of 2^5 .. 2^9 rows run the persistent
+                                     kernel whose tiles (at most 2^value points) arrive by TMA bulk
+                                     copies (bounded waits: a wait past ~1 s of SM clocks ends the pass
+                                     with PIC_ERR_TIMEOUT); 0 (default): one tile per CTA */
 };
 pic_status pic_set_tuning(int knob, int64_t value);
 int64_t pic_get_tuning(int knob);

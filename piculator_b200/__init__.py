@@ -213,6 +213,8 @@ def apply_tuning(path: str = TUNING_FILE) -> bool:
         check(L.pic_set_tuning(TUNE_NTT_FORM, int(prod["ntt_form"])))
     if "dbl_pass_bits" in prod:
         check(L.pic_set_tuning(TUNE_DBL_PASS_TABLES, int(prod["dbl_pass_bits"])))
+    if "cols_bulk" in prod:
+        check(L.pic_set_tuning(TUNE_COLS_BULK, int(prod["cols_bulk"])))
     return True
 
 
@@ -373,7 +375,7 @@ class Transform:
 
 (TUNE_BSR_SCHOOL_MAX, TUNE_MUL_SCHOOL_MAX, TUNE_MUL_FFT_MAX, TUNE_BATCH_GRAPHS, TUNE_BSR_WRAP,
  TUNE_BSR_SMALL_MERGE, TUNE_MUL_WRAP, TUNE_BSR_COMBINE, TUNE_FFT_ACCEPT_PPM, TUNE_BSR_KARATSUBA,
- TUNE_NTT_FORM, TUNE_DBL_PASS_TABLES) = range(12)
+ TUNE_NTT_FORM, TUNE_DBL_PASS_TABLES, TUNE_COLS_BULK) = range(13)
 
 
 def butterfly_rate(form: int = FORM_INT) -> float:

@@ -108,6 +108,7 @@ pic_status pic_synchronize(void)
     return guarded([&] {
         require_init();
         PIC_CUDA(cudaStreamSynchronize(ctx().stream));
+        PIC_REQUIRE(!ntt_take_bulk_error(), PIC_ERR_TIMEOUT, "a bulk-copy wait of an NTT column pass timed out");
     });
 }
 
@@ -656,6 +657,11 @@ pic_status pic_set_tuning(int knob, int64_t value)
             PIC_REQUIRE(value <= 1, PIC_ERR_INVALID, "product form is 0 (integer) or 1 (FP64)");
             mul_set_ntt_form((int)value);
             break;
+        case PIC_TUNE_COLS_BULK:
+            PIC_REQUIRE(value == 0 || (value >= 8 && value <= 12), PIC_ERR_INVALID,
+                        "bulk column tiles are 2^8 .. 2^12 points (0: off)");
+            ntt_set_cols_bulk((int)value);
+            break;
         case PIC_TUNE_DBL_PASS_TABLES:
             PIC_REQUIRE(value <= 24, PIC_ERR_INVALID, "FP64 pass-table bits are 0..24");
             ntt_set_dbl_pass_bits((int)value);
@@ -711,6 +717,7 @@ int64_t pic_get_tuning(int knob)
     case PIC_TUNE_BSR_KARATSUBA: return bsr_karatsuba();
     case PIC_TUNE_NTT_FORM: return mul_ntt_form();
     case PIC_TUNE_DBL_PASS_TABLES: return ntt_dbl_pass_bits();
+    case PIC_TUNE_COLS_BULK: return ntt_cols_bulk();
     }
     return -1;
 }

@@ -2,6 +2,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <map>
 #include <tuple>
 #include <vector>
@@ -1184,6 +1185,176 @@ __global__ void __launch_bounds__(256, ColsMinBlocks<A, RB, INV>::value)
                                            pre);
 }
 
+// ---- column passes fed by TMA bulk copies ------------------------------------
+// A persistent CTA walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
+// Each row of a tile (2^LW consecutive points, and the matching 2^LW pass-table
+// pairs) is one contiguous, 16-byte-aligned run, so warp 0 fetches a tile with
+// 2^LC bulk copies (cp.async.bulk, no multicast) that complete on an
+// mbarrier; two buffers let the copies of tile i + 1 land while tile i is
+// computed.  Every wait is bounded: a wait that outlasts ~1 s of SM clocks
+// sets g_ntt_bulk_error, drains the other buffer's copy (also bounded) and
+// ends the CTA; the host turns the flag into PIC_ERR_TIMEOUT.
+
+__device__ int g_ntt_bulk_error;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase with the given parity; false after ~2^31 SM clocks.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > (1ll << 31)) return false;
+    return true;
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+struct BulkTile {
+    int tr;
+    uint64_t* base;        // the tile's first point (row 0, column c0)
+    const ulonglong2* T;   // its pass-table rows (null: two-level tables)
+    uint32_t c0;
+};
+
+__device__ __forceinline__ BulkTile bulk_tile(const NttBatch& B, const PassTw& pt, int k, int lpre, int lM, int LW,
+                                              size_t t)
+{
+    const int ltiles = lM - LW;
+    BulkTile r;
+    r.tr = (int)(t >> (ltiles + lpre));
+    const size_t rem = t & (((size_t)1 << (ltiles + lpre)) - 1);
+    const size_t ob = rem >> ltiles;
+    r.c0 = (uint32_t)((rem & (((size_t)1 << ltiles) - 1)) << LW);
+    r.base = B.data + (size_t)r.tr * B.stride + (ob << (k - lpre)) + r.c0;
+    r.T = r.tr < B.per_prime ? pt.t[0] : (r.tr < 2 * B.per_prime ? pt.t[1] : pt.t[2]);
+    return r;
+}
+
+// Warp 0 fetches tile t into (d, tb) completing on bar.
+template <int LC, int LW>
+__device__ __forceinline__ void bulk_fetch(const BulkTile& tl, int lM, uint64_t* d, ulonglong2* tb, uint64_t* bar)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t bytes = (uint32_t)((8u + (tl.T != nullptr ? 16u : 0u)) << (LC + LW));
+    if (lane == 0) mbar_expect_tx(bar, bytes);
+    __syncwarp();
+    for (int m = lane; m < (1 << LC); m += 32) {
+        bulk_load(d + (m << LW), tl.base + ((size_t)m << lM), 8u << LW, bar);
+        if (tl.T != nullptr) bulk_load(tb + (m << LW), tl.T + ((size_t)m << lM) + tl.c0, 16u << LW, bar);
+    }
+}
+
+template <int LC, int LW, bool TAB>
+struct BulkShape {
+    static constexpr int TOT = 1 << (LC + LW);
+    static constexpr size_t DATA = sizeof(uint64_t) * TOT;
+    static constexpr size_t TABB = TAB ? sizeof(ulonglong2) * TOT : 0;
+    static constexpr size_t SMEM = 2 * (DATA + TABB) + 64;  // two buffers and the barriers
+};
+
+template <bool INV, int LC, int LW, int RB, bool TAB, class A>
+__global__ void __launch_bounds__(256, 2) ntt_cols_bulk_kernel(NttBatch B, int k, int lpre, PassTw pt, size_t ntiles)
+{
+    using Sh = BulkShape<LC, LW, TAB>;
+    extern __shared__ __align__(128) uint64_t bsm[];
+    uint64_t* dbuf[2] = {bsm, bsm + Sh::TOT};
+    ulonglong2* tbuf[2] = {reinterpret_cast<ulonglong2*>(bsm + 2 * Sh::TOT),
+                           reinterpret_cast<ulonglong2*>(bsm + 2 * Sh::TOT) + Sh::TOT};
+    uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(bsm) + 2 * (Sh::DATA + Sh::TABB));
+    const int lM = k - lpre - LC;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        fence_async_smem();
+    }
+    __syncthreads();
+    const size_t t0 = blockIdx.x, step = gridDim.x;
+    if (threadIdx.x < 32) {
+        if (t0 < ntiles) bulk_fetch<LC, LW>(bulk_tile(B, pt, k, lpre, lM, LW, t0), lM, dbuf[0], tbuf[0], &bars[0]);
+        if (t0 + step < ntiles)
+            bulk_fetch<LC, LW>(bulk_tile(B, pt, k, lpre, lM, LW, t0 + step), lM, dbuf[1], tbuf[1], &bars[1]);
+    }
+    size_t it = 0;
+    for (size_t t = t0; t < ntiles; t += step, it++) {
+        const int b = (int)(it & 1);
+        const bool ok = mbar_wait_bounded(&bars[b], (uint32_t)((it >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicExch(&g_ntt_bulk_error, 1);
+                if (t + step < ntiles) mbar_wait_bounded(&bars[b ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
+            }
+            return;
+        }
+        const BulkTile tl = bulk_tile(B, pt, k, lpre, lM, LW, t);
+        const PrimeDev P = pick_prime(B, tl.tr);
+        const typename A::Ctx L = A::ctx(P);
+        uint64_t* __restrict__ d = dbuf[b];
+        const ulonglong2* __restrict__ tb = tbuf[b];
+        const bool tab = TAB && tl.T != nullptr;
+        const int esh = P.K - (k - lpre);
+        const int S = P.S;
+        const uint64_t smask = ((uint64_t)1 << S) - 1;
+        const ulonglong2* __restrict__ slo = reinterpret_cast<const ulonglong2*>(INV ? P.slo_inv : P.slo_fwd);
+        const ulonglong2* __restrict__ shi = reinterpret_cast<const ulonglong2*>(INV ? P.shi_inv : P.shi_fwd);
+        auto twiddle = [&](typename A::T v, int m, int w) {
+            if (tab) return A::twiddle(v, tb[(m << LW) + w], L);
+            const uint64_t k1 = __brev((unsigned)m) >> (32 - LC);
+            const uint64_t E = ((uint64_t)(tl.c0 + w) * k1) << esh;
+            return A::twiddle(A::twiddle(v, __ldg(shi + (E >> S)), L), __ldg(slo + (E & smask)), L);
+        };
+        auto in = [&](int m, int w) -> typename A::T {
+            const typename A::T v = A::ld(d[(m << LW) + w]);
+            return INV ? twiddle(v, m, w) : v;
+        };
+        auto pre = [&](int m, int w) -> ulonglong2 { return tab ? tb[(m << LW) + w] : make_ulonglong2(0, 0); };
+        auto out = [&](int m, int w, typename A::T v, const ulonglong2* tp) {
+            if (!INV) v = (tp != nullptr && tab) ? A::twiddle(v, *tp, L) : twiddle(v, m, w);
+            tl.base[((size_t)m << lM) + w] = A::st(v);
+        };
+        cols_fast_round<INV, LC, LW, RB, 0, A>(d, L, reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd),
+                                               in, out, pre);
+        __syncthreads();  // buffer b is free again
+        if (threadIdx.x < 32 && t + 2 * step < ntiles) {
+            fence_async_smem();
+            bulk_fetch<LC, LW>(bulk_tile(B, pt, k, lpre, lM, LW, t + 2 * step), lM, dbuf[b], tbuf[b], &bars[b]);
+        }
+    }
+}
+
 // The SplitSrc input written into `data` (for passes that read `data`).
 __global__ void src_split_kernel(NttBatch B, int k)
 {
@@ -1379,6 +1550,88 @@ static bool launch_cols_fast(const NttBatch& b, int k, int lpre, int lc, int lw,
     }
 }
 
+// Column passes through the bulk-copy kernel (PIC_TUNE_COLS_BULK): FP64
+// form, columns of 2^5 .. 2^9 rows, tiles 2^3 .. 2^6 columns wide, data
+// 16-byte aligned with an even item stride.
+// g_cols_bulk: 0 off, else log2 of the largest tile (points) the kernel
+// takes; tiles are narrowed to it so that more CTAs share an SM.
+static int g_cols_bulk = 0;
+void ntt_set_cols_bulk(int bits) { g_cols_bulk = bits; }
+int ntt_cols_bulk() { return g_cols_bulk; }
+
+bool ntt_take_bulk_error()
+{
+    int e = 0, zero = 0;
+    PIC_CUDA(cudaMemcpyFromSymbol(&e, g_ntt_bulk_error, sizeof e));
+    if (e) PIC_CUDA(cudaMemcpyToSymbol(g_ntt_bulk_error, &zero, sizeof zero));
+    return e != 0;
+}
+
+template <bool INV, int LC, int LW, int RB, bool TAB>
+static bool launch_cols_bulk_tab(const NttBatch& b, int k, int lpre, const PassTw& pt, size_t ntiles, cudaStream_t s)
+{
+    auto kern = ntt_cols_bulk_kernel<INV, LC, LW, RB, TAB, ArithDbl>;
+    constexpr size_t smem = BulkShape<LC, LW, TAB>::SMEM;
+    set_smem(kern, smem);
+    int per_sm = 0;
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    if (per_sm < 1) return false;
+    const size_t grid = std::min(ntiles, (size_t)ctx().num_sms * (size_t)per_sm);
+    kern<<<(unsigned)grid, 256, smem, s>>>(b, k, lpre, pt, ntiles);
+    return true;
+}
+
+template <bool INV, int LC, int LW, int RB>
+static bool launch_cols_bulk_t(const NttBatch& b, int k, int lpre, size_t ntiles, cudaStream_t s)
+{
+    PassTw pt{};
+    bool all = true;
+    for (int q = 0; q * b.per_prime < b.count; q++) {
+        pt.t[q] = pass_table(b.prime[q], INV, k - lpre, LC, s);
+        all = all && pt.t[q] != nullptr;
+    }
+    if (!all) return launch_cols_bulk_tab<INV, LC, LW, RB, false>(b, k, lpre, PassTw{}, ntiles, s);
+    return launch_cols_bulk_tab<INV, LC, LW, RB, true>(b, k, lpre, pt, ntiles, s);
+}
+
+template <bool INV, int LC, int RB>
+static bool launch_cols_bulk_lc(const NttBatch& b, int k, int lpre, int lw, size_t ntiles, cudaStream_t s)
+{
+    switch (lw) {
+    case 3: if constexpr (LC + 3 <= 12) return launch_cols_bulk_t<INV, LC, 3, RB>(b, k, lpre, ntiles, s); break;
+    case 4: if constexpr (LC + 4 <= 12) return launch_cols_bulk_t<INV, LC, 4, RB>(b, k, lpre, ntiles, s); break;
+    case 5: if constexpr (LC + 5 <= 12) return launch_cols_bulk_t<INV, LC, 5, RB>(b, k, lpre, ntiles, s); break;
+    case 6: if constexpr (LC + 6 <= 12) return launch_cols_bulk_t<INV, LC, 6, RB>(b, k, lpre, ntiles, s); break;
+    default: break;
+    }
+    return false;
+}
+
+template <bool INV>
+static bool launch_cols_bulk(const NttBatch& b, int k, int lpre, int lc, int lw, size_t ntiles, cudaStream_t s)
+{
+    if (!g_cols_bulk || !b.prime[0].fp64 || b.src.words != nullptr || ((uintptr_t)b.data & 15) || (b.stride & 1))
+        return false;
+    if (lc + lw > g_cols_bulk) lw = g_cols_bulk - lc;
+    if (lw < 3) return false;
+    ntiles = (size_t)b.count << (k - lpre - lc - lw + lpre);  // tiles of the narrowed width
+    if (geom_of(b, k).rbits == 4) {
+        switch (lc) {
+        case 8: return launch_cols_bulk_lc<INV, 8, 4>(b, k, lpre, lw, ntiles, s);
+        case 9: return launch_cols_bulk_lc<INV, 9, 4>(b, k, lpre, lw, ntiles, s);
+        default: break;
+        }
+    }
+    switch (lc) {
+    case 5: return launch_cols_bulk_lc<INV, 5, 3>(b, k, lpre, lw, ntiles, s);
+    case 6: return launch_cols_bulk_lc<INV, 6, 3>(b, k, lpre, lw, ntiles, s);
+    case 7: return launch_cols_bulk_lc<INV, 7, 3>(b, k, lpre, lw, ntiles, s);
+    case 8: return launch_cols_bulk_lc<INV, 8, 3>(b, k, lpre, lw, ntiles, s);
+    case 9: return launch_cols_bulk_lc<INV, 9, 3>(b, k, lpre, lw, ntiles, s);
+    default: return false;
+    }
+}
+
 template <bool INV>
 static bool launch_rows_fast_any(const NttBatch& b, int k, int lr, cudaStream_t s)
 {
@@ -1452,6 +1705,12 @@ static void launch_cols(bool inv, const NttBatch& b, int k, int lpre, int lc, cu
     const size_t grid = (size_t)b.count << (lM - lw + lpre);
     const size_t smem = sizeof(uint64_t) << (lc + lw);
     ProfScope ps(KC_NTT_COLS, 16.0 * (double)b.count * (double)((size_t)1 << k), s);
+    if (fast_ok(b, k) && b.prime[0].slo_fwd != nullptr &&
+        (inv ? launch_cols_bulk<true>(b, k, lpre, lc, lw, grid, s) : launch_cols_bulk<false>(b, k, lpre, lc, lw, grid, s))) {
+        PIC_CHECK_LAUNCH();
+        count_launch();
+        return;
+    }
     if (fast_ok(b, k) && b.prime[0].slo_fwd != nullptr &&
         (inv ? launch_cols_fast_any<true>(b, k, lpre, lc, lw, grid, s)
              : launch_cols_fast_any<false>(b, k, lpre, lc, lw, grid, s))) {

@@ -144,6 +144,14 @@ void ntt_set_geometry(int k, int row_bits, int col_lw, int rbits, int form = kFo
 // 2^bits points (0: never), else the two-level tables.
 void ntt_set_dbl_pass_bits(int bits);
 int ntt_dbl_pass_bits();
+// FP64 column passes of 2^5 .. 2^9 rows through the persistent kernel fed by
+// TMA bulk copies, with tiles of at most 2^bits points (0: the
+// one-tile-per-CTA kernel).
+void ntt_set_cols_bulk(int bits);
+int ntt_cols_bulk();
+// True (and cleared) when a bulk-copy wait of a column pass timed out since
+// the last call; synchronises with the device.
+bool ntt_take_bulk_error();
 void ntt_get_geometry(int k, int* row_bits, int* col_lw, int* rbits, int form = kFormInt);
 
 }  // namespace pic

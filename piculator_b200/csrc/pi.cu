@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "mul.cuh"
 #include "pi.cuh"
+#include "ntt.cuh"
 
 namespace pic {
 
@@ -146,6 +147,7 @@ BigFloat pi_compute(uint64_t decimal_digits, int mode, pic_pi_stats* st)
     }
     set_mul_mode(saved_mode);
     timeline_dump();
+    PIC_REQUIRE(!ntt_take_bulk_error(), PIC_ERR_TIMEOUT, "a bulk-copy wait of an NTT column pass timed out");
     if (st) {
         memset(st, 0, sizeof *st);
         st->hex_digits = hex;

@@ -122,3 +122,42 @@ def test_pi_in_fp64_form_large(pic, golden, digits):
     import hashlib
     text, _ = _pi_in_form(pic, digits, pic.FORM_DBL)
     assert hashlib.md5(text).hexdigest() == golden["pi"][str(digits)]["md5"]
+
+
+@pytest.mark.parametrize("row_bits", [11, 12, 13])
+def test_cols_bulk_kernel_matches_integer_form(pic, row_bits):
+    """FP64 column passes through the persistent kernel fed by TMA bulk copies
+    (PIC_TUNE_COLS_BULK): every column height 2^5 .. 2^9 it serves, tile widths
+    2^3 .. 2^6, radix 8 and 16, with and without per-point pass tables, give
+    the integer form's words."""
+    saved = {k: pic.get_ntt_geometry(k, pic.FORM_DBL) for k in range(14, 26)}
+    knobs = {pic.TUNE_COLS_BULK: pic.get_tuning(pic.TUNE_COLS_BULK),
+             pic.TUNE_DBL_PASS_TABLES: pic.get_tuning(pic.TUNE_DBL_PASS_TABLES)}
+    try:
+        for lg, bits in ((16, 12), (19, 10), (22, 11)):
+            pic.set_tuning(pic.TUNE_COLS_BULK, bits)
+            n = 1 << lg
+            a, b = random_words(lg + 3 * row_bits, n), random_words(lg + 5 * row_bits, n - 7)
+            want = pic.mul_host(a, b, "ntt3")
+            for lw, rb, tables in ((0, 3, 24), (3, 4, 24), (6, 3, 0), (4, 3, 20)):
+                pic.set_tuning(pic.TUNE_DBL_PASS_TABLES, tables)
+                for k in range(14, 26):
+                    pic.set_ntt_geometry(k, row_bits, lw, rb, pic.FORM_DBL)
+                assert np.array_equal(pic.mul_host(a, b, "ntt3d"), want), (lg, lw, rb, tables)
+    finally:
+        for k, (r, lw, rb) in saved.items():
+            pic.set_ntt_geometry(k, r, lw, rb, pic.FORM_DBL)
+        for k, v in knobs.items():
+            pic.set_tuning(k, v)
+
+
+@pytest.mark.parametrize("digits", [1_000_000, 10_000_000, 27_182_818])
+def test_pi_with_cols_bulk_kernel(pic, golden, digits):
+    import hashlib
+    saved = pic.get_tuning(pic.TUNE_COLS_BULK)
+    pic.set_tuning(pic.TUNE_COLS_BULK, 10)
+    try:
+        text, _ = _pi_in_form(pic, digits, pic.FORM_DBL)
+    finally:
+        pic.set_tuning(pic.TUNE_COLS_BULK, saved)
+    assert hashlib.md5(text).hexdigest() == golden["pi"][str(digits)]["md5"]
