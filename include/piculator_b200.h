@@ -295,7 +295,8 @@ enum {
     PIC_TUNE_BSR_KARATSUBA = 9,   /* CTA schoolbook merges take one Karatsuba level for operands of at
                                      least this many words (0 = never) */
     PIC_TUNE_NTT_FORM = 10,       /* three-prime form of AUTO products and binary-splitting merges:
-                                     0 integer (PIC_MUL_NTT3), 1 FP64 (PIC_MUL_NTT3D) */
+                                     0 integer (PIC_MUL_NTT3), 1 FP64 (PIC_MUL_NTT3D), 2 chosen per
+                                     product (or merge level) by the transform work of the two forms */
     PIC_TUNE_DBL_PASS_TABLES = 11, /* FP64 column passes over blocks of at most 2^value points (0..24,
                                      default 20) stream per-point twiddle tables; longer blocks form the
                                      twiddles from the two-level tables */

@@ -31,8 +31,8 @@ CKPT_WRITE, CKPT_RESUME = 1, 2
 MUL_AUTO, MUL_NTT_REF, MUL_NTT3, MUL_FFT, MUL_SCHOOL, MUL_NTT3D = range(6)
 MUL_MODES = {"auto": MUL_AUTO, "ntt_ref": MUL_NTT_REF, "ntt3": MUL_NTT3, "fft": MUL_FFT,
              "school": MUL_SCHOOL, "ntt3d": MUL_NTT3D}
-# three-prime product forms (PIC_TUNE_NTT_FORM)
-FORM_INT, FORM_DBL = 0, 1
+# three-prime product forms (PIC_TUNE_NTT_FORM; FORM_CHOSEN picks per product)
+FORM_INT, FORM_DBL, FORM_CHOSEN = 0, 1, 2
 # pi forms
 PI_CHOSEN, PI_PLAIN = 0, 1
 

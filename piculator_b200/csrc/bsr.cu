@@ -1332,7 +1332,10 @@ constexpr size_t kDblMergeMaxPieces = (size_t)1 << 26;
 static MergeShape merge_shape(uint32_t cmax)
 {
     MergeShape m;
-    m.form = (mul_ntt_form() == kFormDbl && pieces56(cmax) <= kDblMergeMaxPieces) ? kFormDbl : kFormInt;
+    {
+        const size_t si = ((size_t)cmax + 1) / 2, sd = pieces56(cmax);
+        m.form = (sd <= kDblMergeMaxPieces && ntt_form_for(si, si, sd, sd, g_wrap) == kFormDbl) ? kFormDbl : kFormInt;
+    }
     const size_t smax = m.form == kFormDbl ? pieces56(cmax) : ((size_t)cmax + 1) / 2;
     const size_t L = smax ? 2 * smax - 1 : 1;
     int k = ceil_log2_sz(L);

@@ -654,7 +654,7 @@ pic_status pic_set_tuning(int knob, int64_t value)
             mul_set_fft_accept((double)value * 1e-6);
             break;
         case PIC_TUNE_NTT_FORM:
-            PIC_REQUIRE(value <= 1, PIC_ERR_INVALID, "product form is 0 (integer) or 1 (FP64)");
+            PIC_REQUIRE(value <= 2, PIC_ERR_INVALID, "product form is 0 (integer), 1 (FP64) or 2 (chosen per product)");
             mul_set_ntt_form((int)value);
             break;
         case PIC_TUNE_COLS_BULK:

@@ -1231,14 +1231,52 @@ void mul_set_thresholds(int64_t school_max, int64_t fft_max)
 int64_t mul_school_max() { return g_school_max_words; }
 int64_t mul_fft_max() { return g_fft_max_words; }
 
-// The three-prime form AUTO and the binary splitting use (kFormInt / kFormDbl).
+// The three-prime form AUTO and the binary splitting use: kFormInt,
+// kFormDbl, or kFormChosen (per product, the form with less transform work).
 static int g_ntt_form = kFormInt;
 void mul_set_ntt_form(int form)
 {
-    PIC_REQUIRE(form == kFormInt || form == kFormDbl, PIC_ERR_INVALID, "unknown product form");
+    PIC_REQUIRE(form == kFormInt || form == kFormDbl || form == kFormChosen, PIC_ERR_INVALID,
+                "unknown product form");
     g_ntt_form = form;
 }
 int mul_ntt_form() { return g_ntt_form; }
+
+// Butterfly work (sum of N log2 N over the transforms) of a three-prime
+// product with `coefs` coefficients and operands of at most per_max pieces,
+// under the plain / wrapped rule of mul_ntt3 and mul_ntt3d.
+static double ntt_work(size_t coefs, size_t per_max, bool wrap)
+{
+    int k = ceil_log2(coefs);
+    if (k < 1) k = 1;
+    const size_t N = (size_t)1 << k;
+    if (wrap && k >= 4) {
+        const size_t Nm = N / 2;
+        if (per_max <= Nm && coefs > Nm) {
+            int kt = ceil_log2(2 * (coefs - Nm) - 1);
+            if (kt < 2) kt = 2;
+            if (((size_t)1 << kt) <= Nm / 2) return (double)Nm * (k - 1) + (double)((size_t)1 << kt) * kt;
+        }
+    }
+    return (double)N * k;
+}
+
+// The FP64 form's cost per butterfly relative to the integer form's, at equal
+// transform length (isolated products of 2^20 .. 2^26 points: 0.83 - 0.90).
+constexpr double kDblWorkRatio = 0.87;
+
+int ntt_form_for(size_t pieces_int_a, size_t pieces_int_b, size_t pieces_dbl_a, size_t pieces_dbl_b, bool wrap)
+{
+    if (g_ntt_form != kFormChosen) return g_ntt_form;
+    const double wi = ntt_work(pieces_int_a + pieces_int_b - 1, std::max(pieces_int_a, pieces_int_b), wrap);
+    const double wd = ntt_work(pieces_dbl_a + pieces_dbl_b - 1, std::max(pieces_dbl_a, pieces_dbl_b), wrap);
+    return wd * kDblWorkRatio < wi ? kFormDbl : kFormInt;
+}
+
+static int product_form(size_t na, size_t nb)
+{
+    return ntt_form_for((na + 1) / 2, (nb + 1) / 2, pieces56(na), pieces56(nb), g_mul_wrap);
+}
 
 int mul_auto_mode(size_t na, size_t nb)
 {
@@ -1246,7 +1284,7 @@ int mul_auto_mode(size_t na, size_t nb)
     const size_t zw = na + nb;
     if (zw <= kSchoolMaxWords && (mn <= 48 || (int64_t)zw <= g_school_max_words)) return PIC_MUL_SCHOOL;
     if ((int64_t)zw <= g_fft_max_words) return PIC_MUL_FFT;
-    return g_ntt_form == kFormDbl ? PIC_MUL_NTT3D : PIC_MUL_NTT3;
+    return product_form(na, nb) == kFormDbl ? PIC_MUL_NTT3D : PIC_MUL_NTT3;
 }
 
 static std::atomic<uint64_t> g_fft_err_bits{0};
@@ -1307,7 +1345,7 @@ void mul_dispatch(uint32_t* z, const uint32_t* a, size_t na, const uint32_t* b, 
             // the NTT is the oracle: a product whose rounding distance passed
             // the acceptance threshold is redone exactly
             ctx().fft_recomputes.fetch_add(1);
-            if (g_ntt_form == kFormDbl) mul_ntt3d(z, a, na, b, nb, s);
+            if (product_form(na, nb) == kFormDbl) mul_ntt3d(z, a, na, b, nb, s);
             else mul_ntt3(z, a, na, b, nb, s);
         }
         return;

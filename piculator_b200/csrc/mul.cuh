@@ -23,9 +23,13 @@ void ntt3d_batch_to_words(const uint64_t* y, size_t istride, size_t pstride, siz
                           uint32_t zcap, const uint32_t* zlen, cudaStream_t s, size_t ncoef, bool offset);
 void launch_wrap_fix_d(uint64_t* y, size_t ystride, const uint64_t* tail, size_t T, size_t nitems,
                        size_t item_mul, size_t nchild, size_t Nm, size_t W, cudaStream_t s);
-// The three-prime form of AUTO products and binary-splitting merges.
+// The three-prime form of AUTO products and binary-splitting merges
+// (kFormInt, kFormDbl, or kFormChosen: per product by transform work).
 void mul_set_ntt_form(int form);
 int mul_ntt_form();
+// The form a product of operands of the given piece counts (64-bit pieces
+// for the integer form, 56-bit for the FP64 one) takes under the setting.
+int ntt_form_for(size_t pieces_int_a, size_t pieces_int_b, size_t pieces_dbl_a, size_t pieces_dbl_b, bool wrap);
 
 // While alive, three-prime products on this thread that take the operand
 // (src, n) transform it once per transform length and reuse that forward

@@ -89,7 +89,7 @@ const PrimeTables& dbl_prime_tables(uint64_t p);
 // Product forms: the integer three-prime NTT (64-bit pieces, primes below
 // 2^61, lazy Shoup butterflies) and the FP64 one (56-bit pieces, primes below
 // 2^47, butterflies on the FP64 pipe).
-enum NttForm { kFormInt = 0, kFormDbl = 1 };
+enum NttForm { kFormInt = 0, kFormDbl = 1, kFormChosen = 2 };
 
 // A batch of transforms of length 2^k laid out at data + i * stride
 // (i < count); transform i uses prime[i / per_prime].

@@ -161,3 +161,25 @@ def test_pi_with_cols_bulk_kernel(pic, golden, digits):
     finally:
         pic.set_tuning(pic.TUNE_COLS_BULK, saved)
     assert hashlib.md5(text).hexdigest() == golden["pi"][str(digits)]["md5"]
+
+
+@pytest.mark.parametrize("digits", [1_000_000, 10_000_000, 27_182_818])
+def test_pi_in_chosen_form(pic, golden, digits):
+    """Form chosen per product and merge level (PIC_TUNE_NTT_FORM 2): levels
+    and products of both forms in one computation, the reference's digits."""
+    import hashlib
+    text, _ = _pi_in_form(pic, digits, pic.FORM_CHOSEN)
+    assert hashlib.md5(text).hexdigest() == golden["pi"][str(digits)]["md5"]
+
+
+@pytest.mark.parametrize("n", [1000, 5000, 1 << 14, 40000, 1 << 17, 300001])
+def test_auto_products_in_chosen_form(pic, n):
+    a = random_words(n + 17, n)
+    b = random_words(n + 19, n - 3)
+    saved = pic.get_tuning(pic.TUNE_NTT_FORM)
+    pic.set_tuning(pic.TUNE_NTT_FORM, pic.FORM_CHOSEN)
+    try:
+        z = pic.mul_host(a, b, "auto")
+    finally:
+        pic.set_tuning(pic.TUNE_NTT_FORM, saved)
+    assert _int(z) == _int(a) * _int(b)
