@@ -917,8 +917,9 @@ __global__ void __launch_bounds__(256) merge_pointwise_kernel(uint64_t* __restri
 }
 
 // The same on FP64-form residues (signed doubles, fp64mod.cuh): forward
-// outputs |x| <= 0.75 p give products |y| <= 0.75 p, and T1 +- T2 stays below
-// 1.5 p, inside what the FP64 inverse accepts.
+// outputs |x| <= p give products |y| <= 0.75 p (the quotient of a product
+// below p^2 is off by far less than 1/4), and T1 +- T2 stays below 1.5 p,
+// inside what the FP64 inverse accepts.
 struct DblMod3 {
     double p[3], pinv[3];
 };

@@ -45,19 +45,17 @@ __global__ void __launch_bounds__(256) butterfly_ceiling_kernel(uint64_t* out, c
 }
 
 // The same radix-8 DIF groups with the FP64 butterflies of the FP64 form
-// (fp64mod.cuh): signed residues below 0.75 p in and out of every group, the
-// sums reduced at the group's last level, mod the first FP64 prime.
+// (fp64mod.cuh, twiddles w with the companion formed per use): signed
+// residues below p in and out of every group, the sums reduced at the
+// group's last level, mod the first FP64 prime.
 __global__ void __launch_bounds__(256) butterfly_ceiling_dbl_kernel(uint64_t* out, const uint64_t* tw, double p,
                                                                     int iters)
 {
     const double pinv = 1.0 / p;
     double x[8];
     for (int m = 0; m < 8; m++) x[m] = dreduce((double)(threadIdx.x * 8 + m + blockIdx.x), p, pinv);
-    double w[7], wp[7];
-    for (int i = 0; i < 7; i++) {
-        w[i] = dbits(tw[2 * (i + threadIdx.x % 8)]);
-        wp[i] = dbits(tw[2 * (i + threadIdx.x % 8) + 1]);
-    }
+    double w[7];
+    for (int i = 0; i < 7; i++) w[i] = dbits(tw[i + threadIdx.x % 8]);
     for (int it = 0; it < iters; it++) {
 #pragma unroll
         for (int l = 0; l < 3; l++) {
@@ -67,7 +65,7 @@ __global__ void __launch_bounds__(256) butterfly_ceiling_dbl_kernel(uint64_t* ou
                 if (m & hm) continue;
                 const int ti = (l == 0 ? 0 : (l == 1 ? 4 : 6)) + (m & (hm - 1));
                 const double sm = __dadd_rn(x[m], x[m + hm]), d = __dadd_rn(x[m], -x[m + hm]);
-                x[m + hm] = dmul_tw(d, w[ti], wp[ti], p);
+                x[m + hm] = dmul_w(d, w[ti], p, pinv);
                 x[m] = l == 2 ? dreduce(sm, p, pinv) : sm;
             }
         }
@@ -83,10 +81,9 @@ double butterfly_ceiling_dbl(cudaStream_t s)
     uint64_t htw[32];
     uint64_t w = 1;
     const uint64_t g = host_powmod(smallest_generator(p), (p - 1) >> 16, p);  // a root of order 2^16
-    for (int i = 0; i < 16; i++) {
-        const double wd = (double)w, wp = wd / (double)p;
-        memcpy(&htw[2 * i], &wd, 8);
-        memcpy(&htw[2 * i + 1], &wp, 8);
+    for (int i = 0; i < 32; i++) {
+        const double wd = (double)w;
+        memcpy(&htw[i], &wd, 8);
         w = host_mulmod(w, g, p);
     }
     const int blocks = ctx().num_sms * 8, threads = 256, iters = 1000;

@@ -10,6 +10,9 @@
 //    r = (h - q p) + l.  With |y| < 2^51 the quotient is within 0.75 of
 //    y w / p, so |r| <= 0.75 p, and h - q p is an integer below 2^50 in
 //    magnitude, hence exact; r + l is exact for the same reason.
+//  * the same with the companion formed in place, wp = fl(w fl(1 / p))
+//    (dmul_w, what the transforms use: their tables hold w alone): the
+//    quotient is within 1 of y w / p, |r| <= p.
 //  * a b mod p for two residues: the same with q = rint(h / p) from
 //    fl(1 / p); |r| <= 0.75 p whenever |a b| < 2^51 p.
 //  * reduction s mod p: s - rint(s / p) p, |r| <= p / 2 + 1 (for |s| < 2^56).
@@ -34,6 +37,14 @@ __device__ __forceinline__ double dmul_tw(double y, double w, double wp, double 
     const double h = __dmul_rn(y, w);
     const double l = __fma_rn(y, w, -h);
     return __dadd_rn(__fma_rn(-q, p, h), l);
+}
+
+// y * w mod p with the companion formed here, wp = fl(w fl(1 / p)) (relative
+// error below 2^-52, so the quotient is within 1 of y w / p): |result| <= p,
+// for |y| < 2^51, 0 <= w < p.  The FP64 form's twiddle tables hold w alone.
+__device__ __forceinline__ double dmul_w(double y, double w, double p, double pinv)
+{
+    return dmul_tw(y, w, __dmul_rn(w, pinv), p);
 }
 
 // a * b mod p, |result| <= 0.75 p, for |a b| < 2^51 p (|a|, |b| < 2^51).

@@ -191,11 +191,12 @@ const PrimeTables& prime_tables(uint64_t p)
     return *t;
 }
 
-static void dbl_pairs(std::vector<uint64_t>& v, size_t i, uint64_t w, uint64_t p)
+// An FP64 table entry: w as a double (the companion fl(w fl(1 / p)) is formed
+// where the twiddle is used).
+static void dbl_entry(std::vector<uint64_t>& v, size_t i, uint64_t w)
 {
-    const double wd = (double)w, wp = wd / (double)p;
-    memcpy(&v[2 * i], &wd, 8);
-    memcpy(&v[2 * i + 1], &wp, 8);
+    const double wd = (double)w;
+    memcpy(&v[i], &wd, 8);
 }
 
 const PrimeTables& dbl_prime_tables(uint64_t p)
@@ -220,34 +221,34 @@ const PrimeTables& dbl_prime_tables(uint64_t p)
     const uint64_t wIi = host_powmod(wKi, (uint64_t)1 << (K - IB), p);
     // per-level inner tables: the root of order 2^m is wI^(2^(IB - m)); pair
     // 2^(m-1) - 1 + e holds its e-th power
-    std::vector<uint64_t> lf((size_t)2 << IB), li((size_t)2 << IB);
+    std::vector<uint64_t> lf((size_t)1 << IB), li((size_t)1 << IB);
     for (int lm = 1; lm <= IB; lm++) {
         const uint64_t r = host_powmod(wI, (uint64_t)1 << (IB - lm), p);
         const uint64_t ri = host_powmod(wIi, (uint64_t)1 << (IB - lm), p);
         uint64_t a = 1, b = 1;
         for (size_t e = 0; e < ((size_t)1 << (lm - 1)); e++) {
             const size_t dst = ((size_t)1 << (lm - 1)) - 1 + e;
-            dbl_pairs(lf, dst, a, p);
-            dbl_pairs(li, dst, b, p);
+            dbl_entry(lf, dst, a);
+            dbl_entry(li, dst, b);
             a = host_mulmod(a, r, p);
             b = host_mulmod(b, ri, p);
         }
     }
     // two-level outer tables: root_(2^K)^i (i < 2^S) and root_(2^K)^(i 2^S)
-    std::vector<uint64_t> lof((size_t)2 << S), loi((size_t)2 << S);
-    std::vector<uint64_t> hif((size_t)2 << (K - S)), hii((size_t)2 << (K - S));
+    std::vector<uint64_t> lof((size_t)1 << S), loi((size_t)1 << S);
+    std::vector<uint64_t> hif((size_t)1 << (K - S)), hii((size_t)1 << (K - S));
     uint64_t a = 1, b = 1;
     for (size_t i = 0; i < ((size_t)1 << S); i++) {
-        dbl_pairs(lof, i, a, p);
-        dbl_pairs(loi, i, b, p);
+        dbl_entry(lof, i, a);
+        dbl_entry(loi, i, b);
         a = host_mulmod(a, wK, p);
         b = host_mulmod(b, wKi, p);
     }
     const uint64_t wS = a, wSi = b;
     a = 1, b = 1;
     for (size_t i = 0; i < ((size_t)1 << (K - S)); i++) {
-        dbl_pairs(hif, i, a, p);
-        dbl_pairs(hii, i, b, p);
+        dbl_entry(hif, i, a);
+        dbl_entry(hii, i, b);
         a = host_mulmod(a, wS, p);
         b = host_mulmod(b, wSi, p);
     }
@@ -772,14 +773,17 @@ __device__ __forceinline__ void fbfly_unit_dit(uint64_t& a, uint64_t& b, const L
 
 // Arithmetic of the fast passes.  ArithInt: lazy Shoup butterflies on 64-bit
 // residues (lazy primes).  ArithDbl: FP64 butterflies (FP64 primes, values
-// stored as the bits of doubles).  `LAST` marks the last level of a register
+// stored as the bits of doubles; twiddles w form their companion per use,
+// so a product lands below p).  `LAST` marks the last level of a register
 // round: the FP64 forward butterflies reduce their sums there, so every
-// round starts and ends with |x| <= 0.75 p; inside a round of B levels the
-// values stay below 2^B 0.75 p (12 p for radix-16, under 2^51).  FP64
-// inverse butterflies add at most 0.75 p per level and never reduce: a pass
-// of L levels over inputs below X ends below 2 X + (L - 1) 0.75 p.
+// round starts and ends with |x| <= p; inside a round of B levels the values
+// stay below 2^B p (16 p for radix-16, under 2^51 for primes below 2^47).
+// FP64 inverse butterflies add at most p per level and never reduce: a pass
+// of L levels over inputs below X ends below 2 X + (L - 1) p (15 p for a
+// 13-level row pass over the merges' T1 +- T2, below 1.5 p).
 struct ArithInt {
     using T = uint64_t;
+    using Tw = ulonglong2;  // twiddle table entry: Shoup pair (w, w')
     using Ctx = LazyPrime;
     static __device__ __forceinline__ Ctx ctx(const PrimeDev& P) { return lazy_prime(P); }
     static __device__ __forceinline__ T ld(uint64_t v) { return v; }
@@ -804,6 +808,7 @@ struct ArithInt {
 
 struct ArithDbl {
     using T = double;
+    using Tw = double;  // twiddle table entry: w; the companion is formed per use (dmul_w)
     struct Ctx {
         double p, pinv;
     };
@@ -811,10 +816,10 @@ struct ArithDbl {
     static __device__ __forceinline__ T ld(uint64_t v) { return dbits(v); }
     static __device__ __forceinline__ uint64_t st(T v) { return dstore(v); }
     template <bool LAST>
-    static __device__ __forceinline__ void dif(T& a, T& b, const ulonglong2 t, const Ctx& L)
+    static __device__ __forceinline__ void dif(T& a, T& b, const Tw t, const Ctx& L)
     {
         const double s = __dadd_rn(a, b), d = __dadd_rn(a, -b);
-        b = dmul_tw(d, dbits(t.x), dbits(t.y), L.p);
+        b = dmul_w(d, t, L.p, L.pinv);
         a = LAST ? dreduce(s, L.p, L.pinv) : s;
     }
     template <bool LAST>
@@ -824,9 +829,9 @@ struct ArithDbl {
         a = LAST ? dreduce(s, L.p, L.pinv) : s;
         b = LAST ? dreduce(d, L.p, L.pinv) : d;
     }
-    static __device__ __forceinline__ void dit(T& a, T& b, const ulonglong2 t, const Ctx& L)
+    static __device__ __forceinline__ void dit(T& a, T& b, const Tw t, const Ctx& L)
     {
-        const double u = dmul_tw(b, dbits(t.x), dbits(t.y), L.p);
+        const double u = dmul_w(b, t, L.p, L.pinv);
         b = __dadd_rn(a, -u);
         a = __dadd_rn(a, u);
     }
@@ -836,10 +841,7 @@ struct ArithDbl {
         b = __dadd_rn(a, -b);
         a = s;
     }
-    static __device__ __forceinline__ T twiddle(T v, const ulonglong2 t, const Ctx& L)
-    {
-        return dmul_tw(v, dbits(t.x), dbits(t.y), L.p);
-    }
+    static __device__ __forceinline__ T twiddle(T v, const Tw t, const Ctx& L) { return dmul_w(v, t, L.p, L.pinv); }
     static __device__ __forceinline__ T piece(const NttBatch& B, const SrcRow& r, size_t j, const Ctx& L)
     {
         return dpiece56(src_piece56_raw(r.x, r.n, B.src.first + j), L.p, L.pinv);
@@ -852,7 +854,7 @@ struct ArithDbl {
 // lanes with consecutive j read consecutive pairs.
 template <int B, bool INV, int LST, class A>
 __device__ __forceinline__ void group_fast(typename A::T (&x)[1 << B], int j, const typename A::Ctx& L,
-                                           const ulonglong2* __restrict__ tw)
+                                           const typename A::Tw* __restrict__ tw)
 {
     static_assert(B + LST <= 13, "sub-block larger than the inner table");
     if (!INV) {
@@ -868,7 +870,7 @@ __device__ __forceinline__ void group_fast(typename A::T (&x)[1 << B], int j, co
             for (int m = 0; m < (1 << B); m++) {
                 if (m & hm) continue;
                 const int u = m & (hm - 1);
-                const ulonglong2 t = __ldg(tw + ((1 << (B - l + LST - 1)) - 1) + j + (u << LST));
+                const typename A::Tw t = __ldg(tw + ((1 << (B - l + LST - 1)) - 1) + j + (u << LST));
                 if (l == B - 1) A::template dif<true>(x[m], x[m + hm], t, L);
                 else A::template dif<false>(x[m], x[m + hm], t, L);
             }
@@ -916,7 +918,7 @@ struct RoundPlan {
 // through out(t, e, v).  The rounds between exchange through shared memory.
 template <bool INV, int LR, int LRPC, int NT, int RB, int R, bool OUT_DIRECT, class A, class In, class Out>
 __device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const NttBatch& Bt, size_t row0,
-                                                const typename A::Ctx& L0, const ulonglong2* __restrict__ tw0,
+                                                const typename A::Ctx& L0, const typename A::Tw* __restrict__ tw0,
                                                 const In& in, const Out& out)
 {
     using Plan = RoundPlan<LR, RB>;
@@ -935,11 +937,11 @@ __device__ __forceinline__ void rows_fast_round(uint64_t* __restrict__ s, const 
         const int base = ((gi >> LST) << LB) + j;
         uint64_t* ptr = s + (t << LR);
         typename A::Ctx L = L0;
-        const ulonglong2* tw = tw0;
+        const typename A::Tw* tw = tw0;
         if (LRPC > 0 && row0 + t < (size_t)Bt.count) {  // rows past the batch keep the CTA's prime
             const PrimeDev Pt = pick_prime(Bt, (int)(row0 + t));
             L = A::ctx(Pt);
-            tw = reinterpret_cast<const ulonglong2*>(INV ? Pt.lvl_inv : Pt.lvl_fwd);
+            tw = reinterpret_cast<const typename A::Tw*>(INV ? Pt.lvl_inv : Pt.lvl_fwd);
         }
         typename A::T x[1 << B];
 #pragma unroll
@@ -1004,7 +1006,7 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape
         if (LRPC == 0 || row0 + t < nrows) data[at(t, e)] = A::st(v);
     };
     rows_fast_round<INV, LR, LRPC, NT, RB, 0, INV, A>(
-        smem, B, row0, L, reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd), in, out);
+        smem, B, row0, L, reinterpret_cast<const typename A::Tw*>(INV ? P.lvl_inv : P.lvl_fwd), in, out);
     if constexpr (!INV) {
 #pragma unroll
         for (int i = 0; i < TOT / NT; i++) {
@@ -1031,7 +1033,7 @@ __global__ void __launch_bounds__(RowsFastShape<LR, LRPC, RB>::NT, RowsFastShape
 
 template <bool INV, int LC, int LW, int RB, int R, class A, class In, class Out, class Pre>
 __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const typename A::Ctx& L,
-                                                const ulonglong2* __restrict__ tw, const In& in, const Out& out,
+                                                const typename A::Tw* __restrict__ tw, const In& in, const Out& out,
                                                 const Pre& pre)
 {
     using Plan = RoundPlan<LC, RB>;
@@ -1055,7 +1057,7 @@ __device__ __forceinline__ void cols_fast_round(uint64_t* __restrict__ s, const 
             else x[m] = A::ld(s[(r << LW) + w]);
         }
         constexpr bool PRE = LAST && !INV && PIC_COLS_TW_PREFETCH;
-        ulonglong2 tp[PRE ? (1 << B) : 1];
+        typename A::Tw tp[PRE ? (1 << B) : 1];
         if constexpr (PRE) {
 #pragma unroll
             for (int m = 0; m < (1 << B); m++) tp[m] = pre(base + (m << LST), w);
@@ -1089,26 +1091,31 @@ __device__ __forceinline__ uint64_t shoup_companion_dev(uint64_t x, uint64_t p, 
 // (FP64 primes: the pair (w, fl(w / p)) of doubles), laid out like the data
 // so the pass streams it with the same coalescing.
 struct PassTw {
-    const ulonglong2* t[kMaxPrimesPerBatch];
+    const void* t[kMaxPrimesPerBatch];  // ulonglong2 Shoup pairs, or doubles (FP64 primes)
 };
 
-__global__ void pass_table_kernel(ulonglong2* __restrict__ out, PrimeDev P, int inv, int lblock, int lc)
+__global__ void pass_table_kernel(void* __restrict__ out_v, PrimeDev P, int inv, int lblock, int lc)
 {
     const size_t n = (size_t)1 << lblock;
     const int lM = lblock - lc;
     const int esh = P.K - lblock;
-    const ulonglong2* slo = reinterpret_cast<const ulonglong2*>(inv ? P.slo_inv : P.slo_fwd);
-    const ulonglong2* shi = reinterpret_cast<const ulonglong2*>(inv ? P.shi_inv : P.shi_fwd);
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
         const uint64_t m = g >> lM, c = g & (((size_t)1 << lM) - 1);
         const uint64_t k1 = __brev((unsigned)m) >> (32 - lc);
         const uint64_t E = (c * k1) << esh;
-        const ulonglong2 h = __ldg(shi + (E >> P.S)), l = __ldg(slo + (E & (((uint64_t)1 << P.S) - 1)));
-        if (P.fp64) {
-            const double x = dcanon(dmul_tw(dbits(h.x), dbits(l.x), dbits(l.y), P.pd), P.pd);
-            out[g] = make_ulonglong2(dstore(x), dstore(__ddiv_rn(x, P.pd)));
+        const uint64_t ehi = E >> P.S, elo = E & (((uint64_t)1 << P.S) - 1);
+        if (P.fp64) {  // doubles w, |w| < p after dmul_w, brought into [0, p)
+            const double* dlo = reinterpret_cast<const double*>(inv ? P.slo_inv : P.slo_fwd);
+            const double* dhi = reinterpret_cast<const double*>(inv ? P.shi_inv : P.shi_fwd);
+            double x = dmul_w(__ldg(dhi + ehi), __ldg(dlo + elo), P.pd, P.pinv);
+            x = dcanon(x >= P.pd ? __dadd_rn(x, -P.pd) : x, P.pd);
+            reinterpret_cast<double*>(out_v)[g] = x;
             continue;
         }
+        const ulonglong2* slo = reinterpret_cast<const ulonglong2*>(inv ? P.slo_inv : P.slo_fwd);
+        const ulonglong2* shi = reinterpret_cast<const ulonglong2*>(inv ? P.shi_inv : P.shi_fwd);
+        ulonglong2* out = reinterpret_cast<ulonglong2*>(out_v);
+        const ulonglong2 h = __ldg(shi + ehi), l = __ldg(slo + elo);
         const LazyPrime L = lazy_prime(P);
         uint64_t x = shoup_lazy32(h.x, l.x, l.y, L.c);
         x = x >= L.p ? x - L.p : x;
@@ -1151,15 +1158,17 @@ __global__ void __launch_bounds__(256, ColsMinBlocks<A, RB, INV>::value)
     const int esh = P.K - (k - lpre);  // exponents of a root of order 2^(k - lpre), scaled to order 2^K
     const int S = P.S;
     const uint64_t smask = ((uint64_t)1 << S) - 1;
-    const ulonglong2* __restrict__ slo = reinterpret_cast<const ulonglong2*>(INV ? P.slo_inv : P.slo_fwd);
-    const ulonglong2* __restrict__ shi = reinterpret_cast<const ulonglong2*>(INV ? P.shi_inv : P.shi_fwd);
-    const ulonglong2* __restrict__ T = tr < B.per_prime ? pt.t[0] : (tr < 2 * B.per_prime ? pt.t[1] : pt.t[2]);
+    using Tw = typename A::Tw;
+    const Tw* __restrict__ slo = reinterpret_cast<const Tw*>(INV ? P.slo_inv : P.slo_fwd);
+    const Tw* __restrict__ shi = reinterpret_cast<const Tw*>(INV ? P.shi_inv : P.shi_fwd);
+    const Tw* __restrict__ T =
+        static_cast<const Tw*>(tr < B.per_prime ? pt.t[0] : (tr < 2 * B.per_prime ? pt.t[1] : pt.t[2]));
     auto twiddle = [&](typename A::T v, int m, int w) {
         if (T != nullptr)  // the pass table: one product, streamed like the data
             return A::twiddle(v, __ldg(T + ((size_t)m << lM) + c0 + w), L);
         const uint64_t k1 = __brev((unsigned)m) >> (32 - LC);
         const uint64_t E = ((uint64_t)(c0 + w) * k1) << esh;
-        const ulonglong2 h = __ldg(shi + (E >> S)), l = __ldg(slo + (E & smask));
+        const Tw h = __ldg(shi + (E >> S)), l = __ldg(slo + (E & smask));
         return A::twiddle(A::twiddle(v, h, L), l, L);
     };
     // first forward column pass (lpre == 0) with a split source: point
@@ -1173,16 +1182,13 @@ __global__ void __launch_bounds__(256, ColsMinBlocks<A, RB, INV>::value)
     };
     // pre(m, w): the pass-table pair of point (m, w) (zero without a table);
     // out applies a preloaded pair when it gets one
-    auto pre = [&](int m, int w) -> ulonglong2 {
-        return T != nullptr ? __ldg(T + ((size_t)m << lM) + c0 + w) : make_ulonglong2(0, 0);
-    };
-    auto out = [&](int m, int w, typename A::T v, const ulonglong2* t) {
+    auto pre = [&](int m, int w) -> Tw { return T != nullptr ? __ldg(T + ((size_t)m << lM) + c0 + w) : Tw{}; };
+    auto out = [&](int m, int w, typename A::T v, const Tw* t) {
         if (!INV) v = (t != nullptr && T != nullptr) ? A::twiddle(v, *t, L) : twiddle(v, m, w);
         base[((size_t)m << lM) + w] = A::st(v);
     };
     cols_fast_round<INV, LC, LW, RB, 0, A>(smem, L,
-                                           reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd), in, out,
-                                           pre);
+                                           reinterpret_cast<const Tw*>(INV ? P.lvl_inv : P.lvl_fwd), in, out, pre);
 }
 
 // ---- column passes fed by TMA bulk copies ------------------------------------
@@ -1245,7 +1251,7 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 struct BulkTile {
     int tr;
     uint64_t* base;        // the tile's first point (row 0, column c0)
-    const ulonglong2* T;   // its pass-table rows (null: two-level tables)
+    const double* T;       // its pass-table rows (FP64 twiddles w; null: two-level tables)
     uint32_t c0;
 };
 
@@ -1259,21 +1265,21 @@ __device__ __forceinline__ BulkTile bulk_tile(const NttBatch& B, const PassTw& p
     const size_t ob = rem >> ltiles;
     r.c0 = (uint32_t)((rem & (((size_t)1 << ltiles) - 1)) << LW);
     r.base = B.data + (size_t)r.tr * B.stride + (ob << (k - lpre)) + r.c0;
-    r.T = r.tr < B.per_prime ? pt.t[0] : (r.tr < 2 * B.per_prime ? pt.t[1] : pt.t[2]);
+    r.T = static_cast<const double*>(r.tr < B.per_prime ? pt.t[0] : (r.tr < 2 * B.per_prime ? pt.t[1] : pt.t[2]));
     return r;
 }
 
 // Warp 0 fetches tile t into (d, tb) completing on bar.
 template <int LC, int LW>
-__device__ __forceinline__ void bulk_fetch(const BulkTile& tl, int lM, uint64_t* d, ulonglong2* tb, uint64_t* bar)
+__device__ __forceinline__ void bulk_fetch(const BulkTile& tl, int lM, uint64_t* d, double* tb, uint64_t* bar)
 {
     const int lane = threadIdx.x & 31;
-    const uint32_t bytes = (uint32_t)((8u + (tl.T != nullptr ? 16u : 0u)) << (LC + LW));
+    const uint32_t bytes = (uint32_t)((8u + (tl.T != nullptr ? 8u : 0u)) << (LC + LW));
     if (lane == 0) mbar_expect_tx(bar, bytes);
     __syncwarp();
     for (int m = lane; m < (1 << LC); m += 32) {
         bulk_load(d + (m << LW), tl.base + ((size_t)m << lM), 8u << LW, bar);
-        if (tl.T != nullptr) bulk_load(tb + (m << LW), tl.T + ((size_t)m << lM) + tl.c0, 16u << LW, bar);
+        if (tl.T != nullptr) bulk_load(tb + (m << LW), tl.T + ((size_t)m << lM) + tl.c0, 8u << LW, bar);
     }
 }
 
@@ -1281,7 +1287,7 @@ template <int LC, int LW, bool TAB>
 struct BulkShape {
     static constexpr int TOT = 1 << (LC + LW);
     static constexpr size_t DATA = sizeof(uint64_t) * TOT;
-    static constexpr size_t TABB = TAB ? sizeof(ulonglong2) * TOT : 0;
+    static constexpr size_t TABB = TAB ? sizeof(double) * TOT : 0;
     static constexpr size_t SMEM = 2 * (DATA + TABB) + 64;  // two buffers and the barriers
 };
 
@@ -1291,8 +1297,7 @@ __global__ void __launch_bounds__(256, 2) ntt_cols_bulk_kernel(NttBatch B, int k
     using Sh = BulkShape<LC, LW, TAB>;
     extern __shared__ __align__(128) uint64_t bsm[];
     uint64_t* dbuf[2] = {bsm, bsm + Sh::TOT};
-    ulonglong2* tbuf[2] = {reinterpret_cast<ulonglong2*>(bsm + 2 * Sh::TOT),
-                           reinterpret_cast<ulonglong2*>(bsm + 2 * Sh::TOT) + Sh::TOT};
+    double* tbuf[2] = {reinterpret_cast<double*>(bsm + 2 * Sh::TOT), reinterpret_cast<double*>(bsm + 3 * Sh::TOT)};
     uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(bsm) + 2 * (Sh::DATA + Sh::TABB));
     const int lM = k - lpre - LC;
     if (threadIdx.x == 0) {
@@ -1323,13 +1328,13 @@ __global__ void __launch_bounds__(256, 2) ntt_cols_bulk_kernel(NttBatch B, int k
         const PrimeDev P = pick_prime(B, tl.tr);
         const typename A::Ctx L = A::ctx(P);
         uint64_t* __restrict__ d = dbuf[b];
-        const ulonglong2* __restrict__ tb = tbuf[b];
+        const double* __restrict__ tb = tbuf[b];
         const bool tab = TAB && tl.T != nullptr;
         const int esh = P.K - (k - lpre);
         const int S = P.S;
         const uint64_t smask = ((uint64_t)1 << S) - 1;
-        const ulonglong2* __restrict__ slo = reinterpret_cast<const ulonglong2*>(INV ? P.slo_inv : P.slo_fwd);
-        const ulonglong2* __restrict__ shi = reinterpret_cast<const ulonglong2*>(INV ? P.shi_inv : P.shi_fwd);
+        const double* __restrict__ slo = reinterpret_cast<const double*>(INV ? P.slo_inv : P.slo_fwd);
+        const double* __restrict__ shi = reinterpret_cast<const double*>(INV ? P.shi_inv : P.shi_fwd);
         auto twiddle = [&](typename A::T v, int m, int w) {
             if (tab) return A::twiddle(v, tb[(m << LW) + w], L);
             const uint64_t k1 = __brev((unsigned)m) >> (32 - LC);
@@ -1340,12 +1345,12 @@ __global__ void __launch_bounds__(256, 2) ntt_cols_bulk_kernel(NttBatch B, int k
             const typename A::T v = A::ld(d[(m << LW) + w]);
             return INV ? twiddle(v, m, w) : v;
         };
-        auto pre = [&](int m, int w) -> ulonglong2 { return tab ? tb[(m << LW) + w] : make_ulonglong2(0, 0); };
-        auto out = [&](int m, int w, typename A::T v, const ulonglong2* tp) {
+        auto pre = [&](int m, int w) -> double { return tab ? tb[(m << LW) + w] : 0.0; };
+        auto out = [&](int m, int w, typename A::T v, const double* tp) {
             if (!INV) v = (tp != nullptr && tab) ? A::twiddle(v, *tp, L) : twiddle(v, m, w);
             tl.base[((size_t)m << lM) + w] = A::st(v);
         };
-        cols_fast_round<INV, LC, LW, RB, 0, A>(d, L, reinterpret_cast<const ulonglong2*>(INV ? P.lvl_inv : P.lvl_fwd),
+        cols_fast_round<INV, LC, LW, RB, 0, A>(d, L, reinterpret_cast<const double*>(INV ? P.lvl_inv : P.lvl_fwd),
                                                in, out, pre);
         __syncthreads();  // buffer b is free again
         if (threadIdx.x < 32 && t + 2 * step < ntiles) {
@@ -1459,7 +1464,7 @@ static bool launch_rows_fast(const NttBatch& b, int k, int lr, cudaStream_t s)
 // reads a complete table.
 constexpr int kPassTableMaxBits = 24;
 static std::mutex g_pass_lock;
-static std::map<std::tuple<int, uint64_t, int, int, int>, ulonglong2*> g_pass_tables;
+static std::map<std::tuple<int, uint64_t, int, int, int>, void*> g_pass_tables;
 
 // FP64 column passes stream the per-point table only for blocks of at most
 // 2^g_dbl_pass_bits points (tables that stay in L2); longer ones form each
@@ -1469,7 +1474,8 @@ static int g_dbl_pass_bits = 20;
 void ntt_set_dbl_pass_bits(int bits) { g_dbl_pass_bits = bits; }
 int ntt_dbl_pass_bits() { return g_dbl_pass_bits; }
 
-static const ulonglong2* pass_table(const PrimeDev& P, bool inv, int lblock, int lc, cudaStream_t s)
+// Entries are Shoup pairs (16 bytes), or the twiddle w alone (8 bytes) for FP64 primes.
+static const void* pass_table(const PrimeDev& P, bool inv, int lblock, int lc, cudaStream_t s)
 {
     if (lblock > kPassTableMaxBits || (P.fp64 && lblock > g_dbl_pass_bits)) return nullptr;
     int dev = 0;
@@ -1481,8 +1487,8 @@ static const ulonglong2* pass_table(const PrimeDev& P, bool inv, int lblock, int
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     PIC_CUDA(cudaStreamIsCapturing(s, &cs));
     if (cs != cudaStreamCaptureStatusNone) return nullptr;
-    ulonglong2* d = nullptr;
-    if (raw_dev_alloc((void**)&d, sizeof(ulonglong2) << lblock) != cudaSuccess)
+    void* d = nullptr;
+    if (raw_dev_alloc(&d, (P.fp64 ? sizeof(double) : sizeof(ulonglong2)) << lblock) != cudaSuccess)
         return nullptr;  // no room: the pass keeps the two-level tables
     const size_t n = (size_t)1 << lblock;
     pass_table_kernel<<<grid_for(n, 256), 256, 0, s>>>(d, P, inv ? 1 : 0, lblock, lc);
@@ -1816,7 +1822,7 @@ __global__ void pointwise_mont_kernel(NttBatch B, const uint64_t* __restrict__ o
         const size_t tr = g >> k, i = g & (n - 1);
         const PrimeDev P = pick_prime(B, (int)tr);
         uint64_t* d = B.data + tr * B.stride + i;
-        if (P.fp64) {  // forward outputs |x| <= 0.75 p: the product is below 0.57 p^2
+        if (P.fp64) {  // forward outputs |x| <= p: the product is below p^2
             *d = dstore(dmul_mod(dbits(*d), dbits(other[tr * ostride + i]), P.pd, P.pinv));
             continue;
         }

@@ -59,8 +59,9 @@ struct PrimeDev {
     // floor(2^128 / p) = mu_hi 2^64 + mu_lo: Shoup companions on the device
     uint64_t mu_hi, mu_lo;
     // FP64 primes (below 2^47, the FP64 product form): residues are doubles
-    // holding signed integers, and every table pair is (w, fl(w / p)) as the
-    // bits of two doubles.  Only the fast passes serve them.
+    // holding signed integers, and every table entry is the twiddle w as the
+    // bits of one double (the level, outer and pass tables keep their indexing
+    // with 8-byte entries).  Only the fast passes serve them.
     int fp64;
     double pd, pinv;  // p and fl(1 / p)
 };

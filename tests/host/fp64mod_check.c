@@ -1,6 +1,7 @@
 /* Host restatement of the FP64 modular arithmetic of fp64mod.cuh (the FP64
  * three-prime form), checked against 128-bit integer arithmetic:
- *   dmul_tw:  y w mod p, |r| <= 0.75 p, |y| < 2^51, 0 <= w < p, wp = fl(w / p)
+ *   dmul_tw:  y w mod p, |r| <= 0.75 p, |y| < 2^51, 0 <= w < p, wp = fl(w / p);
+ *             |r| <= p with wp = fl(w fl(1 / p)) (the FP64 form's companion)
  *   dmul_mod: a b mod p, |r| <= 0.75 p, |a b| < 2^51 p
  *   dreduce:  s mod p,   |r| <= p / 2 + 1, |s| < 2^56
  * Built with -ffp-contract=off so that every multiply, add and fma rounds
@@ -76,6 +77,18 @@ int main(int argc, char** argv)
             if (want < 0) want += p;
             const double wd = (double)w;
             if (!check(dmul_tw((double)y, wd, wd / pd, pd), want, pd, 0.75 * pd, &maxr)) bad++;
+            /* the companion formed in the butterfly, fl(w fl(1/p)): |r| <= p
+               for |y| up to 16 p (the largest forward value of a radix-16
+               round and the CRT's largest input) */
+            {
+                const int64_t lim16 = (int64_t)(16 * p) - 1;
+                int64_t y16 = (it & 1) ? (int64_t)(rnd() % (2 * (uint64_t)lim16 + 1)) - lim16
+                                       : ((it & 2) ? lim16 - (int64_t)(rnd() % 64) : -lim16 + (int64_t)(rnd() % 64));
+                __int128 w16 = ((__int128)y16 * (int64_t)w) % (__int128)p;
+                if (w16 < 0) w16 += p;
+                double maxr16 = 0;
+                if (!check(dmul_tw((double)y16, wd, wd * pinv, pd), w16, pd, pd, &maxr16)) bad++;
+            }
             /* two residues below 0.75 p */
             const int64_t a = (int64_t)(rnd() % (p + p / 2)) - (int64_t)(3 * p / 4);
             const int64_t b = (int64_t)(rnd() % (p + p / 2)) - (int64_t)(3 * p / 4);
