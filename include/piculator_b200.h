@@ -236,7 +236,9 @@ typedef struct {
     double seconds_hex;
     double seconds_total;
     uint64_t kernel_launches;
-    uint64_t products;     /* number of big products formed */
+    uint64_t products;     /* products formed: four per merge above the binary splitting's
+                              bottom depth, plus every BigFloat product (the bottom depth's
+                              merges of two leaves, done in registers, are not counted) */
     double fft_max_err;    /* largest FFT rounding distance seen */
     uint64_t fft_recomputes;
     uint64_t transform_reuses; /* Newton products that reused the iterate's forward transform */

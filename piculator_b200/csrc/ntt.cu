@@ -1195,7 +1195,7 @@ __global__ void __launch_bounds__(256, ColsMinBlocks<A, RB, INV>::value)
 // A persistent CTA walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
 // Each row of a tile (2^LW consecutive points, and the matching 2^LW pass-table
 // pairs) is one contiguous, 16-byte-aligned run, so warp 0 fetches a tile with
-// 2^LC bulk copies (cp.async.bulk, no multicast) that complete on an
+// 2^LC bulk copies (plain cp.async.bulk into the CTA's own shared memory) that complete on an
 // mbarrier; two buffers let the copies of tile i + 1 land while tile i is
 // computed.  Every wait is bounded: a wait that outlasts ~1 s of SM clocks
 // sets g_ntt_bulk_error, drains the other buffer's copy (also bounded) and
