@@ -223,6 +223,54 @@ class Oracle(_Lib):
             raise RuntimeError(n)
         return buf.raw[:n]
 
+    def pi_number(self, digits: int) -> BF:
+        """Pi()'s final number before base conversion (PI.h:176-199), composed
+        from the restated operations: the series, the combination with
+        13591409 and 4270934400, the division, invsqrt(10005) and the final
+        product, each at precision p."""
+        _, p, terms = self.pi_sizes(digits)
+        P, Q, _ = self.bsr(0, terms, p)
+        P = self.add(self.mul_u32(Q, 13591409), P, p)
+        Q = self.mul_u32(Q, 4270934400)
+        P = self.div(Q, P, p)
+        return self.mul(P, self.invsqrt(10005, p), p)
+
+
+def _below_top(x: BF) -> tuple[int, int]:
+    """(M, B): the integer held by every word below the top one, and its bit
+    width B = 32 (L - 1)."""
+    w = np.ascontiguousarray(x.words[:-1], dtype="<u4")
+    return int.from_bytes(w.tobytes(), "little"), 32 * (x.L - 1)
+
+
+def to_string_dec(x: BF, digits: int) -> bytes:
+    """BigFloat::to_string_dec (BigFloat.cpp:83-94): the top word in decimal,
+    a point, then nine digits per round -- clear the top word, multiply the
+    number by 10^9 (mul(uint32), BigFloat.cpp:156-183) and print the new top
+    word -- and the text cut to 2 + digits characters.  With the top word
+    cleared the multiply never carries out of the top word, so the length
+    stays L and each round is M <- M 10^9, digit group = M >> B, M <- M mod
+    2^B on the words below the top.  Sign and exponent are not printed."""
+    M, B = _below_top(x)
+    mask = (1 << B) - 1
+    out = [str(int(x.words[-1])), "."]
+    for _ in range((digits + 8) // 9):
+        M *= 1_000_000_000
+        out.append("%09d" % (M >> B))
+        M &= mask
+    return "".join(out)[: 2 + digits].encode()
+
+
+def to_string_hex(x: BF, digits: int) -> bytes:
+    """BigFloat::to_string_hex (BigFloat.cpp:95-106): the top word in decimal,
+    a point, then the words below it from the top down as eight hex digits
+    each, cut to 2 + digits characters."""
+    w = x.words
+    if (digits + 7) // 8 > x.L - 1:
+        raise ValueError("more hex digits than words below the top (the reference reads before T[0])")
+    groups = "".join("%08x" % int(w[x.L - 2 - i]) for i in range((digits + 7) // 8))
+    return (str(int(w[-1])) + "." + groups)[: 2 + digits].encode()
+
 
 class Reference(_Lib):
     """The reference's own code (oracle/_ref/libpicref.so)."""

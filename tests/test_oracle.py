@@ -146,3 +146,66 @@ def test_fft_convention_vs_reference(oracle, reference):
         a = oracle.fft(k, x, inverse=inv)
         b = reference.fft(k, x, inverse=inv)
         assert np.allclose(a, b, rtol=1e-12, atol=1e-9)
+
+
+# ---- decimal output (BigFloat::to_string_dec, BigFloat.cpp:83-94) -------------
+
+def _dec_case_words(rec):
+    w = random_words(rec["seed"], rec["L"])
+    if rec["top_mod7"]:
+        w[-1] = (w[-1] % 7) + 1
+    return w
+
+
+_DEC_EDGE = {"ones": np.full(300, 0xFFFFFFFF, dtype=np.uint32),
+             "zeros_below_top": np.array([0] * 299 + [3], dtype=np.uint32),
+             "single_low_bit": np.array([1] + [0] * 298 + [3], dtype=np.uint32)}
+
+
+def _dec_closed_form(x: BF, digits: int) -> bytes:
+    """The closed form the GPU decimal conversion computes: the digits after
+    the point are those of N = floor(M 10^D / 2^B), M the words below the top,
+    B = 32 (L - 1), D = 9 ceil(digits / 9), written with D digits."""
+    import sys
+    if hasattr(sys, "set_int_max_str_digits"):
+        sys.set_int_max_str_digits(0)  # the decimal text of N has D digits
+    w = np.ascontiguousarray(x.words[:-1], dtype="<u4")
+    M, B = int.from_bytes(w.tobytes(), "little"), 32 * (x.L - 1)
+    D = 9 * ((digits + 8) // 9)
+    text = str(int(x.words[-1])) + "." + str((M * 10 ** D) >> B).zfill(D)
+    return text[: 2 + digits].encode()
+
+
+@pytest.mark.parametrize("form", ["literal", "closed"])
+def test_decimal_text_matches_reference_numbers(golden, form):
+    """Seeded numbers (one- and multi-character integer parts, 0..190,000
+    digits) and edge cases, against the reference program's own text."""
+    from oracle.ffi import to_string_dec
+    conv = to_string_dec if form == "literal" else _dec_closed_form
+    for rec in golden["dec"]["numbers"]:
+        if form == "literal" and rec["digits"] > 30_000:
+            continue  # the nine-digit loop is quadratic; the closed form covers these
+        text = conv(BF(True, -rec["L"] + 1, _dec_case_words(rec)), rec["digits"])
+        assert len(text) == rec["len"], rec
+        if "text" in rec:
+            assert text.decode() == rec["text"], rec
+        assert hashlib.md5(text).hexdigest() == rec["md5"], rec
+    for rec in golden["dec"]["edge"]:
+        text = conv(BF(True, 0, _DEC_EDGE[rec["kind"]]), rec["digits"])
+        assert hashlib.md5(text).hexdigest() == rec["md5"] and text[-60:].decode() == rec["tail"], rec["kind"]
+
+
+@pytest.mark.parametrize("digits", [10_000, 100_000])
+def test_pi_decimal_text_matches_reference(oracle, golden, digits):
+    """Pi()'s final number from the restated operations: its hex text is the
+    oracle's pi.txt, and its decimal text (nine-digit loop and closed form)
+    is the reference program's to_string_dec of the same number."""
+    from oracle.ffi import to_string_dec, to_string_hex
+    x = oracle.pi_number(digits)
+    hexd, _, _ = oracle.pi_sizes(digits)
+    assert to_string_hex(x, hexd) == oracle.pi_hex(digits)
+    g = golden["dec"]["pi"][str(digits)]
+    lit = to_string_dec(x, digits)
+    assert lit == _dec_closed_form(x, digits)
+    assert len(lit) == g["len"] and lit[:80].decode() == g["head"] and lit[-80:].decode() == g["tail"]
+    assert hashlib.md5(lit).hexdigest() == g["md5"]
