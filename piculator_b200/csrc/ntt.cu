@@ -29,7 +29,8 @@ const uint64_t kProductPrimes[3] = {2305842979148922881ull, 2305842949084151809u
 // product form's: their product is ~2^140.99, so a convolution of 56-bit
 // pieces whose shorter operand has at most 2^28 pieces (coefficients below
 // 2^140) is recovered exactly, and with the offset 2^140 so is a signed sum
-// of two products of at most 2^27 pieces.  Below 2^47, forward values up to
+// of two products of at most 2^26 pieces (the merges' limit; at 2^27 the
+// worst case would pass the primes' product).  Below 2^47, forward values up to
 // 16 p stay under 2^51, the range of the FP64 quotient.
 const uint64_t kDblPrimes[3] = {140496970186753ull, 140458315481089ull, 140449725546497ull};
 
