@@ -172,6 +172,35 @@ def max_over_ranks(values, dist=None, device="cpu"):
 
 
 # ---------------------------------------------------------- reference arm ----
+def reference_small_configs(threads: int) -> dict:
+    """The reference program at its CPU-runnable configurations, on all host
+    threads and on one: Pi() to 10^6 digits (its own timer, tables excluded)
+    and isolated products BigFloat::mul(x, 0) of 2^12 / 2^16 / 2^20-word
+    splitmix64 operands (seeds 42 and 43, the operands of the GPU arm's
+    isolated products; best of three, one run at 2^20)."""
+    from oracle.ffi import BF, REF_SO, Reference, random_words
+    counts = sorted({1, threads})
+    out = {"pi_1e6_s": {str(th): run_reference_pi(1_000_000, th) for th in counts}}
+    if os.path.exists(REF_SO):
+        ref = Reference()
+        prods = {}
+        for lg in (12, 16, 20):
+            a = BF(True, 0, random_words(42, 1 << lg))
+            b = BF(True, 0, random_words(43, 1 << lg))
+            row = {}
+            for th in counts:
+                best = float("inf")
+                for _ in range(3 if lg < 20 else 1):
+                    t0 = time.perf_counter()
+                    ref.mul(a, b, 0, th)
+                    best = min(best, time.perf_counter() - t0)
+                row[str(th)] = best
+            prods[str(lg)] = row
+        out["isolated_products_s"] = prods
+    out["unit"] = "s, keyed by host thread count"
+    return out
+
+
 def reference_arm(args):
     rank, _, world = rank_info()
     if rank != 0:
@@ -203,6 +232,10 @@ def reference_arm(args):
     else:
         value = t_step * (args.digits / sample)
         basis = f"reference Pi() at {sample} digits per step, scaled linearly to {args.digits} digits"
+    try:
+        small = reference_small_configs(threads)
+    except Exception as e:  # a reported baseline only: the line still prints
+        small = {"error": f"{type(e).__name__}: {e}"}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1000.0,
@@ -210,6 +243,7 @@ def reference_arm(args):
         "data": "synthetic", "config": {"workload": f"pi_{args.digits:.0e}_digits", "digits": args.digits,
                                         "parallelism": "replicas"},
         "measured": {f"pi_{sample:.0e}_s": t_step, f"pi_{calib:.0e}_s": t_calib, "threads": threads},
+        "cpu_runnable_configs": small,
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference",
                          "sample": basis},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -55,3 +55,32 @@ def test_measured_peak_is_read_from_the_driver_file():
     peak, kind = bench.measured_peaks()
     assert peak > 1000.0
     assert kind in ("measured", "fallback")
+
+
+def test_reference_arm_line_at_small_sizes():
+    """--impl reference on the host cores (no GPU): one JSON line with the
+    measured calibration run, the bounded samples and the CPU-runnable
+    configurations at one and all threads."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    import pytest
+
+    from oracle.ffi import REF_PI, REF_SO
+    if not (os.path.exists(REF_PI) and os.path.exists(REF_SO)):
+        pytest.skip("oracle/_ref not built (the reference sources are not in this checkout)")
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(bench.ROOT, "bench.py"), "--impl", "reference",
+                        "--steps", "1", "--warmup", "1", "--digits", "1000000", "--ref-sample", "10000",
+                        "--ref-calibration", "100000"], capture_output=True, text=True, env=env, timeout=600,
+                       check=True)
+    line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+    assert line["impl"] == "reference" and line["unit"] == "s" and line["higher_is_better"] is False
+    assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "reference"
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    small = line["cpu_runnable_configs"]
+    assert "error" not in small, small
+    assert small["pi_1e6_s"]["1"] > 0
+    assert set(small["isolated_products_s"]) == {"12", "16", "20"}
