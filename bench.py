@@ -137,12 +137,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def run_reference_pi(digits: int, threads: int) -> float:
+def run_reference_pi(digits: int, threads: int, with_tables: bool = False):
+    """Seconds of one reference Pi() run (its own timer, table construction
+    excluded); with_tables: (pi seconds, table seconds)."""
     from oracle.ffi import REF_PI
     with tempfile.TemporaryDirectory() as d:
         r = subprocess.run([REF_PI, str(digits), str(threads)], cwd=d, capture_output=True, text=True,
                            check=True)
-    return float(json.loads(r.stderr.strip().splitlines()[-1])["pi_s"])
+    rec = json.loads(r.stderr.strip().splitlines()[-1])
+    return (float(rec["pi_s"]), float(rec["tables_s"])) if with_tables else float(rec["pi_s"])
 
 
 def golden_pi():
@@ -174,13 +177,15 @@ def max_over_ranks(values, dist=None, device="cpu"):
 # ---------------------------------------------------------- reference arm ----
 def reference_small_configs(threads: int) -> dict:
     """The reference program at its CPU-runnable configurations, on all host
-    threads and on one: Pi() to 10^6 digits (its own timer, tables excluded)
-    and isolated products BigFloat::mul(x, 0) of 2^12 / 2^16 / 2^20-word
+    threads and on one: Pi() to 10^6 digits (its own timer, tables excluded;
+    the table construction reported beside it) and isolated products BigFloat::mul(x, 0) of 2^12 / 2^16 / 2^20-word
     splitmix64 operands (seeds 42 and 43, the operands of the GPU arm's
     isolated products; best of three, one run at 2^20)."""
     from oracle.ffi import BF, REF_SO, Reference, random_words
     counts = sorted({1, threads})
-    out = {"pi_1e6_s": {str(th): run_reference_pi(1_000_000, th) for th in counts}}
+    out = {"pi_1e6_s": {}, "pi_1e6_tables_s": {}}
+    for th in counts:
+        out["pi_1e6_s"][str(th)], out["pi_1e6_tables_s"][str(th)] = run_reference_pi(1_000_000, th, True)
     if os.path.exists(REF_SO):
         ref = Reference()
         prods = {}
