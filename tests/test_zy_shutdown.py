@@ -1,6 +1,7 @@
 """pic_shutdown frees the top-level workspace and trims the memory pool; a
-fresh pic_init afterwards computes the same digits (runs last: it replaces
-the library stream the other GPU tests use)."""
+fresh pic_init afterwards computes the same digits (runs after the other
+tests that use the library stream, which it replaces; only the
+allocation-free product's file is collected after it)."""
 from __future__ import annotations
 
 import hashlib
