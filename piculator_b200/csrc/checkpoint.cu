@@ -19,12 +19,14 @@
 //   count x { int32 sign, int32 pad, int64 exp, uint64 L, uint64 hash }
 //   the words of the count numbers, in order
 // hash = ckpt_hash over the number's words (see below); a file whose header
-// or hashes do not match is rejected (PIC_ERR_IO), never used.  A new file
-// is written beside the old one and renamed over it, so a crash while
-// writing leaves the previous checkpoint intact.
+// or hashes do not match, or whose length fields do not add up to the file's
+// size, is rejected (PIC_ERR_IO), never used.  A new file is written beside
+// the old one, flushed to disk and renamed over it, so a crash while writing
+// leaves the previous checkpoint intact.
 #include <errno.h>
 #include <stdio.h>
 #include <string.h>
+#include <unistd.h>
 
 #include <string>
 #include <vector>
@@ -103,8 +105,21 @@ int checkpoint_inspect_file(const char* path, uint64_t* digits, uint64_t* p_word
     if (p_words) *p_words = h.p_words;
     if (phase) *phase = h.phase;
     if (!verify) return 0;
+    // the words must fill the rest of the file exactly: checked before any
+    // buffer is sized from a length field, so a damaged length cannot ask
+    // for an enormous allocation
+    uint64_t want = 0;
     for (uint32_t i = 0; i < h.count; i++) {
         if (ent[i].L > ((uint64_t)1 << 36)) io_error("bad length", path);
+        want += 4 * ent[i].L;
+    }
+    const long pos = ftell(f.f);
+    if (pos < 0 || fseek(f.f, 0, SEEK_END) != 0) io_error("cannot seek", path);
+    const long end = ftell(f.f);
+    if (end < pos || fseek(f.f, pos, SEEK_SET) != 0) io_error("cannot seek", path);
+    if ((uint64_t)(end - pos) < want) io_error("truncated words", path);
+    if ((uint64_t)(end - pos) > want) io_error("trailing bytes", path);
+    for (uint32_t i = 0; i < h.count; i++) {
         std::vector<uint32_t> w(ent[i].L);
         if (ent[i].L && fread(w.data(), 4, ent[i].L, f.f) != ent[i].L) io_error("truncated words", path);
         if (ckpt_hash(w.data(), w.size()) != ent[i].hash) io_error("words do not match their hash", path);
@@ -161,7 +176,9 @@ void checkpoint_save(int phase, uint64_t digits, uint64_t p_words, uint64_t term
         if (!f.f) io_error(std::string("cannot create (") + strerror(errno) + ")", tmp);  // PI.h:42
         bool ok = fwrite(&h, sizeof h, 1, f.f) == 1 && fwrite(ent.data(), sizeof(Entry), ent.size(), f.f) == ent.size();
         for (const auto& w : words) ok = ok && (w.empty() || fwrite(w.data(), 4, w.size(), f.f) == w.size());
-        ok = ok && fflush(f.f) == 0;
+        // on disk before the rename, so the name never points at a file
+        // whose data a system crash could still lose
+        ok = ok && fflush(f.f) == 0 && fsync(fileno(f.f)) == 0;
         if (!ok) io_error("write failed", tmp);
     }
     if (rename(tmp.c_str(), path.c_str()) != 0) io_error(std::string("rename failed (") + strerror(errno) + ")", path);

@@ -79,3 +79,16 @@ def test_damaged_files_are_rejected(ck, damage):
         else:
             ck = ck + ".absent"
     _expect_io(ck)
+
+
+def test_huge_length_field_is_rejected_before_any_allocation(ck):
+    """A damaged length field (2^34 words, 64 GB) in a small file: the reader
+    compares the lengths with the file's size first and never sizes a buffer
+    from the field."""
+    import struct as S
+    w = np.arange(1, 94, dtype=np.uint32)
+    with open(ck, "wb") as f:
+        f.write(b"PICKPT01" + S.pack("<QQQII", 1000, 93, 72, 2, 1))
+        f.write(S.pack("<iiqQQ", 1, 0, -91, 1 << 34, ckpt_hash(w)))
+        f.write(w.astype("<u4").tobytes())
+    assert "truncated" in _expect_io(ck)
