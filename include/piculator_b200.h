@@ -116,6 +116,17 @@ pic_status pic_int_to_fft(double* T, int k, const uint32_t* A, size_t AL,
 pic_status pic_fft_to_int(const double* T, int k, uint32_t* A, size_t AL,
                           pic_stream s);                               /* FFT.h:9 */
 double pic_fft_last_max_err(void);
+/* The piece width FFT products use at transform length 2^k (one real piece
+ * per complex point): the widest b in 8..16 whose worst-case rounding error,
+ * pic_fft_error_bound(k, b), stays below 1/4; 0 when none does (k >= 27).
+ * Host arithmetic only, callable before pic_init.  No reference counterpart:
+ * the reference always packs 8-bit pieces and never bounds the error
+ * (FFT.cpp:485-519). */
+int pic_fft_piece_bits(int k);
+/* Worst-case rounding error of a length-2^k FFT convolution of b-bit pieces
+ * (C. Percival, Math. Comp. 72 (2003), Theorem 5.1, with twiddle error
+ * 2.5 * 2^-53); -1 for k outside 1..62 or bits outside 1..32. */
+double pic_fft_error_bound(int k, int bits);
 /* FFT products whose largest rounding distance passed the acceptance
  * threshold (0.25 unless PIC_TUNE_FFT_ACCEPT_PPM lowers it) and were
  * recomputed with the exact three-prime NTT, since pic_init.  No reference

@@ -107,6 +107,8 @@ _SIGS = {
     "pic_int_to_fft": ([_DP, C.c_int, _U32P, C.c_size_t, _P], C.c_int),
     "pic_fft_to_int": ([_DP, C.c_int, _U32P, C.c_size_t, _P], C.c_int),
     "pic_fft_last_max_err": ([], C.c_double),
+    "pic_fft_piece_bits": ([C.c_int], C.c_int),
+    "pic_fft_error_bound": ([C.c_int, C.c_int], C.c_double),
     "pic_fft_recompute_count": ([], C.c_uint64),
     "pic_product_count": ([], C.c_uint64),
     "pic_mul": ([_U32P, _U32P, C.c_size_t, _U32P, C.c_size_t, C.c_int, _P], C.c_int),

@@ -305,6 +305,13 @@ pic_status pic_fft_to_int(const double* T, int k, uint32_t* A, size_t AL, pic_st
 
 double pic_fft_last_max_err(void) { return fft_last_max_err(); }
 
+int pic_fft_piece_bits(int k) { return k < 1 || k > 62 ? 0 : fft_piece_bits(k); }
+
+double pic_fft_error_bound(int k, int bits)
+{
+    return k < 1 || k > 62 || bits < 1 || bits > 32 ? -1.0 : fft_error_bound(k, bits);
+}
+
 uint64_t pic_fft_recompute_count(void) { return ctx().fft_recomputes.load(); }
 
 uint64_t pic_product_count(void) { return ctx().products.load(); }
