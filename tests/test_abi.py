@@ -47,3 +47,24 @@ def test_calls_before_init_fail_cleanly():
     assert L.pic_synchronize() == P.ERR_NOT_INITIALIZED
     assert L.pic_init(0) in (P.ERR_CUDA, P.ERR_INVALID)
     assert L.pic_last_error()
+
+
+@pytest.mark.parametrize("lang", ["c99", "c++17"])
+def test_header_is_plain_c_and_links(tmp_path, lang):
+    """include/piculator_b200.h compiles warning-free as strict C99 and as
+    C++17, and a C program links the library and calls a host-only entry
+    point (the FFT piece width at 2^20 points) without a GPU."""
+    import shutil
+    cc = "gcc" if lang == "c99" else "g++"
+    if shutil.which(cc) is None:
+        pytest.skip(f"{cc} not available")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / ("main.c" if lang == "c99" else "main.cpp")
+    src.write_text('#include "piculator_b200.h"\n'
+                   "int main(void) { return pic_fft_piece_bits(20) == 11 ? 0 : 1; }\n")
+    exe = tmp_path / "main"
+    libdir = os.path.dirname(P.LIB_PATH)
+    subprocess.run([cc, f"-std={lang}", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                    "-I", os.path.join(root, "include"), str(src), "-L", libdir, "-lpiculator_b200",
+                    f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True, capture_output=True)
+    assert subprocess.run([str(exe)]).returncode == 0
