@@ -100,7 +100,7 @@ def _worker(rank, world, port, digits, q):
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3, 4])
+@pytest.mark.parametrize("world", [2, 3, 4, 6, 8])
 def test_pi_over_gloo_ranks_equals_single_process(world):
     digits = 20_000
     ctx = mp.get_context("spawn")
