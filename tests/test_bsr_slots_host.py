@@ -73,3 +73,29 @@ def test_merges_at_the_far_end_of_large_series_fit(end, size):
     fill = [0.0]
     _node(end - size, end, fill)
     assert fill[0] <= 1.0
+
+
+def _leaf(b: int):
+    P = (13591409 + 545140134 * b) * (2 * b - 1) * (6 * b - 5) * (6 * b - 1)
+    return P, 10939058860032000 * b ** 3, (2 * b - 1) * (6 * b - 5) * (6 * b - 1)
+
+
+def test_bottom_kernel_register_widths_hold_up_to_the_term_limit():
+    """The bottom depth's leaves and two-leaf merges are formed in fixed
+    register arrays (bsr.cu: LeafV's SW<6> / SW<5> / SW<4>, the merge's
+    SW<12> / SW<10> / SW<8>).  The largest values, at the last terms below the
+    reference's 2^32-term limit (PI.h:149-151), fit with the carry word."""
+    import re
+    src = open(os.path.join(ROOT, "piculator_b200", "csrc", "bsr.cu")).read()
+    leaf = re.search(r"struct LeafV \{\s*SW<(\d+)> P;\s*bool sP;\s*SW<(\d+)> Q;\s*SW<(\d+)> R;", src)
+    merge = re.search(r"SW<(\d+)> t1, t2, P;.*?SW<(\d+)> Q;\s*SW<(\d+)> R;", src, re.S)
+    assert leaf and merge
+    lp, lq, lr = (32 * int(v) for v in leaf.groups())
+    mp, mq, mr = (32 * int(v) for v in merge.groups())
+    b = 2 ** 32 - 1
+    P0, Q0, R0 = _leaf(b - 1)
+    P1, Q1, R1 = _leaf(b)
+    assert P1.bit_length() <= lp and Q1.bit_length() <= lq and R1.bit_length() <= lr
+    # P0 Q1 + P1 R0 with both signs alike (the sum), Q0 Q1, R0 R1
+    assert (P0 * Q1 + P1 * R0).bit_length() <= mp
+    assert (Q0 * Q1).bit_length() <= mq and (R0 * R1).bit_length() <= mr
