@@ -28,6 +28,7 @@ import argparse
 import ctypes as C
 import json
 import os
+import tempfile
 import time
 
 import numpy as np
@@ -230,6 +231,26 @@ def tune_bsr(quick: bool) -> dict:
             "seconds": res}
 
 
+def _read_table(path: str) -> dict:
+    with open(path) as f:
+        return json.load(f)
+
+
+def _write_table(path: str, result: dict) -> None:
+    """Write the table beside its destination and rename it over it, so an
+    interrupted run never leaves a truncated file for init() to load."""
+    d = os.path.dirname(os.path.abspath(path))
+    with tempfile.NamedTemporaryFile("w", suffix=".json", dir=d, delete=False) as f:
+        json.dump(result, f, indent=1)
+        tmp = f.name
+    try:
+        os.replace(tmp, path)
+    except BaseException:
+        os.unlink(tmp)
+        raise
+    print("wrote", path)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--quick", action="store_true")
@@ -245,31 +266,25 @@ def main():
     args = ap.parse_args()
     if args.only_fp64:
         P.init(0, tuned=True)
-        result = json.load(open(args.out))
+        result = _read_table(args.out)
         got = tune_ntt_batched(1_000_000_000, ks=range(10, 28), form=P.FORM_DBL, rows=(11, 12),
                                pass_bits=(20, 24))
         result.setdefault("products", {})["dbl_pass_bits"] = got.pop("dbl_pass_bits", 20)
         result["ntt_fp64"] = got
-        with open(args.out, "w") as f:
-            json.dump(result, f, indent=1)
-        print("wrote", args.out)
+        _write_table(args.out, result)
         return
     if args.only_bsr:
         P.init(0, tuned=True)
-        result = json.load(open(args.out))
+        result = _read_table(args.out)
         P.apply_tuning(args.out)
         result["bsr"] = tune_bsr(False)
-        with open(args.out, "w") as f:
-            json.dump(result, f, indent=1)
-        print("wrote", args.out)
+        _write_table(args.out, result)
         return
     if args.only_batched:
         P.init(0, tuned=True)
-        result = json.load(open(args.out))
+        result = _read_table(args.out)
         result["ntt"].update(tune_ntt_batched(1_000_000_000))
-        with open(args.out, "w") as f:
-            json.dump(result, f, indent=1)
-        print("wrote", args.out)
+        _write_table(args.out, result)
         return
     P.init(0, tuned=False)
     timer = Timer()
@@ -287,9 +302,7 @@ def main():
     P.set_tuning(P.TUNE_MUL_SCHOOL_MAX, prod["school_max_words"])
     P.set_tuning(P.TUNE_MUL_FFT_MAX, prod["fft_max_words"])
     result["bsr"] = tune_bsr(args.quick)
-    with open(args.out, "w") as f:
-        json.dump(result, f, indent=1)
-    print("wrote", args.out)
+    _write_table(args.out, result)
 
 
 if __name__ == "__main__":

@@ -47,3 +47,25 @@ def test_committed_tuning_table_is_well_formed():
     assert t["products"]["school_max_words"] >= 0
     assert t["products"]["fft_max_words"] >= 0
     assert t["bsr"]["bsr_school_max_words"] > 0
+
+
+def test_table_write_replaces_the_file_whole(tmp_path):
+    """The tuner writes its table beside the destination and renames it over
+    it: the old table stays until the new one is complete, and no temporary
+    file is left behind."""
+    from piculator_b200 import autotune
+    out = tmp_path / "tuning.json"
+    out.write_text('{"old": 1}')
+    autotune._write_table(str(out), {"ntt": {"20": {"row_bits": 11}}})
+    assert autotune._read_table(str(out)) == {"ntt": {"20": {"row_bits": 11}}}
+    assert sorted(p.name for p in tmp_path.iterdir()) == ["tuning.json"]
+
+
+def test_table_write_failure_keeps_the_old_table(tmp_path):
+    from piculator_b200 import autotune
+    out = tmp_path / "tuning.json"
+    out.write_text('{"old": 1}')
+    import pytest
+    with pytest.raises(TypeError):
+        autotune._write_table(str(out), {"bad": object()})  # not serialisable
+    assert autotune._read_table(str(out)) == {"old": 1}
