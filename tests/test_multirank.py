@@ -47,7 +47,7 @@ def test_max_over_ranks_single_process_is_identity():
     assert bench.max_over_ranks([3.0, 4.0]) == [3.0, 4.0]
 
 
-@pytest.mark.parametrize("n", [2, 3])
+@pytest.mark.parametrize("n", [2, 3, 8])
 def test_bench_gpus_flag_launches_n_replicas(n):
     """`bench.py --gpus N` outside torchrun re-launches itself as N ranks
     (torch.distributed.run on 127.0.0.1); with the launcher's self-test arm
@@ -74,3 +74,24 @@ def test_bench_rejects_rank_count_mismatch():
     r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--impl",
                         "replica-check"], capture_output=True, text=True, timeout=120, env=env, cwd=root)
     assert r.returncode != 0 and "ranks were launched" in r.stderr
+
+
+def test_reference_arm_under_two_ranks_prints_one_line():
+    """`bench.py --gpus 2 --impl reference`: rank 0 alone times the reference
+    program and prints the line; the other rank exits 0 without work."""
+    import json
+    import subprocess
+    import sys
+
+    from oracle.ffi import REF_PI, REF_SO
+    if not (os.path.exists(REF_PI) and os.path.exists(REF_SO)):
+        pytest.skip("oracle/_ref not built (the reference sources are not in this checkout)")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--impl", "reference",
+                        "--steps", "1", "--warmup", "1", "--digits", "1000000", "--ref-sample", "10000",
+                        "--ref-calibration", "100000"], capture_output=True, text=True, timeout=600, env=env,
+                       cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1 and lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
